@@ -1,0 +1,211 @@
+"""ctypes bindings of the CPU checkers. TEST INFRASTRUCTURE ONLY.
+
+``Oracle``    -- oracle/liboracle.so, the C restatement of the reference's generic kernels.
+``RefKernels`` -- oracle/_ref/libexaref{2,3}d.so, the reference's OWN generic kernels compiled in
+                 place behind a shim (present only where the reference checkout was available at
+                 build time; the built libraries travel with the repository snapshot).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+PDE_EULER, PDE_SWE, PDE_ACOUSTIC, PDE_ELASTIC = 0, 1, 2, 3
+# ADER-DG PNPM table by order (Toolkit/exahype/toolkit/solverController.py:17)
+PNPM = [1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015]
+
+
+class ExoCfg(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("nvar", ctypes.c_int), ("npar", ctypes.c_int),
+                ("pde", ctypes.c_int), ("use_ncp", ctypes.c_int), ("cfl", ctypes.c_double),
+                ("pnpm", ctypes.c_double), ("max_picard", ctypes.c_int)]
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Oracle:
+    """The C restatement, one configuration (dim, order, PDE) per instance."""
+
+    def __init__(self, dim, order, pde=PDE_EULER, nvar=None, npar=0, cfl=0.9, max_picard=0):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so missing: run make -C oracle")
+        self.lib = ctypes.CDLL(path)
+        self.lib.exo_predictor.restype = ctypes.c_int
+        self.lib.exo_dt.restype = ctypes.c_double
+        if nvar is None:
+            nvar = {PDE_EULER: 5, PDE_SWE: 4}[pde]
+        self.cfg = ExoCfg(dim, order, nvar, npar, pde, 1 if pde == PDE_SWE else 0, cfl, PNPM[order], max_picard)
+        self.dim, self.n, self.v, self.D = dim, order + 1, nvar, nvar + npar
+        self.nd = self.n ** dim
+        self.nf = self.n ** (dim - 1)
+
+    def tables(self):
+        n = self.n
+        t = {k: np.zeros(n) for k in ("nodes", "weights", "F0", "F1")}
+        for k in ("Kxi", "iK1", "dudx"):
+            t[k] = np.zeros((n, n))
+        self.lib.exo_tables(n - 1, _p(t["nodes"]), _p(t["weights"]), _p(t["Kxi"]), _p(t["iK1"]), _p(t["dudx"]),
+                            _p(t["F0"]), _p(t["F1"]))
+        return t
+
+    def _dx(self, dx):
+        d = np.zeros(3)
+        d[: self.dim] = dx[: self.dim] if np.ndim(dx) else dx
+        return d
+
+    def predictor(self, luh, dx, dt, centre=None, t=0.0):
+        n, nd, D, v, dim = self.n, self.nd, self.D, self.v, self.dim
+        out = dict(lQi=np.zeros(nd * n * D), lFi=np.zeros(n * nd * (dim + 1) * v), lQhi=np.zeros(nd * D),
+                   lFhi=np.zeros((dim + 1) * nd * v), lQhbnd=np.zeros(2 * dim * self.nf * D),
+                   lFhbnd=np.zeros(2 * dim * self.nf * v))
+        sw = ctypes.c_int(0)
+        c = np.zeros(3) if centre is None else _f64(centre)
+        ret = self.lib.exo_predictor(ctypes.byref(self.cfg), _p(_f64(luh)), _p(c), _p(self._dx(dx)),
+                                     ctypes.c_double(t), ctypes.c_double(dt), _p(out["lQi"]), _p(out["lFi"]),
+                                     _p(out["lQhi"]), _p(out["lFhi"]), _p(out["lQhbnd"]), _p(out["lFhbnd"]),
+                                     ctypes.byref(sw))
+        out["ret"] = ret
+        out["sweeps"] = sw.value
+        return out
+
+    def volume(self, lFhi, dx):
+        lduh = np.zeros(self.nd * self.v)
+        self.lib.exo_volume(ctypes.byref(self.cfg), _p(lduh), _p(_f64(lFhi)), _p(self._dx(dx)))
+        return lduh
+
+    def riemann(self, FL, FR, QL, QR, dx, direction):
+        FL, FR = _f64(FL).copy(), _f64(FR).copy()
+        self.lib.exo_riemann(ctypes.byref(self.cfg), _p(FL), _p(FR), _p(_f64(QL)), _p(_f64(QR)), _p(self._dx(dx)),
+                             int(direction))
+        return FL, FR
+
+    def surface(self, lduh, lFhbnd, dx):
+        lduh = _f64(lduh).copy()
+        self.lib.exo_surface(ctypes.byref(self.cfg), _p(lduh), _p(_f64(lFhbnd)), _p(self._dx(dx)))
+        return lduh
+
+    def face(self, lduh, lFhbnd_face, direction, orientation, dx):
+        lduh = _f64(lduh).copy()
+        self.lib.exo_face(ctypes.byref(self.cfg), _p(lduh), _p(_f64(lFhbnd_face)), int(direction), int(orientation),
+                          _p(self._dx(dx)))
+        return lduh
+
+    def update(self, luh, lduh, dt):
+        out = _f64(luh).copy()
+        self.lib.exo_update(ctypes.byref(self.cfg), _p(out), _p(_f64(luh)), _p(_f64(lduh)), ctypes.c_double(dt))
+        return out
+
+    def dt(self, luh, dx):
+        return float(self.lib.exo_dt(ctypes.byref(self.cfg), _p(_f64(luh)), _p(self._dx(dx))))
+
+    def flux(self, Q):
+        F = np.zeros(self.dim * self.v)
+        self.lib.exo_flux(ctypes.byref(self.cfg), _p(_f64(Q)), _p(F))
+        return F.reshape(self.dim, self.v)
+
+    def run(self, luh, ncell, size, nsteps, offset=(0.0, 0.0, 0.0), walls=False, t0=0.0, fixed_dt=0.0,
+            nthreads=0, want_picard=False):
+        """Advance a uniform patch in place; returns (t, dts, picard sweeps per step and cell)."""
+        luh = np.ascontiguousarray(luh, dtype=np.float64)
+        nc = int(np.prod(ncell))
+        dts = np.zeros(nsteps)
+        pic = np.zeros(nsteps * nc, dtype=np.int32) if want_picard else None
+        t = ctypes.c_double(0.0)
+        nce = np.array(list(ncell) + [1] * (3 - len(ncell)), dtype=np.int32)
+        self.lib.exo_run(ctypes.byref(self.cfg), _p(nce), _p(self._dx(np.array(offset, dtype=float))),
+                         _p(self._dx(np.array(size, dtype=float))), int(walls), _p(luh), int(nsteps),
+                         ctypes.c_double(t0), ctypes.c_double(fixed_dt), ctypes.byref(t), _p(dts),
+                         _p(pic) if pic is not None else None, int(nthreads))
+        return t.value, dts, (pic.reshape(nsteps, nc) if pic is not None else None)
+
+
+class RefKernels:
+    """The reference's own generic kernels (oracle/_ref), one instantiation per instance."""
+
+    def __init__(self, dim, order, pde="euler", npar=0):
+        path = os.path.join(HERE, "_ref", "libexaref%dd.so" % dim)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.prefix = "exaref%dd_%s_o%d_p%d" % (dim, pde, order, npar)
+        if not hasattr(self.lib, self.prefix + "_predictor"):
+            raise AttributeError("instantiation %s not built" % self.prefix)
+        self.dim, self.n = dim, order + 1
+        self.v = {"euler": 5, "swe": 4}[pde]
+        self.D = self.v + npar
+        self.nd, self.nf = self.n ** dim, self.n ** (dim - 1)
+        getattr(self.lib, self.prefix + "_predictor").restype = ctypes.c_int
+        getattr(self.lib, self.prefix + "_dt").restype = ctypes.c_double
+
+    def _f(self, name):
+        return getattr(self.lib, self.prefix + "_" + name)
+
+    def _dx(self, dx):
+        d = np.zeros(3)
+        d[: self.dim] = dx[: self.dim] if np.ndim(dx) else dx
+        return d
+
+    def predictor(self, luh, dx, dt, centre=None, t=0.0):
+        n, nd, D, v, dim = self.n, self.nd, self.D, self.v, self.dim
+        out = dict(lQi=np.zeros(nd * n * D), rhs=np.zeros(nd * n * D), lFi=np.zeros(n * nd * (dim + 1) * v),
+                   gradQ=np.zeros(dim * v * nd), lQhi=np.zeros(nd * D), lFhi=np.zeros((dim + 1) * nd * v),
+                   lQhbnd=np.zeros(2 * dim * self.nf * D), lFhbnd=np.zeros(2 * dim * self.nf * v))
+        c = np.zeros(3) if centre is None else _f64(centre)
+        out["ret"] = self._f("predictor")(_p(_f64(luh)), _p(c), _p(self._dx(dx)), ctypes.c_double(t),
+                                          ctypes.c_double(dt), _p(out["lQi"]), _p(out["rhs"]), _p(out["lFi"]),
+                                          _p(out["gradQ"]), _p(out["lQhi"]), _p(out["lFhi"]), _p(out["lQhbnd"]),
+                                          _p(out["lFhbnd"]))
+        return out
+
+    def volume(self, lFhi, dx):
+        lduh = np.zeros(self.nd * self.v)
+        self._f("volume")(_p(lduh), _p(_f64(lFhi)), _p(self._dx(dx)))
+        return lduh
+
+    def riemann(self, FL, FR, QL, QR, dx, direction):
+        FL, FR = _f64(FL).copy(), _f64(FR).copy()
+        self._f("riemann")(_p(FL), _p(FR), _p(_f64(QL)), _p(_f64(QR)), ctypes.c_double(0.0), ctypes.c_double(0.0),
+                           _p(self._dx(dx)), int(direction))
+        return FL, FR
+
+    def surface(self, lduh, lFhbnd, dx):
+        lduh = _f64(lduh).copy()
+        self._f("surface")(_p(lduh), _p(_f64(lFhbnd)), _p(self._dx(dx)))
+        return lduh
+
+    def face(self, lduh, lFhbnd_face, direction, orientation, dx):
+        lduh = _f64(lduh).copy()
+        self._f("face")(_p(lduh), _p(_f64(lFhbnd_face)), int(direction), int(orientation), _p(self._dx(dx)))
+        return lduh
+
+    def update(self, luh, lduh, dt):
+        out = _f64(luh).copy()
+        self._f("update")(_p(out), _p(_f64(luh)), _p(_f64(lduh)), ctypes.c_double(dt))
+        return out
+
+    def dt(self, luh, dx):
+        return float(self._f("dt")(_p(_f64(luh)), _p(self._dx(dx))))
+
+    def run(self, luh, ncell, size, nsteps, offset=(0.0, 0.0, 0.0), walls=False, t0=0.0, fixed_dt=0.0,
+            nthreads=0, want_picard=False):
+        luh = np.ascontiguousarray(luh, dtype=np.float64)
+        nc = int(np.prod(ncell))
+        dts = np.zeros(nsteps)
+        pic = np.zeros(nsteps * nc, dtype=np.int32) if want_picard else None
+        t = ctypes.c_double(0.0)
+        nce = np.array(list(ncell) + [1] * (3 - len(ncell)), dtype=np.int32)
+        self._f("run")(_p(nce), _p(self._dx(np.array(offset, dtype=float))), _p(self._dx(np.array(size, dtype=float))),
+                       int(walls), _p(luh), int(nsteps), ctypes.c_double(t0), ctypes.c_double(fixed_dt),
+                       ctypes.byref(t), _p(dts), _p(pic) if pic is not None else None, int(nthreads))
+        return t.value, dts, (pic.reshape(nsteps, nc) if pic is not None else None)
