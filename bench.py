@@ -1,0 +1,313 @@
+"""Benchmark: ADER-DG DoF-updates/s on 3D compressible Euler, order N=5, 81^3 periodic cells.
+
+One "step" is one ADER-DG time step of the whole grid: CFL dt (fused into the previous step's
+update), fused space-time predictor + volume integral, Rusanov on every face, surface integral +
+solution update. Seeded synthetic entropy-wave state (BASELINE workload "3D Euler N=5 81^3"),
+inputs resident in HBM; 4.6 GB of luh per step, far above the 126 MB L2, so no L2 flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0). With --gpus N > 1 (torchrun) every rank advances its own
+81^3 grid (weak scaling, no data-path collective; timing is the max over ranks).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "exahype-engine_b200"))
+
+NCELL = (81, 81, 81)
+ORDER = 5
+NVAR = 5
+METRIC = "ADER-DG DoF-updates/s (3D Euler N=5, 81^3 cells)"
+# CPU baseline sample: a 27^3 periodic block of the same state (same dx, same dt scale)
+SAMPLE_NCELL = (27, 27, 27)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ncell", type=int, default=81, help="cells per axis (81 = the benchmark workload)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.stop = threading.Event()
+        self.t = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[0]) for s in self.samples if len(s) >= 6 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 6 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples if len(s) >= 6 for k in range(4) if s[2 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def flops_per_cell_step(sweeps):
+    """Algorithmic FLOPs of one cell-step of the reference algorithm (3D Euler, N=5):
+    395,280 per Picard sweep (contractions 2(d+1) n^(d+2) v + n^(d+1) (flux 40 + 5v)),
+    116,640 for time averaging, extrapolation and volume integral, 31,000 for faces, update, CFL."""
+    return 395280.0 * sweeps + 116640.0 + 31000.0
+
+
+PRED_BYTES_PER_CELL = 8.0 * (1080 + 1080 + 1080 + 1080)  # luh in; lduh, lQhbnd, lFhbnd out
+
+
+def cpu_baseline(steps=2, kind="reference"):
+    """The reference's own generic kernels (oracle/_ref) with OpenMP on every host core, on a
+    27^3 periodic block of the benchmark state. Returns DoF-updates/s."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import exa_scenarios as sc
+    from pyoracle import Oracle, RefKernels
+    luh, _ = sc.euler_entropy_wave(SAMPLE_NCELL, ORDER, seed=0)
+    size = [SAMPLE_NCELL[k] / NCELL[k] for k in range(3)]
+    try:
+        runner = RefKernels(3, ORDER)
+    except Exception:
+        runner, kind = Oracle(3, ORDER), "port"
+    cores = os.cpu_count()
+    runner.run(luh, SAMPLE_NCELL, size, 1, nthreads=cores)  # warm-up
+    t0 = time.perf_counter()
+    runner.run(luh, SAMPLE_NCELL, size, steps, nthreads=cores)
+    el = time.perf_counter() - t0
+    cells = int(np.prod(SAMPLE_NCELL))
+    dof = cells * NVAR * (ORDER + 1) ** 3 * steps
+    return {"value": dof / el, "unit": "DoF-updates/s", "cores": cores, "kind": kind,
+            "sample": "%dx%dx%d periodic block of the 81^3 N=5 Euler state (dx=1/81), %d steps, %.1f s"
+                      % (SAMPLE_NCELL + (steps, el))}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    W, K = args.warmup, args.steps
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import exa_scenarios as sc
+    from pyoracle import Oracle, RefKernels
+    kind = "reference"
+    try:
+        runner = RefKernels(3, ORDER)
+    except Exception:
+        runner, kind = Oracle(3, ORDER), "port"
+    luh, _ = sc.euler_entropy_wave(SAMPLE_NCELL, ORDER, seed=0)
+    size = [SAMPLE_NCELL[k] / NCELL[k] for k in range(3)]
+    cores = os.cpu_count()
+    runner.run(luh, SAMPLE_NCELL, size, W, nthreads=cores)
+    t0 = time.perf_counter()
+    runner.run(luh, SAMPLE_NCELL, size, K, nthreads=cores)
+    el = time.perf_counter() - t0
+    cells = int(np.prod(SAMPLE_NCELL))
+    value = cells * NVAR * (ORDER + 1) ** 3 * K / el
+    sample = "%dx%dx%d periodic block of the 81^3 N=5 Euler state (dx=1/81) per step" % SAMPLE_NCELL
+    line = {"metric": METRIC, "value": value, "unit": "DoF-updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": K, "warmup": W, "ms_per_step": 1e3 * el / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D Euler N=5 entropy wave, generic kernels, OpenMP over cells",
+                       "sample": sample, "cells_per_step": cells},
+            "cpu_baseline": {"value": value, "unit": "DoF-updates/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "DoF-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    import exa_aderdg as exa
+    import exa_scenarios as sc
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    W, K = args.warmup, args.steps
+    ncell = (args.ncell,) * 3
+    cells = int(np.prod(ncell))
+    dof_step = cells * NVAR * (ORDER + 1) ** 3
+
+    solver = exa.Solver(exa.PDE_EULER, 3, ORDER)
+    patch = exa.Patch(solver, [dict(ncell=ncell, size=[1.0, 1.0, 1.0])])
+    luh0, wave = sc.euler_entropy_wave(ncell, ORDER, seed=0)
+    patch.set_solution(luh0)
+    stream = torch.cuda.ExternalStream(patch.stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- device-resident steps (graph per step), CUDA events on the patch's stream ----
+    patch.step(W)
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        barrier()
+        ev0.record(stream)
+        patch.step(K)
+        ev1.record(stream)
+        ev1.synchronize()
+        barrier()
+    ms = ev0.elapsed_time(ev1) / K
+    ms_t = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    stats = patch.stats()
+    status = patch.status()
+    t_now, dt_now = patch.time()
+
+    # ---- dominant kernel (predictor) timed alone, events on the same stream ----
+    import ctypes
+    lib = exa.load_library()
+    nd, nf = (ORDER + 1) ** 3, (ORDER + 1) ** 2
+    luh_dev = torch.empty(cells * nd * NVAR, dtype=torch.float64, device="cuda")
+    patch.get_solution(luh_dev)
+    lduh = torch.empty(cells * nd * NVAR, dtype=torch.float64, device="cuda")
+    qhb = torch.empty(cells * 6 * nf * NVAR, dtype=torch.float64, device="cuda")
+    fhb = torch.empty_like(qhb)
+    pic = torch.zeros(cells, dtype=torch.int32, device="cuda")
+    dxv = [1.0 / ncell[0]] * 3
+    dtv = float(dt_now[0])
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            solver.fused_predictor_volume_integral(luh_dev, lduh, qhb, fhb, dxv, dtv, picard=pic, stream=patch.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record(stream)
+        for _ in range(reps):
+            solver.fused_predictor_volume_integral(luh_dev, lduh, qhb, fhb, dxv, dtv, picard=pic, stream=patch.stream)
+        e1.record(stream)
+    e1.synchronize()
+    pred_ms = e0.elapsed_time(e1) / reps
+    mean_sweeps = float(pic.double().mean().item())
+    # FP64 tensor-pipe peak measured here with cuBLAS DGEMM (MEASURED_PEAKS.json carries no FP64 figure)
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(3):
+        torch.matmul(a, b)
+    g1.record()
+    g1.synchronize()
+    fp64_peak = 3 * 2 * 8192.0 ** 3 / (g0.elapsed_time(g1) * 1e-3) / 1e12
+    del a, b
+    flops_launch = cells * (395280.0 * mean_sweeps + 116640.0)
+    achieved = flops_launch / (pred_ms * 1e-3) / 1e12
+
+    # ---- end to end through the C ABI with host buffers: H2D state, step, D2H state ----
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(luh0).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        nbytes = host_in.numel() * 8
+        def e2e_step():
+            patch.set_solution(host_in.numpy())  # H2D + CFL dt of the uploaded state
+            patch.step(1)
+            patch.get_solution(host_out.numpy())  # D2H of the result
+        e2e_step()
+        barrier()
+        t0 = time.perf_counter()
+        ke = max(2, min(K, 5))
+        for _ in range(ke):
+            e2e_step()
+        barrier()
+        e2e_ms = (time.perf_counter() - t0) * 1e3 / ke
+        e2e_t = torch.tensor([e2e_ms], device="cuda")
+        if world > 1:
+            dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(e2e_t.item())
+        e2e = {"value": world * dof_step / (e2e_ms * 1e-3), "unit": "DoF-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "ms_per_step": e2e_ms}
+
+    pk, pk_kind = peaks()
+    line = {
+        "metric": METRIC, "value": world * dof_step / (ms * 1e-3), "unit": "DoF-updates/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3D Euler N=5 (6^3 nodes, nVar=5) entropy wave, %d^3 periodic cells, CFL 0.9, "
+                               "FP64 Picard predictor + Rusanov + update, one CUDA graph per step" % ncell[0],
+                   "cells": cells, "dof_per_step": dof_step, "l2": "inputs 4.6 GB > L2, no flush needed",
+                   "precision": "fp64"},
+        "cell_updates_per_s": world * cells / (ms * 1e-3),
+        "picard_sweeps_mean": stats["picard_mean"], "status_bits": status,
+        "roofline": {"bound": "tensor", "kernel": "predictor_kernel (fused Picard + volume integral)",
+                     "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                     "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
+                     "traffic": None, "algorithmic_flops_per_launch": flops_launch, "launch_ms": pred_ms,
+                     "hbm_gbs_of_launch": cells * PRED_BYTES_PER_CELL / (pred_ms * 1e-3) / 1e9,
+                     "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},
+        "gpu_launches": K * 4,
+        "clocks": clocks.summary(),
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if rank == 0 and not args.no_cpu:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as ex:  # the baseline must not sink the GPU line
+            line["cpu_baseline"] = {"value": None, "error": str(ex)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    patch.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,831 @@
+// Host runtime and C ABI of the B200 ADER-DG cell update (include/exa_aderdg.h).
+//
+// One shared library, libexa_aderdg.so, compiled for sm_100a. The PDE functors, dimensions and
+// orders are template instantiations registered in make_ops(); the C ABI dispatches to them
+// through the Ops interface. Everything device-side lives in exa_kernels.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/exa_aderdg.h"
+#include "exa_kernels.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  return EXA_ERR_CUDA;
+}
+#define EXA_CUDA(call)                                      \
+  do {                                                      \
+    cudaError_t e_ = (call);                                \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);     \
+  } while (0)
+
+// ADER-DG PNPM table by order (Toolkit/exahype/toolkit/solverController.py:17-23)
+double default_pnpm(int order) {
+  static const double t[10] = {1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015};
+  if (order < 10) return t[order];
+  static const double c[6] = {0.18525, 0.1204125, 0.078268125, 0.05087428125, 0.0330682828125, 0.021494383828125};
+  if (order < 16) return c[order - 10] / (2 * order + 1);
+  return 0.0;
+}
+
+}  // namespace
+
+namespace exa {
+
+// One instantiation (PDE, DIM, N, P): launchers of every kernel.
+struct Ops {
+  int dim, order, nvar, npar, nd, nf, cpb;
+  size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
+  bool ncp;
+  virtual ~Ops() {}
+  virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st) = 0;
+  virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
+  virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
+  virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
+};
+
+template <class PDE, int DIM, int N, int P>
+struct OpsImpl final : Ops {
+  using S = Shape<PDE, DIM, N, P>;
+  bool smem_set = false;
+  OpsImpl() {
+    dim = DIM;
+    order = N;
+    nvar = S::V;
+    npar = P;
+    nd = S::nd;
+    nf = S::nf;
+    cpb = S::CPB;
+    ncp = PDE::kNCP;
+    sz_luh = (size_t)S::nd * S::D;
+    sz_lduh = (size_t)S::nd * S::V;
+    sz_qhb = S::sizeQhb;
+    sz_fhb = S::sizeFhb;
+    sz_lQi = (size_t)S::nd * S::n * S::D;
+    sz_lFi = (size_t)S::n * S::nd * (DIM + 1) * S::V;
+    sz_lQhi = (size_t)S::nd * S::D;
+    sz_lFhi = (size_t)(DIM + 1) * S::nd * S::V;
+  }
+  cudaError_t predictor(const CellArgs& a, cudaStream_t st) override {
+    if (a.ncells <= 0) return cudaSuccess;
+    if (!smem_set) {
+      cudaError_t e = cudaFuncSetAttribute(predictor_kernel<PDE, DIM, N, P>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::predictor_smem);
+      if (e != cudaSuccess) return e;
+      smem_set = true;
+    }
+    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
+    predictor_kernel<PDE, DIM, N, P><<<blocks, S::TPB, S::predictor_smem, st>>>(a);
+    return cudaGetLastError();
+  }
+  cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
+    if (a.ncells <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
+    if (surface && upd)
+      update_kernel<PDE, DIM, N, P, true, true><<<blocks, S::TPB, 0, st>>>(a);
+    else if (upd)
+      update_kernel<PDE, DIM, N, P, false, true><<<blocks, S::TPB, 0, st>>>(a);
+    else
+      update_kernel<PDE, DIM, N, P, false, false><<<blocks, S::TPB, 0, st>>>(a);
+    return cudaGetLastError();
+  }
+  cudaError_t riemann(const FaceArgs& f, cudaStream_t st) override {
+    if (f.nfaces <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((f.nfaces + 7) / 8);
+    riemann_kernel<PDE, DIM, N, P><<<blocks, 256, 0, st>>>(f);
+    return cudaGetLastError();
+  }
+  cudaError_t boundary(const FaceArgs& f, cudaStream_t st) override {
+    if (f.nfaces <= 0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((f.nfaces + 7) / 8);
+    boundary_kernel<PDE, DIM, N, P><<<blocks, 256, 0, st>>>(f);
+    return cudaGetLastError();
+  }
+};
+
+// The instantiations this library carries.
+std::unique_ptr<Ops> make_ops(int pde, int dim, int order, int npar) {
+#define EXA_CASE(PDEID, PDET, D_, N_, P_) \
+  if (pde == PDEID && dim == D_ && order == N_ && npar == P_) return std::unique_ptr<Ops>(new OpsImpl<PDET, D_, N_, P_>());
+  EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 5, 0)
+  EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 3, 0)
+  EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 3, 1)
+  EXA_CASE(EXA_PDE_EULER, EulerPDE, 2, 3, 0)
+  EXA_CASE(EXA_PDE_EULER, EulerPDE, 2, 3, 1)
+  EXA_CASE(EXA_PDE_SWE, SWEPDE, 2, 4, 0)
+#undef EXA_CASE
+  return nullptr;
+}
+
+}  // namespace exa
+
+// ------------------------------------------------------------------------------------------
+// solver handle
+// ------------------------------------------------------------------------------------------
+struct exa_solver {
+  exa_solver_config cfg;
+  std::unique_ptr<exa::Ops> ops;
+  double cfl = 0.9, pnpm = 0.0;
+  unsigned* d_status = nullptr;
+  std::mutex mu;
+  // scratch of the per-cell shims (grown on demand)
+  double* d_scratch = nullptr;
+  size_t scratch_doubles = 0;
+  int* d_iscratch = nullptr;
+};
+
+static exa::CellArgs base_args(exa_solver* s, int ncells) {
+  exa::CellArgs a;
+  memset(&a, 0, sizeof(a));
+  a.ncells = ncells;
+  a.status = s->d_status;
+  a.max_picard = s->cfg.max_picard;
+  a.cfl_pnpm = s->cfl * s->pnpm;
+  return a;
+}
+
+extern "C" {
+
+const char* exa_last_error(void) { return g_err.c_str(); }
+const char* exa_version(void) { return "exa_aderdg 0.1 (sm_100a)"; }
+
+int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
+  if (!cfg || !out) return fail(EXA_ERR_INVALID, "null argument");
+  *out = nullptr;
+  if (cfg->dim != 2 && cfg->dim != 3) return fail(EXA_ERR_INVALID, "dim must be 2 or 3");
+  if (cfg->order < 1 || cfg->order > 9) return fail(EXA_ERR_INVALID, "order must be in 1..9");
+  if (cfg->npar < 0) return fail(EXA_ERR_INVALID, "npar must be >= 0");
+  if (cfg->max_picard < 0) return fail(EXA_ERR_INVALID, "max_picard must be >= 0");
+  if (cfg->precision != EXA_PREC_FP64 && cfg->precision != EXA_PREC_MIXED)
+    return fail(EXA_ERR_INVALID, "unknown precision");
+  auto ops = exa::make_ops(cfg->pde, cfg->dim, cfg->order, cfg->npar);
+  if (!ops || cfg->precision != EXA_PREC_FP64)
+    return fail(EXA_ERR_UNSUPPORTED, "no kernel instantiation for pde=" + std::to_string(cfg->pde) +
+                                         " dim=" + std::to_string(cfg->dim) + " order=" +
+                                         std::to_string(cfg->order) + " npar=" + std::to_string(cfg->npar) +
+                                         " precision=" + std::to_string(cfg->precision));
+  std::unique_ptr<exa_solver> s(new exa_solver());
+  s->cfg = *cfg;
+  s->ops = std::move(ops);
+  s->cfl = cfg->cfl > 0 ? cfg->cfl : 0.9;
+  s->pnpm = cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order);
+  EXA_CUDA(cudaMalloc(&s->d_status, sizeof(unsigned)));
+  EXA_CUDA(cudaMemset(s->d_status, 0, sizeof(unsigned)));
+  *out = s.release();
+  return EXA_OK;
+}
+
+int exa_solver_destroy(exa_solver* s) {
+  if (!s) return EXA_OK;
+  cudaFree(s->d_status);
+  cudaFree(s->d_scratch);
+  cudaFree(s->d_iscratch);
+  delete s;
+  return EXA_OK;
+}
+
+int exa_solver_sizes(const exa_solver* s, exa_sizes* o) {
+  if (!s || !o) return fail(EXA_ERR_INVALID, "null argument");
+  const exa::Ops& p = *s->ops;
+  o->nvar = p.nvar;
+  o->ndata = p.nvar + p.npar;
+  o->nodes_per_cell = p.nd;
+  o->nodes_per_face = p.nf;
+  o->luh = p.sz_luh;
+  o->lduh = p.sz_lduh;
+  o->lQhbnd = p.sz_qhb;
+  o->lFhbnd = p.sz_fhb;
+  o->lQi = p.sz_lQi;
+  o->lFi = p.sz_lFi;
+  o->lQhi = p.sz_lQhi;
+  o->lFhi = p.sz_lFhi;
+  return EXA_OK;
+}
+
+int exa_solver_status(exa_solver* s, unsigned* bits) {
+  if (!s || !bits) return fail(EXA_ERR_INVALID, "null argument");
+  EXA_CUDA(cudaDeviceSynchronize());
+  EXA_CUDA(cudaMemcpy(bits, s->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  EXA_CUDA(cudaMemset(s->d_status, 0, sizeof(unsigned)));
+  return EXA_OK;
+}
+
+// ---- batched kernels ---------------------------------------------------------------------
+static void set_uniform(exa::CellArgs& a, const exa_solver* s, const double* dx, double dt) {
+  for (int d = 0; d < 3; d++) a.u_dx[d] = d < s->cfg.dim ? dx[d] : 1.0;
+  a.u_dt = dt;
+}
+
+int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double* luh, double* lduh, double* lQhbnd,
+                                        double* lFhbnd, int* picard_sweeps, const double* dx, double t, double dt,
+                                        void* stream) {
+  (void)t;
+  if (!s || ncells < 0 || (ncells > 0 && (!luh || !lduh || !lQhbnd || !lFhbnd || !dx)))
+    return fail(EXA_ERR_INVALID, "null argument");
+  exa::CellArgs a = base_args(s, ncells);
+  a.luh = luh;
+  a.lduh = lduh;
+  a.lQhbnd = lQhbnd;
+  a.lFhbnd = lFhbnd;
+  a.picard = picard_sweeps;
+  set_uniform(a, s, dx, dt);
+  EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream));
+  return EXA_OK;
+}
+
+static int check_faces(int nfaces) { return nfaces < 0 ? fail(EXA_ERR_INVALID, "nfaces < 0") : EXA_OK; }
+
+int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, const int* right, const signed char* dir,
+                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+  if (!s) return fail(EXA_ERR_INVALID, "null solver");
+  if (int e = check_faces(nfaces)) return e;
+  if (nfaces > 0 && (!left || !right || !dir || !lQhbnd || !lFhbnd)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::FaceArgs f;
+  memset(&f, 0, sizeof(f));
+  f.nfaces = nfaces;
+  f.left = left;
+  f.right = right;
+  f.dir = reinterpret_cast<const int8_t*>(dir);
+  f.lQhbnd = lQhbnd;
+  f.lFhbnd = lFhbnd;
+  EXA_CUDA(s->ops->riemann(f, (cudaStream_t)stream));
+  return EXA_OK;
+}
+
+int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, const signed char* face,
+                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+  if (!s) return fail(EXA_ERR_INVALID, "null solver");
+  if (int e = check_faces(nfaces)) return e;
+  if (nfaces > 0 && (!cell || !face || !lQhbnd || !lFhbnd)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::FaceArgs f;
+  memset(&f, 0, sizeof(f));
+  f.nfaces = nfaces;
+  f.bcell = cell;
+  f.bface = reinterpret_cast<const int8_t*>(face);
+  f.lQhbnd = lQhbnd;
+  f.lFhbnd = lFhbnd;
+  EXA_CUDA(s->ops->boundary(f, (cudaStream_t)stream));
+  return EXA_OK;
+}
+
+int exa_surface_integral_and_update(exa_solver* s, int ncells, double* luh, const double* lduh, const double* lFhbnd,
+                                    const double* dx, double dt, void* stream) {
+  if (!s || ncells < 0 || (ncells > 0 && (!luh || !lduh || !lFhbnd || !dx)))
+    return fail(EXA_ERR_INVALID, "null argument");
+  exa::CellArgs a = base_args(s, ncells);
+  a.luh = luh;
+  a.luh_out = luh;
+  a.lduh = const_cast<double*>(lduh);
+  a.lFhbnd = const_cast<double*>(lFhbnd);
+  set_uniform(a, s, dx, dt);
+  EXA_CUDA(s->ops->update(a, true, true, (cudaStream_t)stream));
+  return EXA_OK;
+}
+
+int exa_solution_update(exa_solver* s, int ncells, double* luh, const double* luhOld, const double* lduh, double dt,
+                        void* stream) {
+  if (!s || ncells < 0 || (ncells > 0 && (!luh || !luhOld || !lduh))) return fail(EXA_ERR_INVALID, "null argument");
+  exa::CellArgs a = base_args(s, ncells);
+  a.luh = luhOld;
+  a.luh_out = luh;
+  a.lduh = const_cast<double*>(lduh);
+  double one[3] = {1.0, 1.0, 1.0};
+  set_uniform(a, s, one, dt);
+  EXA_CUDA(s->ops->update(a, false, true, (cudaStream_t)stream));
+  return EXA_OK;
+}
+
+int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
+                              double* dt_min, void* stream) {
+  if (!s || ncells < 0 || (ncells > 0 && (!luh || !dx))) return fail(EXA_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  cudaStream_t st = (cudaStream_t)stream;
+  exa::CellArgs a = base_args(s, ncells);
+  a.luh = luh;
+  a.cell_dt = cell_dt;
+  set_uniform(a, s, dx, 0.0);
+  if (dt_min) {
+    if (!s->d_scratch) {
+      EXA_CUDA(cudaMalloc(&s->d_scratch, 1024 * sizeof(double)));
+      s->scratch_doubles = 1024;
+    }
+    exa::fill_kernel<<<1, 32, 0, st>>>(1, s->d_scratch, INFINITY);
+    a.grid_dt_next = s->d_scratch;
+  }
+  EXA_CUDA(s->ops->update(a, false, false, st));
+  if (dt_min) {
+    EXA_CUDA(cudaMemcpyAsync(dt_min, s->d_scratch, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EXA_CUDA(cudaStreamSynchronize(st));
+  }
+  return EXA_OK;
+}
+
+// ---- per-cell shims on host pointers ---------------------------------------------------------
+static int shim_scratch(exa_solver* s, size_t doubles) {
+  if (s->scratch_doubles >= doubles && s->d_scratch) return EXA_OK;
+  cudaFree(s->d_scratch);
+  s->d_scratch = nullptr;
+  s->scratch_doubles = 0;
+  EXA_CUDA(cudaMalloc(&s->d_scratch, doubles * sizeof(double)));
+  s->scratch_doubles = doubles;
+  if (!s->d_iscratch) EXA_CUDA(cudaMalloc(&s->d_iscratch, 64 * sizeof(int)));
+  return EXA_OK;
+}
+
+int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbnd, double* lQi, double* lFi,
+                                    double* lQhi, double* lFhi, const double* luh, const double* cellCenter,
+                                    const double* invDx, double t, double dt) {
+  (void)cellCenter;
+  (void)t;
+  if (!s || !lQhbnd || !lFhbnd || !luh || !invDx) {
+    fail(EXA_ERR_INVALID, "null argument");
+    return -1;
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  const exa::Ops& o = *s->ops;
+  const size_t total = o.sz_luh + o.sz_lduh + o.sz_qhb + o.sz_fhb + o.sz_lQi + o.sz_lFi + o.sz_lQhi + o.sz_lFhi;
+  if (shim_scratch(s, total)) return -1;
+  double* d = s->d_scratch;
+  double *d_luh = d, *d_lduh = d_luh + o.sz_luh, *d_qhb = d_lduh + o.sz_lduh, *d_fhb = d_qhb + o.sz_qhb;
+  double *d_lQi = d_fhb + o.sz_fhb, *d_lFi = d_lQi + o.sz_lQi, *d_lQhi = d_lFi + o.sz_lFi, *d_lFhi = d_lQhi + o.sz_lQhi;
+  if (cudaMemcpy(d_luh, luh, o.sz_luh * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+  exa::CellArgs a = base_args(s, 1);
+  a.luh = d_luh;
+  a.lduh = d_lduh;
+  a.lQhbnd = d_qhb;
+  a.lFhbnd = d_fhb;
+  a.picard = s->d_iscratch;
+  a.ex_lQi = d_lQi;
+  a.ex_lFi = d_lFi;
+  a.ex_lQhi = d_lQhi;
+  a.ex_lFhi = d_lFhi;
+  double dx[3] = {1.0, 1.0, 1.0};
+  for (int k = 0; k < s->cfg.dim; k++) dx[k] = 1.0 / invDx[k];
+  set_uniform(a, s, dx, dt);
+  cudaError_t e = s->ops->predictor(a, 0);
+  if (e != cudaSuccess) {
+    cuda_fail(e, "predictor");
+    return -1;
+  }
+  int sweeps = 0;
+  if (cudaMemcpy(&sweeps, s->d_iscratch, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  cudaMemcpy(lQhbnd, d_qhb, o.sz_qhb * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaMemcpy(lFhbnd, d_fhb, o.sz_fhb * sizeof(double), cudaMemcpyDeviceToHost);
+  if (lQi) cudaMemcpy(lQi, d_lQi, o.sz_lQi * sizeof(double), cudaMemcpyDeviceToHost);
+  if (lFi) cudaMemcpy(lFi, d_lFi, o.sz_lFi * sizeof(double), cudaMemcpyDeviceToHost);
+  if (lQhi) cudaMemcpy(lQhi, d_lQhi, o.sz_lQhi * sizeof(double), cudaMemcpyDeviceToHost);
+  if (lFhi) cudaMemcpy(lFhi, d_lFhi, o.sz_lFhi * sizeof(double), cudaMemcpyDeviceToHost);
+  if (cudaDeviceSynchronize() != cudaSuccess) return -1;
+  // the reference's return value (3d/...:408-412 breaks at the converging index; 2d/...:303-305
+  // reports MaxIterations+2 on convergence)
+  const int maxIter = s->cfg.max_picard > 0 ? s->cfg.max_picard : 2 * (s->cfg.order + 1);
+  const bool converged = s->cfg.max_picard <= 0 && sweeps < maxIter ? true : false;
+  if (s->cfg.max_picard > 0) return maxIter;
+  if (s->cfg.dim == 2) return converged ? maxIter + 2 : maxIter;
+  return converged ? sweeps - 1 : maxIter;
+}
+
+int exa_volumeIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhi, const double* dx) {
+  (void)s; (void)lduh; (void)lFhi; (void)dx;
+  return fail(EXA_ERR_UNSUPPORTED, "volumeIntegralNonlinear is fused into exa_fused_predictor_volume_integral");
+}
+
+int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const double* QL, const double* QR, double t,
+                               double dt, const double* dx, int direction) {
+  (void)t; (void)dt; (void)dx;
+  if (!s || !FL || !FR || !QL || !QR) return fail(EXA_ERR_INVALID, "null argument");
+  if (direction < 0 || direction >= s->cfg.dim) return fail(EXA_ERR_INVALID, "direction out of range");
+  std::lock_guard<std::mutex> lk(s->mu);
+  const exa::Ops& o = *s->ops;
+  // two one-cell blocks: cell 0 holds QL/FL on face 2d+1, cell 1 holds QR/FR on face 2d
+  const size_t total = 2 * (o.sz_qhb + o.sz_fhb);
+  if (int e = shim_scratch(s, total)) return e;
+  double* qhb = s->d_scratch;
+  double* fhb = qhb + 2 * o.sz_qhb;
+  const size_t fq = o.sz_qhb / (2 * o.dim), ff = o.sz_fhb / (2 * o.dim);
+  EXA_CUDA(cudaMemcpy(qhb + (2 * direction + 1) * fq, QL, fq * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(qhb + o.sz_qhb + (2 * direction) * fq, QR, fq * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(fhb + (2 * direction + 1) * ff, FL, ff * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(fhb + o.sz_fhb + (2 * direction) * ff, FR, ff * sizeof(double), cudaMemcpyHostToDevice));
+  int* idx = s->d_iscratch;
+  int h[3] = {0, 1, 0};
+  int8_t dd = (int8_t)direction;
+  EXA_CUDA(cudaMemcpy(idx, h, 2 * sizeof(int), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(idx + 2, &dd, 1, cudaMemcpyHostToDevice));
+  exa::FaceArgs f;
+  memset(&f, 0, sizeof(f));
+  f.nfaces = 1;
+  f.left = idx;
+  f.right = idx + 1;
+  f.dir = reinterpret_cast<const int8_t*>(idx + 2);
+  f.lQhbnd = qhb;
+  f.lFhbnd = fhb;
+  EXA_CUDA(s->ops->riemann(f, 0));
+  EXA_CUDA(cudaMemcpy(FL, fhb + (2 * direction + 1) * ff, ff * sizeof(double), cudaMemcpyDeviceToHost));
+  EXA_CUDA(cudaMemcpy(FR, fhb + o.sz_fhb + (2 * direction) * ff, ff * sizeof(double), cudaMemcpyDeviceToHost));
+  return EXA_OK;
+}
+
+int exa_surfaceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, const double* dx) {
+  (void)s; (void)lduh; (void)lFhbnd; (void)dx;
+  return fail(EXA_ERR_UNSUPPORTED, "surfaceIntegralNonlinear is fused into exa_surface_integral_and_update");
+}
+
+int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const double* lduh, double dt) {
+  if (!s || !luh || !luhOld || !lduh) return fail(EXA_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  const exa::Ops& o = *s->ops;
+  if (int e = shim_scratch(s, 2 * o.sz_luh + o.sz_lduh)) return e;
+  double* d_old = s->d_scratch;
+  double* d_new = d_old + o.sz_luh;
+  double* d_du = d_new + o.sz_luh;
+  EXA_CUDA(cudaMemcpy(d_old, luhOld, o.sz_luh * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(d_new, luhOld, o.sz_luh * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(d_du, lduh, o.sz_lduh * sizeof(double), cudaMemcpyHostToDevice));
+  exa::CellArgs a = base_args(s, 1);
+  a.luh = d_old;
+  a.luh_out = d_new;
+  a.lduh = d_du;
+  double one[3] = {1.0, 1.0, 1.0};
+  set_uniform(a, s, one, dt);
+  EXA_CUDA(s->ops->update(a, false, true, 0));
+  // parameters are not touched by solutionUpdate: keep the caller's luh entries for them
+  std::vector<double> tmp(o.sz_luh);
+  EXA_CUDA(cudaMemcpy(tmp.data(), d_new, o.sz_luh * sizeof(double), cudaMemcpyDeviceToHost));
+  const int D = o.nvar + o.npar;
+  for (int p = 0; p < o.nd; p++)
+    for (int m = 0; m < o.nvar; m++) luh[p * D + m] = tmp[p * D + m];
+  return EXA_OK;
+}
+
+int exa_stableTimeStepSize(exa_solver* s, const double* luh, const double* dx, double* dt) {
+  if (!s || !luh || !dx || !dt) return fail(EXA_ERR_INVALID, "null argument");
+  double* d_luh = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (int e = shim_scratch(s, s->ops->sz_luh + 8)) return e;
+    d_luh = s->d_scratch + 8;
+    EXA_CUDA(cudaMemcpy(d_luh, luh, s->ops->sz_luh * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  double* cell = nullptr;
+  EXA_CUDA(cudaMalloc(&cell, sizeof(double)));
+  int r = exa_stable_time_step_size(s, 1, d_luh, dx, cell, nullptr, 0);
+  if (r == EXA_OK) {
+    cudaError_t e = cudaMemcpy(dt, cell, sizeof(double), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) r = cuda_fail(e, "copy dt");
+  }
+  cudaFree(cell);
+  return r;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// device-resident patches
+// ------------------------------------------------------------------------------------------
+struct exa_patch {
+  exa_solver* s = nullptr;
+  std::vector<exa_grid_desc> grids;
+  long long ncells = 0;
+  std::vector<long long> grid_first;
+  double *luh = nullptr, *lduh = nullptr, *lQhbnd = nullptr, *lFhbnd = nullptr;
+  int* picard = nullptr;
+  int* cell_grid = nullptr;
+  double *grid_dx = nullptr, *grid_t = nullptr, *grid_dt = nullptr, *grid_dt_next = nullptr;
+  long long* steps = nullptr;
+  int *fL = nullptr, *fR = nullptr;
+  int8_t* fdir = nullptr;
+  int nfaces = 0;
+  int* bcell = nullptr;
+  int8_t* bface = nullptr;
+  int nbfaces = 0;
+  unsigned* status = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph_cfl = nullptr, graph_fixed = nullptr;
+  bool track_picard = false;
+  double fixed_dt = -1.0;
+};
+
+static void patch_free(exa_patch* p) {
+  if (p->graph_cfl) cudaGraphExecDestroy(p->graph_cfl);
+  if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
+  void* ptrs[] = {p->luh, p->lduh, p->lQhbnd, p->lFhbnd, p->picard, p->cell_grid, p->grid_dx, p->grid_t,
+                  p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  if (p->stream) cudaStreamDestroy(p->stream);
+}
+
+static exa::CellArgs patch_args(exa_patch* p) {
+  exa::CellArgs a = base_args(p->s, (int)p->ncells);
+  a.status = p->status;
+  a.luh = p->luh;
+  a.luh_out = p->luh;
+  a.lduh = p->lduh;
+  a.lQhbnd = p->lQhbnd;
+  a.lFhbnd = p->lFhbnd;
+  a.picard = p->picard;
+  a.cell_grid = p->grids.size() > 1 ? p->cell_grid : nullptr;
+  a.grid_dx = p->grid_dx;
+  a.grid_dt = p->grid_dt;
+  return a;
+}
+
+static exa::FaceArgs patch_faces(exa_patch* p) {
+  exa::FaceArgs f;
+  memset(&f, 0, sizeof(f));
+  f.nfaces = p->nfaces;
+  f.left = p->fL;
+  f.right = p->fR;
+  f.dir = p->fdir;
+  f.lQhbnd = p->lQhbnd;
+  f.lFhbnd = p->lFhbnd;
+  f.bcell = p->bcell;
+  f.bface = p->bface;
+  return f;
+}
+
+// enqueue one step on p->stream (used for capture)
+static int patch_enqueue_step(exa_patch* p, bool cfl) {
+  exa::CellArgs a = patch_args(p);
+  EXA_CUDA(p->s->ops->predictor(a, p->stream));
+  exa::FaceArgs f = patch_faces(p);
+  EXA_CUDA(p->s->ops->riemann(f, p->stream));
+  if (p->nbfaces > 0) {
+    exa::FaceArgs b = f;
+    b.nfaces = p->nbfaces;
+    EXA_CUDA(p->s->ops->boundary(b, p->stream));
+  }
+  exa::CellArgs u = patch_args(p);
+  if (cfl) u.grid_dt_next = p->grid_dt_next;
+  EXA_CUDA(p->s->ops->update(u, true, true, p->stream));
+  const int ng = (int)p->grids.size();
+  if (cfl) {
+    exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, p->grid_dt_next, p->steps);
+  } else {
+    // fixed dt: t += dt, dt unchanged
+    exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, p->grid_dt, p->steps);
+  }
+  EXA_CUDA(cudaGetLastError());
+  return EXA_OK;
+}
+
+static int patch_graph(exa_patch* p, bool cfl, cudaGraphExec_t* out) {
+  if (*out) return EXA_OK;
+  cudaGraph_t g = nullptr;
+  EXA_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  int r = patch_enqueue_step(p, cfl);
+  cudaError_t e = cudaStreamEndCapture(p->stream, &g);
+  if (r != EXA_OK) {
+    if (g) cudaGraphDestroy(g);
+    return r;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+  return EXA_OK;
+}
+
+extern "C" {
+
+int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_patch** out) {
+  if (!s || !grids || !out || ngrids <= 0) return fail(EXA_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  const int dim = s->cfg.dim;
+  std::unique_ptr<exa_patch> p(new exa_patch());
+  p->s = s;
+  p->grids.assign(grids, grids + ngrids);
+  std::vector<int> hcell_grid;
+  std::vector<int> fL, fR, bc;
+  std::vector<int8_t> fd, bf;
+  std::vector<double> hdx(3 * ngrids);
+  long long c0 = 0;
+  for (int g = 0; g < ngrids; g++) {
+    const exa_grid_desc& G = grids[g];
+    int nc[3] = {G.ncell[0], G.ncell[1], dim == 3 ? G.ncell[2] : 1};
+    for (int d = 0; d < dim; d++) {
+      if (nc[d] <= 0 || !(G.size[d] > 0)) return fail(EXA_ERR_INVALID, "grid extents must be positive");
+      if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL) return fail(EXA_ERR_INVALID, "unknown boundary");
+      hdx[3 * g + d] = G.size[d] / nc[d];
+    }
+    for (int d = dim; d < 3; d++) hdx[3 * g + d] = 1.0;
+    const long long n = (long long)nc[0] * nc[1] * nc[2];
+    p->grid_first.push_back(c0);
+    auto idx = [&](int x, int y, int z) { return c0 + ((long long)z * nc[1] + y) * nc[0] + x; };
+    for (int d = 0; d < dim; d++)
+      for (int z = 0; z < nc[2]; z++)
+        for (int y = 0; y < nc[1]; y++)
+          for (int x = 0; x < nc[0]; x++) {
+            int j[3] = {x, y, z};
+            const int i_d = j[d];
+            j[d] += 1;
+            if (j[d] == nc[d]) {
+              if (G.bc[d] == EXA_BC_PERIODIC) {
+                j[d] = 0;
+              } else {
+                bc.push_back((int)idx(x, y, z));
+                bf.push_back((int8_t)(2 * d + 1));
+              }
+            }
+            if (j[d] < nc[d]) {
+              fL.push_back((int)idx(x, y, z));
+              fR.push_back((int)idx(j[0], j[1], j[2]));
+              fd.push_back((int8_t)d);
+            }
+            if (i_d == 0 && G.bc[d] == EXA_BC_WALL) {
+              bc.push_back((int)idx(x, y, z));
+              bf.push_back((int8_t)(2 * d));
+            }
+          }
+    if (ngrids > 1) hcell_grid.insert(hcell_grid.end(), (size_t)n, g);
+    c0 += n;
+  }
+  if (c0 > 0x7fffffffLL) return fail(EXA_ERR_INVALID, "too many cells for 32-bit face indices");
+  p->ncells = c0;
+  p->nfaces = (int)fL.size();
+  p->nbfaces = (int)bc.size();
+  const exa::Ops& o = *s->ops;
+  const long long nc = p->ncells;
+  auto alloc = [&](void** ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 8);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+    return EXA_OK;
+  };
+  int r = EXA_OK;
+#define EXA_ALLOC(ptr, bytes)                          \
+  if ((r = alloc((void**)&(ptr), (bytes))) != EXA_OK) { \
+    patch_free(p.get());                               \
+    return r;                                          \
+  }
+  EXA_ALLOC(p->luh, nc * o.sz_luh * sizeof(double));
+  EXA_ALLOC(p->lduh, nc * o.sz_lduh * sizeof(double));
+  EXA_ALLOC(p->lQhbnd, nc * o.sz_qhb * sizeof(double));
+  EXA_ALLOC(p->lFhbnd, nc * o.sz_fhb * sizeof(double));
+  EXA_ALLOC(p->picard, nc * sizeof(int));
+  EXA_ALLOC(p->grid_dx, 3 * ngrids * sizeof(double));
+  EXA_ALLOC(p->grid_t, ngrids * sizeof(double));
+  EXA_ALLOC(p->grid_dt, ngrids * sizeof(double));
+  EXA_ALLOC(p->grid_dt_next, ngrids * sizeof(double));
+  EXA_ALLOC(p->steps, sizeof(long long));
+  EXA_ALLOC(p->status, sizeof(unsigned));
+  EXA_ALLOC(p->fL, fL.size() * sizeof(int));
+  EXA_ALLOC(p->fR, fR.size() * sizeof(int));
+  EXA_ALLOC(p->fdir, fd.size());
+  EXA_ALLOC(p->bcell, bc.size() * sizeof(int));
+  EXA_ALLOC(p->bface, bf.size());
+  if (ngrids > 1) EXA_ALLOC(p->cell_grid, hcell_grid.size() * sizeof(int));
+#undef EXA_ALLOC
+  cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    patch_free(p.get());
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  std::vector<double> zeros(ngrids, 0.0);
+  bool ok = cudaMemcpy(p->grid_dx, hdx.data(), hdx.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(p->grid_t, zeros.data(), ngrids * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(p->grid_dt, zeros.data(), ngrids * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemset(p->steps, 0, sizeof(long long)) == cudaSuccess &&
+            cudaMemset(p->status, 0, sizeof(unsigned)) == cudaSuccess &&
+            cudaMemset(p->luh, 0, nc * o.sz_luh * sizeof(double)) == cudaSuccess &&
+            cudaMemset(p->picard, 0, nc * sizeof(int)) == cudaSuccess &&
+            (fL.empty() || (cudaMemcpy(p->fL, fL.data(), fL.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+                            cudaMemcpy(p->fR, fR.data(), fR.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+                            cudaMemcpy(p->fdir, fd.data(), fd.size(), cudaMemcpyHostToDevice) == cudaSuccess)) &&
+            (bc.empty() || (cudaMemcpy(p->bcell, bc.data(), bc.size() * sizeof(int), cudaMemcpyHostToDevice) == cudaSuccess &&
+                            cudaMemcpy(p->bface, bf.data(), bf.size(), cudaMemcpyHostToDevice) == cudaSuccess)) &&
+            (ngrids == 1 || cudaMemcpy(p->cell_grid, hcell_grid.data(), hcell_grid.size() * sizeof(int),
+                                       cudaMemcpyHostToDevice) == cudaSuccess);
+  if (!ok) {
+    patch_free(p.get());
+    return cuda_fail(cudaGetLastError(), "patch upload");
+  }
+  *out = p.release();
+  return EXA_OK;
+}
+
+int exa_patch_destroy(exa_patch* p) {
+  if (!p) return EXA_OK;
+  cudaStreamSynchronize(p->stream);
+  patch_free(p);
+  delete p;
+  return EXA_OK;
+}
+
+long long exa_patch_num_cells(const exa_patch* p) { return p ? p->ncells : -1; }
+double* exa_patch_luh(exa_patch* p) { return p ? p->luh : nullptr; }
+void* exa_patch_stream(exa_patch* p) { return p ? (void*)p->stream : nullptr; }
+
+static int patch_initial_dt(exa_patch* p) {
+  const int ng = (int)p->grids.size();
+  exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, INFINITY);
+  exa::CellArgs a = patch_args(p);
+  a.grid_dt_next = p->grid_dt;
+  EXA_CUDA(p->s->ops->update(a, false, false, p->stream));
+  exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt_next, INFINITY);
+  EXA_CUDA(cudaGetLastError());
+  return EXA_OK;
+}
+
+int exa_patch_set_solution(exa_patch* p, const double* luh, int on_device) {
+  if (!p || !luh) return fail(EXA_ERR_INVALID, "null argument");
+  const size_t bytes = (size_t)p->ncells * p->s->ops->sz_luh * sizeof(double);
+  EXA_CUDA(cudaMemcpyAsync(p->luh, luh, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           p->stream));
+  int r = patch_initial_dt(p);
+  if (r) return r;
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_get_solution(exa_patch* p, double* luh, int on_device) {
+  if (!p || !luh) return fail(EXA_ERR_INVALID, "null argument");
+  const size_t bytes = (size_t)p->ncells * p->s->ops->sz_luh * sizeof(double);
+  EXA_CUDA(cudaMemcpyAsync(luh, p->luh, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           p->stream));
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_step(exa_patch* p, int nsteps, double fixed_dt) {
+  if (!p || nsteps < 0) return fail(EXA_ERR_INVALID, "bad argument");
+  const bool cfl = !(fixed_dt > 0);
+  if (!cfl && fixed_dt != p->fixed_dt) {
+    const int ng = (int)p->grids.size();
+    exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, fixed_dt);
+    EXA_CUDA(cudaGetLastError());
+    p->fixed_dt = fixed_dt;
+  }
+  if (cfl && p->fixed_dt > 0) {
+    // back from fixed steps: recompute the CFL dt of the current state
+    if (int r = patch_initial_dt(p)) return r;
+    p->fixed_dt = -1.0;
+  }
+  cudaGraphExec_t* g = cfl ? &p->graph_cfl : &p->graph_fixed;
+  if (int r = patch_graph(p, cfl, g)) return r;
+  for (int i = 0; i < nsteps; i++) EXA_CUDA(cudaGraphLaunch(*g, p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_sync(exa_patch* p) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_time(exa_patch* p, double* t, double* dt) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  const size_t ng = p->grids.size();
+  if (t) EXA_CUDA(cudaMemcpyAsync(t, p->grid_t, ng * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  if (dt) EXA_CUDA(cudaMemcpyAsync(dt, p->grid_dt, ng * sizeof(double), cudaMemcpyDeviceToHost, p->stream));
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_track_picard(exa_patch* p, int on) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  p->track_picard = on != 0;
+  return EXA_OK;
+}
+
+int exa_patch_stats_get(exa_patch* p, exa_patch_stats* st) {
+  if (!p || !st) return fail(EXA_ERR_INVALID, "null argument");
+  memset(st, 0, sizeof(*st));
+  EXA_CUDA(cudaMemcpyAsync(&st->steps, p->steps, sizeof(long long), cudaMemcpyDeviceToHost, p->stream));
+  std::vector<int> pic((size_t)p->ncells);
+  EXA_CUDA(cudaMemcpyAsync(pic.data(), p->picard, pic.size() * sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  double sum = 0;
+  for (int v : pic) {
+    sum += v;
+    st->picard_hist[std::min(std::max(v, 0), 31)]++;
+  }
+  st->picard_mean = pic.empty() ? 0.0 : sum / pic.size();
+  return EXA_OK;
+}
+
+int exa_patch_status(exa_patch* p, unsigned* bits) {
+  if (!p || !bits) return fail(EXA_ERR_INVALID, "null argument");
+  EXA_CUDA(cudaMemcpyAsync(bits, p->status, sizeof(unsigned), cudaMemcpyDeviceToHost, p->stream));
+  EXA_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned), p->stream));
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,333 @@
+"""Python binding of libexa_aderdg.so (include/exa_aderdg.h) over ctypes.
+
+This mirrors the reference's generic-kernel interface for the tests and the benchmark:
+``Solver`` plays the generated ``Abstract<App>Solver_ADERDG`` glue (fusedSpaceTimePredictor-
+VolumeIntegral, riemannSolver, boundaryConditions, faceIntegral + addUpdateToSolution,
+stableTimeStepSize; AbstractGenericADERDGSolverImplementation.template:104-361) on batches of
+device-resident cells, and exposes the per-cell shims with the exact generic-kernel semantics.
+``Patch`` is a device-resident set of uniform grids stepped by one CUDA graph per step.
+
+Device arrays are torch CUDA tensors (float64, contiguous); torch is used only for device
+memory and streams. There is no CPU fallback: constructing a Solver without the built library
+or without a CUDA device raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libexa_aderdg.so")
+
+EXA_OK = 0
+PDE_EULER, PDE_SWE = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+BC_PERIODIC, BC_WALL = 0, 1
+ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT = 1, 2, 4, 8
+NVAR = {PDE_EULER: 5, PDE_SWE: 4}
+
+
+class ExaError(RuntimeError):
+    pass
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("npar", ctypes.c_int), ("pde", ctypes.c_int),
+                ("cfl", ctypes.c_double), ("pnpm", ctypes.c_double), ("max_picard", ctypes.c_int),
+                ("precision", ctypes.c_int)]
+
+
+class _Sizes(ctypes.Structure):
+    _fields_ = [("nvar", ctypes.c_int), ("ndata", ctypes.c_int), ("nodes_per_cell", ctypes.c_int),
+                ("nodes_per_face", ctypes.c_int), ("luh", ctypes.c_size_t), ("lduh", ctypes.c_size_t),
+                ("lQhbnd", ctypes.c_size_t), ("lFhbnd", ctypes.c_size_t), ("lQi", ctypes.c_size_t),
+                ("lFi", ctypes.c_size_t), ("lQhi", ctypes.c_size_t), ("lFhi", ctypes.c_size_t)]
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("ncell", ctypes.c_int * 3), ("offset", ctypes.c_double * 3), ("size", ctypes.c_double * 3),
+                ("bc", ctypes.c_int * 3)]
+
+
+class _PatchStats(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_longlong), ("picard_mean", ctypes.c_double), ("picard_hist", ctypes.c_int * 32)]
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Load libexa_aderdg.so (fails loudly when it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise ExaError("%s is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'`" % path)
+    lib = ctypes.CDLL(path)
+    lib.exa_last_error.restype = ctypes.c_char_p
+    lib.exa_version.restype = ctypes.c_char_p
+    vp, i, d, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)
+    sigs = {
+        "exa_solver_create": [ctypes.POINTER(_Config), ctypes.POINTER(vp)],
+        "exa_solver_destroy": [vp],
+        "exa_solver_sizes": [vp, ctypes.POINTER(_Sizes)],
+        "exa_solver_status": [vp, ctypes.POINTER(ctypes.c_uint)],
+        "exa_fused_predictor_volume_integral": [vp, i, vp, vp, vp, vp, vp, dp, d, d, vp],
+        "exa_riemann_solver_nonlinear": [vp, i, vp, vp, vp, vp, vp, vp],
+        "exa_boundary_conditions_wall": [vp, i, vp, vp, vp, vp, vp],
+        "exa_surface_integral_and_update": [vp, i, vp, vp, vp, dp, d, vp],
+        "exa_solution_update": [vp, i, vp, vp, vp, d, vp],
+        "exa_stable_time_step_size": [vp, i, vp, dp, vp, dp, vp],
+        "exa_spaceTimePredictorNonlinear": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, d, d],
+        "exa_riemannSolverNonlinear": [vp, vp, vp, vp, vp, d, d, dp, i],
+        "exa_solutionUpdate": [vp, vp, vp, vp, d],
+        "exa_stableTimeStepSize": [vp, vp, dp, dp],
+        "exa_patch_create": [vp, i, ctypes.POINTER(GridDesc), ctypes.POINTER(vp)],
+        "exa_patch_destroy": [vp],
+        "exa_patch_set_solution": [vp, vp, i],
+        "exa_patch_get_solution": [vp, vp, i],
+        "exa_patch_step": [vp, i, d],
+        "exa_patch_sync": [vp],
+        "exa_patch_time": [vp, dp, dp],
+        "exa_patch_stats_get": [vp, ctypes.POINTER(_PatchStats)],
+        "exa_patch_status": [vp, ctypes.POINTER(ctypes.c_uint)],
+    }
+    for name, args in sigs.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    lib.exa_patch_num_cells.argtypes = [vp]
+    lib.exa_patch_num_cells.restype = ctypes.c_longlong
+    lib.exa_patch_luh.argtypes = [vp]
+    lib.exa_patch_luh.restype = ctypes.c_void_p
+    lib.exa_patch_stream.argtypes = [vp]
+    lib.exa_patch_stream.restype = ctypes.c_void_p
+    _lib = lib
+    return lib
+
+
+def _check(rc, what):
+    if rc != EXA_OK:
+        raise ExaError("%s failed (%d): %s" % (what, rc, _lib.exa_last_error().decode()))
+
+
+def _ptr(t):
+    """Device pointer of a contiguous torch CUDA tensor (or None)."""
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ExaError("expected a contiguous CUDA tensor")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _dx3(dx, dim):
+    a = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    v = np.broadcast_to(np.asarray(dx, dtype=float), (dim,))
+    for k in range(dim):
+        a[k] = float(v[k])
+    return a
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(stream)
+
+
+class Solver:
+    """One (PDE, dim, order, nPar, precision) instantiation of the cell update."""
+
+    def __init__(self, pde=PDE_EULER, dim=3, order=5, npar=0, cfl=0.9, pnpm=0.0, max_picard=0, precision=PREC_FP64):
+        self.lib = load_library()
+        cfg = _Config(dim, order, npar, pde, cfl, pnpm, max_picard, precision)
+        h = ctypes.c_void_p()
+        _check(self.lib.exa_solver_create(ctypes.byref(cfg), ctypes.byref(h)), "exa_solver_create")
+        self.h = h
+        self.dim, self.order, self.npar, self.pde = dim, order, npar, pde
+        sz = _Sizes()
+        _check(self.lib.exa_solver_sizes(self.h, ctypes.byref(sz)), "exa_solver_sizes")
+        self.sizes = {k: getattr(sz, k) for k, _ in _Sizes._fields_}
+        self.nvar, self.ndata = sz.nvar, sz.ndata
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.exa_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def status(self):
+        bits = ctypes.c_uint(0)
+        _check(self.lib.exa_solver_status(self.h, ctypes.byref(bits)), "exa_solver_status")
+        return bits.value
+
+    # ---- batched, device tensors -------------------------------------------------------
+    def fused_predictor_volume_integral(self, luh, lduh, lQhbnd, lFhbnd, dx, dt, t=0.0, picard=None, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_fused_predictor_volume_integral(
+            self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(picard), _dx3(dx, self.dim),
+            float(t), float(dt), _stream(stream)), "exa_fused_predictor_volume_integral")
+
+    def riemann(self, left, right, direction, lQhbnd, lFhbnd, stream=None):
+        _check(self.lib.exa_riemann_solver_nonlinear(self.h, left.numel(), _ptr(left), _ptr(right), _ptr(direction),
+                                                     _ptr(lQhbnd), _ptr(lFhbnd), _stream(stream)),
+               "exa_riemann_solver_nonlinear")
+
+    def boundary_wall(self, cell, face, lQhbnd, lFhbnd, stream=None):
+        _check(self.lib.exa_boundary_conditions_wall(self.h, cell.numel(), _ptr(cell), _ptr(face), _ptr(lQhbnd),
+                                                     _ptr(lFhbnd), _stream(stream)), "exa_boundary_conditions_wall")
+
+    def surface_integral_and_update(self, luh, lduh, lFhbnd, dx, dt, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_surface_integral_and_update(self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lFhbnd),
+                                                        _dx3(dx, self.dim), float(dt), _stream(stream)),
+               "exa_surface_integral_and_update")
+
+    def solution_update(self, luh, luh_old, lduh, dt, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_solution_update(self.h, ncells, _ptr(luh), _ptr(luh_old), _ptr(lduh), float(dt),
+                                            _stream(stream)), "exa_solution_update")
+
+    def stable_time_step_size(self, luh, dx, cell_dt=None, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        out = ctypes.c_double(0.0)
+        _check(self.lib.exa_stable_time_step_size(self.h, ncells, _ptr(luh), _dx3(dx, self.dim), _ptr(cell_dt),
+                                                  ctypes.byref(out), _stream(stream)), "exa_stable_time_step_size")
+        return out.value
+
+    # ---- per-cell shims, numpy host arrays ------------------------------------------------
+    def space_time_predictor(self, luh, dx, dt, centre=None, t=0.0):
+        s = self.sizes
+        out = {k: np.zeros(s[k]) for k in ("lQhbnd", "lFhbnd", "lQi", "lFi", "lQhi", "lFhi")}
+        inv = (ctypes.c_double * 3)(*(1.0 / np.broadcast_to(np.asarray(dx, float), (self.dim,))).tolist(),
+                                    *([1.0] * (3 - self.dim)))
+        c = np.zeros(3) if centre is None else np.ascontiguousarray(centre, dtype=float)
+        luh = np.ascontiguousarray(luh, dtype=float)
+        ret = self.lib.exa_spaceTimePredictorNonlinear(self.h, _np_ptr(out["lQhbnd"]), _np_ptr(out["lFhbnd"]),
+                                                       _np_ptr(out["lQi"]), _np_ptr(out["lFi"]), _np_ptr(out["lQhi"]),
+                                                       _np_ptr(out["lFhi"]), _np_ptr(luh), _np_ptr(c), inv, float(t),
+                                                       float(dt))
+        if ret < 0:
+            raise ExaError("exa_spaceTimePredictorNonlinear: " + self.lib.exa_last_error().decode())
+        out["ret"] = ret
+        return out
+
+    def riemann_cell(self, FL, FR, QL, QR, dx, direction):
+        FL = np.ascontiguousarray(FL, dtype=float).copy()
+        FR = np.ascontiguousarray(FR, dtype=float).copy()
+        _check(self.lib.exa_riemannSolverNonlinear(self.h, _np_ptr(FL), _np_ptr(FR),
+                                                   _np_ptr(np.ascontiguousarray(QL, dtype=float)),
+                                                   _np_ptr(np.ascontiguousarray(QR, dtype=float)), 0.0, 0.0,
+                                                   _dx3(dx, self.dim), int(direction)), "exa_riemannSolverNonlinear")
+        return FL, FR
+
+    def solution_update_cell(self, luh, lduh, dt):
+        out = np.ascontiguousarray(luh, dtype=float).copy()
+        _check(self.lib.exa_solutionUpdate(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(luh, dtype=float)),
+                                           _np_ptr(np.ascontiguousarray(lduh, dtype=float)), float(dt)),
+               "exa_solutionUpdate")
+        return out
+
+    def stable_time_step_size_cell(self, luh, dx):
+        out = ctypes.c_double(0.0)
+        _check(self.lib.exa_stableTimeStepSize(self.h, _np_ptr(np.ascontiguousarray(luh, dtype=float)),
+                                               _dx3(dx, self.dim), ctypes.byref(out)), "exa_stableTimeStepSize")
+        return out.value
+
+
+class Patch:
+    """Device-resident uniform grid(s); the step is one CUDA graph launch."""
+
+    def __init__(self, solver, grids):
+        """grids: list of dicts {ncell, size, offset=0, bc=periodic} (bc per axis)."""
+        self.solver = solver
+        self.lib = solver.lib
+        arr = (GridDesc * len(grids))()
+        for g, spec in zip(arr, grids):
+            nc = list(spec["ncell"]) + [1] * (3 - len(spec["ncell"]))
+            sz = list(spec["size"]) + [1.0] * (3 - len(spec["size"]))
+            off = list(spec.get("offset", [0.0] * 3)) + [0.0] * 3
+            bc = spec.get("bc", BC_PERIODIC)
+            bcs = list(bc) if hasattr(bc, "__len__") else [bc] * 3
+            bcs = bcs + [BC_PERIODIC] * (3 - len(bcs))
+            for k in range(3):
+                g.ncell[k] = int(nc[k])
+                g.size[k] = float(sz[k])
+                g.offset[k] = float(off[k])
+                g.bc[k] = int(bcs[k])
+        h = ctypes.c_void_p()
+        _check(self.lib.exa_patch_create(solver.h, len(grids), arr, ctypes.byref(h)), "exa_patch_create")
+        self.h = h
+        self.ngrids = len(grids)
+        self.ncells = int(self.lib.exa_patch_num_cells(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.exa_patch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def luh_ptr(self):
+        return self.lib.exa_patch_luh(self.h)
+
+    @property
+    def stream(self):
+        return self.lib.exa_patch_stream(self.h)
+
+    def set_solution(self, luh):
+        """luh: numpy host array (reference layout) or a CUDA tensor."""
+        if isinstance(luh, np.ndarray):
+            a = np.ascontiguousarray(luh, dtype=np.float64)
+            _check(self.lib.exa_patch_set_solution(self.h, _np_ptr(a), 0), "exa_patch_set_solution")
+        else:
+            _check(self.lib.exa_patch_set_solution(self.h, _ptr(luh), 1), "exa_patch_set_solution")
+
+    def get_solution(self, out=None):
+        if out is None:
+            out = np.zeros(self.ncells * self.solver.sizes["luh"])
+            _check(self.lib.exa_patch_get_solution(self.h, _np_ptr(out), 0), "exa_patch_get_solution")
+            return out
+        if isinstance(out, np.ndarray):
+            _check(self.lib.exa_patch_get_solution(self.h, _np_ptr(out), 0), "exa_patch_get_solution")
+        else:
+            _check(self.lib.exa_patch_get_solution(self.h, _ptr(out), 1), "exa_patch_get_solution")
+        return out
+
+    def step(self, nsteps=1, fixed_dt=0.0):
+        _check(self.lib.exa_patch_step(self.h, int(nsteps), float(fixed_dt)), "exa_patch_step")
+
+    def sync(self):
+        _check(self.lib.exa_patch_sync(self.h), "exa_patch_sync")
+
+    def time(self):
+        t = np.zeros(self.ngrids)
+        dt = np.zeros(self.ngrids)
+        _check(self.lib.exa_patch_time(self.h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                       dt.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "exa_patch_time")
+        return t, dt
+
+    def stats(self):
+        st = _PatchStats()
+        _check(self.lib.exa_patch_stats_get(self.h, ctypes.byref(st)), "exa_patch_stats_get")
+        return {"steps": st.steps, "picard_mean": st.picard_mean, "picard_hist": list(st.picard_hist)}
+
+    def status(self):
+        bits = ctypes.c_uint(0)
+        _check(self.lib.exa_patch_status(self.h, ctypes.byref(bits)), "exa_patch_status")
+        return bits.value

@@ -1,0 +1,122 @@
+"""Seeded synthetic initial states for the benchmark and parity workloads.
+
+The reference fills a cell by evaluating the user's ``adjustPointSolution`` at the
+Gauss-Legendre nodes, x = centre + dx * (node - 0.5) (ExaHyPE/kernels/aderdg/generic/c/3d/
+solutionAdjustment.cpph:38-58): nodal interpolation, not L2 projection. ``nodal_positions``
+restates that placement; the state functions below play the role of adjustPointSolution.
+
+Workloads (numpy.random.default_rng(seed), seed 0 unless stated):
+
+* ``euler2d_entropy_wave`` -- 2D Euler, rho = 1 + 0.2 * sum of 4 Fourier modes (integer k,
+  0 < |k| <= 3, random phases), u = v = 0.3, p = 1, periodic unit square.
+* ``euler3d_entropy_wave`` -- 3D Euler, rho = 1 + 0.1 * (1/8) * sum of 8 Fourier modes
+  (0 < |k| <= 4), u = (0.3, 0.2, 0.1), p = 1, periodic unit cube.
+
+Both are entropy waves: pressure and velocity are uniform, so the exact solution of the Euler
+equations is rho advected with u (``*_exact``), which gives an analytic L2 error next to the
+error against the FP64 oracle.
+"""
+import numpy as np
+
+GAMMA = 1.4
+
+
+def gl_nodes(order):
+    """Gauss-Legendre nodes on [0,1], ascending."""
+    x, _ = np.polynomial.legendre.leggauss(order + 1)
+    return 0.5 * (x + 1.0)
+
+
+def gl_weights(order):
+    _, w = np.polynomial.legendre.leggauss(order + 1)
+    return 0.5 * w
+
+
+def nodal_positions(ncell, size, order, offset=None):
+    """Node coordinates of every cell, shape [cells][nodes][dim], reference node order.
+
+    Cell c = (iz*ny + iy)*nx + ix; node p = (z*n + y)*n + x (2D: y*n + x).
+    """
+    dim = len(ncell)
+    offset = np.zeros(dim) if offset is None else np.asarray(offset, dtype=float)
+    dx = np.asarray(size, dtype=float) / np.asarray(ncell)
+    xi = gl_nodes(order)
+    n = order + 1
+    if dim == 3:
+        nx, ny, nz = ncell
+        iz, iy, ix = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+        kz, ky, kx = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+        cx = offset[0] + (ix.reshape(-1, 1) + xi[kx.reshape(1, -1)]) * dx[0]
+        cy = offset[1] + (iy.reshape(-1, 1) + xi[ky.reshape(1, -1)]) * dx[1]
+        cz = offset[2] + (iz.reshape(-1, 1) + xi[kz.reshape(1, -1)]) * dx[2]
+        return np.stack([cx, cy, cz], axis=-1)
+    nx, ny = ncell
+    iy, ix = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    ky, kx = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    cx = offset[0] + (ix.reshape(-1, 1) + xi[kx.reshape(1, -1)]) * dx[0]
+    cy = offset[1] + (iy.reshape(-1, 1) + xi[ky.reshape(1, -1)]) * dx[1]
+    return np.stack([cx, cy], axis=-1)
+
+
+def _modes(rng, nmodes, kmax, dim):
+    ks = []
+    while len(ks) < nmodes:
+        k = rng.integers(-kmax, kmax + 1, size=dim)
+        if 0 < np.linalg.norm(k) <= kmax:
+            ks.append(k)
+    phases = rng.uniform(0.0, 2.0 * np.pi, size=nmodes)
+    return np.array(ks, dtype=float), phases
+
+
+class EntropyWave:
+    """rho = 1 + amp * sum_m cos(2 pi k_m.(x - u t) + phi_m), uniform u and p."""
+
+    def __init__(self, dim, seed=0):
+        rng = np.random.default_rng(seed)
+        self.dim = dim
+        if dim == 2:
+            self.k, self.phi = _modes(rng, 4, 3, 2)
+            self.amp = 0.2
+            self.u = np.array([0.3, 0.3])
+        else:
+            self.k, self.phi = _modes(rng, 8, 4, 3)
+            self.amp = 0.1 / 8.0
+            self.u = np.array([0.3, 0.2, 0.1])
+        self.p = 1.0
+
+    def rho(self, x, t=0.0):
+        xs = x - self.u * t
+        arg = 2.0 * np.pi * np.tensordot(xs, self.k.T, axes=([-1], [0])) + self.phi
+        return 1.0 + self.amp * np.cos(arg).sum(-1)
+
+    def state(self, x, t=0.0):
+        """Conserved Euler state (rho, rho u, rho v, rho w, E) at points x[..., dim]; nVar = 5."""
+        rho = self.rho(x, t)
+        Q = np.zeros(x.shape[:-1] + (5,))
+        Q[..., 0] = rho
+        for d in range(self.dim):
+            Q[..., 1 + d] = rho * self.u[d]
+        Q[..., 4] = self.p / (GAMMA - 1.0) + 0.5 * rho * float(self.u @ self.u)
+        return Q
+
+
+def euler_entropy_wave(ncell, order, seed=0, t=0.0):
+    """Initial (or exact at time t) nodal state, shape [cells * nodes * 5], periodic unit box."""
+    dim = len(ncell)
+    wave = EntropyWave(dim, seed)
+    x = nodal_positions(ncell, [1.0] * dim, order)
+    return wave.state(x, t).reshape(-1), wave
+
+
+def l2_linf_error(luh, exact, order, dim, nvar_out=1, nvar=5):
+    """Quadrature-weighted L2 and max errors of the first ``nvar_out`` variables (unit box)."""
+    w = gl_weights(order)
+    if dim == 3:
+        wn = (w[:, None, None] * w[None, :, None] * w[None, None, :]).reshape(-1)
+    else:
+        wn = (w[:, None] * w[None, :]).reshape(-1)
+    a = np.asarray(luh).reshape(-1, wn.size, nvar)[..., :nvar_out]
+    b = np.asarray(exact).reshape(-1, wn.size, nvar)[..., :nvar_out]
+    ncells = a.shape[0]
+    e2 = ((a - b) ** 2 * wn[None, :, None]).sum() / ncells
+    return float(np.sqrt(e2)), float(np.max(np.abs(a - b)))

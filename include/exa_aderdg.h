@@ -1,0 +1,207 @@
+/* exa_aderdg.h -- C ABI of the B200 ADER-DG cell update (libexa_aderdg.so).
+ *
+ * Drop-in for ExaHyPE's generic nonlinear ADER-DG kernels (kernels::aderdg::generic::c, declared
+ * in ExaHyPE/kernels/aderdg/generic/Kernels.h:59-287) and for the generated solver glue that calls
+ * them (Toolkit/exahype/toolkit/templates/solvers/AbstractGenericADERDGSolverImplementation.template
+ * :104-361). Plain C types only: no torch, no C++ in the signatures.
+ *
+ * Data layouts are the reference's, per cell (row-major, last index fastest), n = Order+1,
+ * D = NumberOfVariables + NumberOfParameters, V = NumberOfVariables:
+ *   luh     [cell][z][y][x][D]        (2D: [cell][y][x][D])
+ *   lduh    [cell][z][y][x][V]
+ *   lQhbnd  [cell][2*DIM][a][b][D]    face 2*dir+orientation; (a,b) tangential, slower axis first
+ *   lFhbnd  [cell][2*DIM][a][b][V]
+ * Batched entry points take DEVICE pointers to arrays of `ncells` such blocks stored one after
+ * another, and a CUDA stream (cudaStream_t passed as void*; NULL = legacy default stream).
+ * They are asynchronous unless stated otherwise.
+ *
+ * Errors: every function returns an exa_status. Numerical trouble found on the device
+ * (non-finite values, Picard cap reached, dt <= 0) is accumulated in a device status word that
+ * exa_solver_status() / exa_patch_status() read and clear. The reference aborts or only logs
+ * in these cases (AbstractGenericADERDGSolverImplementation.template:98-102, 2d/
+ * spaceTimePredictorNonlinear.cpph:307-314); here they are reported, never trapped.
+ */
+#ifndef EXA_ADERDG_H
+#define EXA_ADERDG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  EXA_OK = 0,
+  EXA_ERR_INVALID = 1,     /* bad argument (null pointer, size, index) */
+  EXA_ERR_UNSUPPORTED = 2, /* (pde, dim, order, npar, precision) not instantiated in this build */
+  EXA_ERR_CUDA = 3,        /* a CUDA call failed; exa_last_error() has the message */
+  EXA_ERR_NUMERICS = 4,    /* device status word non-zero (see exa_status_bits) */
+  EXA_ERR_NOT_FOUND = 5
+} exa_status;
+
+/* bits of the device status word */
+typedef enum {
+  EXA_ST_NONFINITE_PREDICTOR = 1,
+  EXA_ST_PICARD_CAP = 2,      /* some cell used all 2(N+1) Picard sweeps without converging */
+  EXA_ST_NONFINITE_UPDATE = 4,
+  EXA_ST_BAD_DT = 8
+} exa_status_bits;
+
+/* PDE systems compiled as device functors (the user hooks flux / eigenvalues /
+ * nonConservativeProduct / boundaryValues of AbstractGenericADERDGSolverHeader.template:220-338). */
+typedef enum {
+  EXA_PDE_EULER = 0, /* compressible Euler, gamma 1.4, V=5 (Euler_ADERDG/EulerSolver_ADERDG.cpp:61-146) */
+  EXA_PDE_SWE = 1    /* shallow water h,hu,hv,b with NCP, V=4 (SWE_ADERDG/MySWESolver.cpp:103-152) */
+} exa_pde;
+
+typedef enum {
+  EXA_PREC_FP64 = 0,  /* every sweep in FP64 (generic-kernel semantics, parity 1e-12) */
+  EXA_PREC_MIXED = 1  /* early Picard sweeps in FP32, final sweep + residual test + update in FP64 */
+} exa_precision;
+
+typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1 } exa_bc;
+
+/* Compile-time constants of the reference's generated solver (AbstractGenericADERDGSolverHeader
+ * .template:34-68), here runtime fields of a solver handle. */
+typedef struct {
+  int dim;            /* 2 or 3 (DIMENSIONS) */
+  int order;          /* Order */
+  int npar;           /* NumberOfParameters */
+  exa_pde pde;
+  double cfl;         /* CFL safety factor; <= 0 selects 0.9 (the toolkit default) */
+  double pnpm;        /* PNPM; <= 0 selects the toolkit's table (solverController.py:17) */
+  int max_picard;     /* 0: residual test with 2(N+1) cap (UseMaxPicardIterations=false);
+                         > 0: exactly this many sweeps (UseMaxPicardIterations=true) */
+  exa_precision precision;
+} exa_solver_config;
+
+typedef struct exa_solver exa_solver;
+typedef struct exa_patch exa_patch;
+
+/* per-cell array sizes in doubles */
+typedef struct {
+  int nvar, ndata, nodes_per_cell, nodes_per_face;
+  size_t luh, lduh, lQhbnd, lFhbnd;
+  /* predictor internals in reference layout (exa_spaceTimePredictorNonlinear) */
+  size_t lQi, lFi, lQhi, lFhi;
+} exa_sizes;
+
+const char* exa_last_error(void);
+const char* exa_version(void);
+
+/* ---- solver handle -------------------------------------------------------------------- */
+int exa_solver_create(const exa_solver_config* cfg, exa_solver** out);
+int exa_solver_destroy(exa_solver* s);
+int exa_solver_sizes(const exa_solver* s, exa_sizes* out);
+/* reads and clears the device status word (synchronises the device) */
+int exa_solver_status(exa_solver* s, unsigned* bits);
+
+/* ---- batched kernels on caller-owned device memory ------------------------------------
+ * `dx` is the cell size (DIM doubles, host memory) shared by all `ncells` cells; `dt` a host
+ * scalar. */
+
+/* Replaces the glue's fusedSpaceTimePredictorVolumeIntegral (AbstractGenericADERDGSolver
+ * Implementation.template:104-235, nonlinear branch :168-211, addVolumeIntegralResultToUpdate=true):
+ * spaceTimePredictorNonlinear (3d/spaceTimePredictorNonlinear.cpph:816-864) followed by
+ * volumeIntegralNonlinear (3d/volumeIntegralNonlinear.cpph:29-223) for every cell.
+ * picard_sweeps (device, nullable): Picard sweeps executed per cell (the reference returns the
+ * loop index instead; exa_spaceTimePredictorNonlinear reproduces that return value). */
+int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double* luh, double* lduh,
+                                        double* lQhbnd, double* lFhbnd, int* picard_sweeps, const double* dx,
+                                        double t, double dt, void* stream);
+
+/* Replaces riemannSolverNonlinear<useNCP,false> (3d/riemannSolverNonlinear.cpph:37-128) for a
+ * list of interior faces: face f joins cell left[f] (its face 2*dir[f]+1) and cell right[f]
+ * (its face 2*dir[f]); FL/FR are the two cells' lFhbnd blocks, updated in place as in the
+ * reference (ADERDGSolver.cpp:1781-1785). left/right/dir are device arrays. */
+int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, const int* right,
+                                 const signed char* dir, const double* lQhbnd, double* lFhbnd, void* stream);
+
+/* Replaces boundaryConditions (3d/boundaryConditions.cpph:29-122) + the Riemann call of the
+ * glue's boundaryConditions (...Implementation.template:307-350) with a reflective wall
+ * (the SWE app's boundaryValues, MySWESolver.cpp:43-62) on faces face[f] of cells cell[f]. */
+int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, const signed char* face,
+                                 const double* lQhbnd, double* lFhbnd, void* stream);
+
+/* Replaces surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90) followed by
+ * solutionUpdate (3d/solutionUpdate.cpph:28-67): luh += dt/w * (lduh - surface terms). lduh is
+ * left unchanged. */
+int exa_surface_integral_and_update(exa_solver* s, int ncells, double* luh, const double* lduh,
+                                    const double* lFhbnd, const double* dx, double dt, void* stream);
+
+/* Replaces solutionUpdate alone (3d/solutionUpdate.cpph:28-67): luh = luhOld + dt/w * lduh
+ * (luh may alias luhOld). */
+int exa_solution_update(exa_solver* s, int ncells, double* luh, const double* luhOld, const double* lduh,
+                        double dt, void* stream);
+
+/* Replaces stableTimeStepSize (3d/stableTimeStepSize.cpph:14-62) and the min-reduction over
+ * cells (ADERDGSolver::updateAdmissibleTimeStepSize, ADERDGSolver.cpp:458-462). cell_dt
+ * (device, nullable) receives every cell's value; *dt_min (host, nullable) the minimum --
+ * requesting it synchronises the stream. */
+int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
+                              double* dt_min, void* stream);
+
+/* ---- per-cell compatibility shims: the exact generic-kernel signatures on HOST pointers ----
+ * One cell per call, synchronous; for conformance tests and glue that has not been batched yet. */
+
+/* spaceTimePredictorNonlinear<useSource=false,useFlux=true,useViscousFlux=false,useNCP,
+ * noTimeAveraging=false> (3d/spaceTimePredictorNonlinear.cpph:816-823): fills lQhbnd, lFhbnd and
+ * the internals lQi [z][y][x][t][D], lFi [t][z][y][x][DIM+1][V] (last sweep), lQhi, lFhi (reference
+ * blocks); any internal may be NULL. Returns the reference's value: 3D the index of the converging
+ * iteration, 2D MaxIterations+2 on convergence (2d/...:303-305); -1 on error. */
+int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbnd, double* lQi, double* lFi,
+                                    double* lQhi, double* lFhi, const double* luh, const double* cellCenter,
+                                    const double* invDx, double t, double dt);
+/* volumeIntegralNonlinear, time-averaged branch (3d/volumeIntegralNonlinear.cpph:133-223). */
+int exa_volumeIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhi, const double* dx);
+/* riemannSolverNonlinear (3d/riemannSolverNonlinear.cpph:37-128), in place on FL/FR. */
+int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const double* QL, const double* QR,
+                               double t, double dt, const double* dx, int direction);
+/* surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90). */
+int exa_surfaceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, const double* dx);
+/* solutionUpdate (3d/solutionUpdate.cpph:28-67). */
+int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const double* lduh, double dt);
+/* stableTimeStepSize (3d/stableTimeStepSize.cpph:14-62); returns the value in *dt. */
+int exa_stableTimeStepSize(exa_solver* s, const double* luh, const double* dx, double* dt);
+
+/* ---- device-resident patches: the per-step chain as one CUDA graph ------------------------
+ * A patch holds one or more uniform grids (all cells of all grids in one batch, cell-major, grid
+ * after grid; inside a grid c = (iz*ny + iy)*nx + ix). Each grid keeps its own t and CFL dt
+ * (global non-fused order of ADERDGSolver: dt = min CFL(luh) -> predictor + volume -> Riemann ->
+ * surface + update; ADERDGSolver.cpp:369-416, 887-947, 1190-1258). */
+typedef struct {
+  int ncell[3];       /* cells per axis (ncell[2] ignored in 2D) */
+  double offset[3];   /* lower corner */
+  double size[3];     /* edge lengths */
+  int bc[3];          /* per axis: EXA_BC_PERIODIC or EXA_BC_WALL (both sides) */
+} exa_grid_desc;
+
+typedef struct {
+  long long steps;          /* steps taken since creation */
+  double picard_mean;       /* mean Picard sweeps per cell over all steps (needs track_picard) */
+  int picard_hist[32];      /* sweeps histogram of the last step (needs track_picard) */
+} exa_patch_stats;
+
+int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_patch** out);
+int exa_patch_destroy(exa_patch* p);
+long long exa_patch_num_cells(const exa_patch* p);
+/* copy the reference-layout solution of all cells in (from host memory, or device memory
+ * when on_device != 0) and compute every grid's first CFL dt. */
+int exa_patch_set_solution(exa_patch* p, const double* luh, int on_device);
+int exa_patch_get_solution(exa_patch* p, double* luh, int on_device);
+/* device pointer of the patch's luh (ncells * luh doubles), valid until destroy */
+double* exa_patch_luh(exa_patch* p);
+/* advance every grid by nsteps steps; fixed_dt > 0 replaces the CFL dt. Asynchronous on the
+ * patch's stream (exa_patch_sync waits). One CUDA graph launch per step. */
+int exa_patch_step(exa_patch* p, int nsteps, double fixed_dt);
+int exa_patch_sync(exa_patch* p);
+int exa_patch_time(exa_patch* p, double* t, double* dt);   /* host arrays of ngrids (synchronises) */
+int exa_patch_track_picard(exa_patch* p, int on);
+int exa_patch_stats_get(exa_patch* p, exa_patch_stats* st);
+int exa_patch_status(exa_patch* p, unsigned* bits);       /* reads and clears (synchronises) */
+void* exa_patch_stream(exa_patch* p);                     /* the cudaStream_t the patch runs on */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* EXA_ADERDG_H */

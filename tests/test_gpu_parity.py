@@ -1,0 +1,286 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the CPU oracle and the reference's
+golden arrays. FP64 form: 1e-12 relative (max |gpu - oracle| / max |oracle|) unless stated.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+from pyoracle import Oracle, PDE_SWE
+
+GOLD = os.path.join(REPO, "tests", "golden")
+TOL = 1e-12
+EPS_REF = 1e-10
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(1e-300, np.max(np.abs(b))))
+
+
+def with_params(arr, nvar, npar):
+    a = np.asarray(arr).reshape(-1, nvar)
+    out = np.zeros((a.shape[0], nvar + npar))
+    out[:, :nvar] = a
+    return out.reshape(-1)
+
+
+def strip_params(arr, nvar, npar):
+    return np.asarray(arr).reshape(-1, nvar + npar)[:, :nvar].reshape(-1)
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch as t
+    return t
+
+
+@pytest.fixture(scope="module")
+def exa():
+    import exa_aderdg
+    return exa_aderdg
+
+
+def euler_cells(rng, ncells, nd, amp=0.1, dim=3):
+    rho = 1.0 + amp * rng.uniform(-1, 1, (ncells, nd))
+    u = 0.3 * rng.uniform(-1, 1, (ncells, nd, 3))
+    if dim == 2:
+        u[..., 2] = 0
+    p = 1.0 + amp * rng.uniform(-1, 1, (ncells, nd))
+    Q = np.zeros((ncells, nd, 5))
+    Q[..., 0] = rho
+    Q[..., 1:4] = rho[..., None] * u
+    Q[..., 4] = p / 0.4 + 0.5 * rho * (u ** 2).sum(-1)
+    return Q
+
+
+# ------------------------------------------------------------------------------------------
+# known-answer arrays of the reference (GenericEulerKernelTest{2D,3D}.cpp)
+# ------------------------------------------------------------------------------------------
+
+def test_golden3d_predictor_riemann_update(exa):
+    g = np.load(os.path.join(GOLD, "generic_euler_3d.npz"))
+    s = exa.Solver(exa.PDE_EULER, 3, 3, npar=1)
+    luh = with_params(g["testSpaceTimePredictorNonlinear.luh"], 5, 1)
+    r = s.space_time_predictor(luh, 0.05, 1.083937460199773e-3)
+    assert r["ret"] == 0
+    assert np.max(np.abs(strip_params(r["lQi"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQi"])) < EPS_REF
+    lFi = r["lFi"].reshape(4, 64, 4, 5)[:, :, :3, :].reshape(-1)
+    assert np.max(np.abs(lFi - g["testSpaceTimePredictorNonlinear.lFi"])) < EPS_REF
+    assert np.max(np.abs(strip_params(r["lQhbnd"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQhbnd"])) < EPS_REF
+    assert np.max(np.abs(r["lFhbnd"] - g["testSpaceTimePredictorNonlinear.lFhbnd"])) < EPS_REF
+    assert np.max(np.abs(strip_params(r["lQhi"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQhi"])) < EPS_REF
+    assert np.max(np.abs(r["lFhi"][:960] - g["testSpaceTimePredictorNonlinear.lFhi"])) < EPS_REF
+    # Rusanov, direction 1
+    FL, FR = s.riemann_cell(np.arange(1, 81, dtype=float), np.arange(-1, 79, dtype=float),
+                            with_params(g["testRiemannSolver.QL"], 5, 1), with_params(g["testRiemannSolver.QR"], 5, 1),
+                            0.5, 1)
+    assert np.max(np.abs(FL - g["testRiemannSolverNonlinear.FL"])) < EPS_REF
+    assert np.max(np.abs(FR - g["testRiemannSolverNonlinear.FR"])) < EPS_REF
+    # solution update
+    luh = np.zeros(6 * 64)
+    luh[0::6] = 1.0
+    luh[4::6] = 2.5
+    out = s.solution_update_cell(luh, np.arange(320, dtype=float), 1.40831757919882352703e-03)
+    assert np.max(np.abs(strip_params(out, 5, 1) - g["testSolutionUpdate.luh"])) < EPS_REF
+    assert s.status() == 0
+
+
+def test_golden2d_predictor_riemann_update(exa):
+    g = np.load(os.path.join(GOLD, "generic_euler_2d.npz"))
+    s = exa.Solver(exa.PDE_EULER, 2, 3, npar=1)
+    luh = with_params(g["testSpaceTimePredictorNonlinear.luh"], 5, 1)
+    r = s.space_time_predictor(luh, 0.05, 1.686854344081342e-3)
+    assert r["ret"] == 2 * 4 + 2
+    assert np.max(np.abs(strip_params(r["lQi"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQi"])) < EPS_REF
+    lFi = r["lFi"].reshape(4, 16, 3, 5)[:, :, :2, :].reshape(-1)
+    assert np.max(np.abs(lFi - g["testSpaceTimePredictorNonlinear.lFi"])) < EPS_REF
+    assert np.max(np.abs(strip_params(r["lQhi"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQhi"])) < EPS_REF
+    assert np.max(np.abs(r["lFhi"][:160] - g["testSpaceTimePredictorNonlinear.lFhi"])) < EPS_REF
+    assert np.max(np.abs(strip_params(r["lQhbnd"], 5, 1) - g["testSpaceTimePredictorNonlinear.lQhbnd"])) < EPS_REF
+    assert np.max(np.abs(r["lFhbnd"] - g["testSpaceTimePredictorNonlinear.lFhbnd"])) < EPS_REF
+    for case, d in ((1, 0), (2, 1)):
+        FL, FR = s.riemann_cell(g["testRiemannSolverNonlinear.FL_%d_in" % case],
+                                g["testRiemannSolverNonlinear.FR_%d_in" % case],
+                                with_params(g["testRiemannSolverNonlinear.QL_%d_in" % case], 5, 1),
+                                with_params(g["testRiemannSolverNonlinear.QR_%d_in" % case], 5, 1), 0.5, d)
+        ref = g["testRiemannSolverNonlinear.F_%d_out" % case]
+        assert np.max(np.abs(FL - ref)) < EPS_REF and np.max(np.abs(FR - ref)) < EPS_REF
+    luh = np.zeros(6 * 16)
+    luh[0::6] = 1.0
+    luh[4::6] = 2.5
+    out = s.solution_update_cell(luh, g["testSolutionUpdate.lduh"], 1.40831757919882352703e-03)
+    assert np.max(np.abs(strip_params(out, 5, 1) - g["testSolutionUpdate.luh"])) < EPS_REF
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_picard_nontrivial_vs_reference_fixture(exa, dim):
+    """Reference outputs on non-constant cells (the Picard loop really iterates here)."""
+    fx = np.load(os.path.join(GOLD, "picard_euler%dd_o3.npz" % dim))
+    s = exa.Solver(exa.PDE_EULER, dim, 3)
+    for c in range(int(fx["ncase"][0])):
+        k = lambda name: fx["case%d.%s" % (c, name)]
+        r = s.space_time_predictor(k("luh"), k("dx")[:dim], float(k("dt")[0]))
+        assert r["ret"] == int(k("iters")[0])
+        for key in ("lQi", "lQhi", "lFhi", "lQhbnd", "lFhbnd"):
+            assert rel(r[key], k(key)) < TOL, (c, key, rel(r[key], k(key)))
+
+
+# ------------------------------------------------------------------------------------------
+# batched kernels vs the oracle
+# ------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dim,order", [(3, 5), (3, 3), (2, 3)])
+def test_batched_predictor_volume_vs_oracle(exa, torch, dim, order):
+    rng = np.random.default_rng(100 + order)
+    n = order + 1
+    nd, nf = n ** dim, n ** (dim - 1)
+    ncells = 37
+    luh = euler_cells(rng, ncells, nd, amp=0.05, dim=dim).reshape(-1)
+    dx = np.array([0.02, 0.025, 0.03])[:dim]
+    o = Oracle(dim, order)
+    dt = min(o.dt(luh.reshape(ncells, -1)[c], dx) for c in range(ncells))
+    s = exa.Solver(exa.PDE_EULER, dim, order)
+    dev = torch.device("cuda")
+    t_luh = torch.from_numpy(luh).to(dev)
+    lduh = torch.zeros(ncells * nd * 5, dtype=torch.float64, device=dev)
+    qhb = torch.zeros(ncells * 2 * dim * nf * 5, dtype=torch.float64, device=dev)
+    fhb = torch.zeros_like(qhb)
+    pic = torch.zeros(ncells, dtype=torch.int32, device=dev)
+    s.fused_predictor_volume_integral(t_luh, lduh, qhb, fhb, dx, dt, picard=pic)
+    torch.cuda.synchronize()
+    lduh, qhb, fhb, pic = lduh.cpu().numpy(), qhb.cpu().numpy(), fhb.cpu().numpy(), pic.cpu().numpy()
+    for c in range(ncells):
+        r = o.predictor(luh.reshape(ncells, -1)[c], dx, dt)
+        assert pic[c] == r["sweeps"]
+        assert rel(qhb.reshape(ncells, -1)[c], r["lQhbnd"]) < TOL
+        assert rel(fhb.reshape(ncells, -1)[c], r["lFhbnd"]) < TOL
+        assert rel(lduh.reshape(ncells, -1)[c], o.volume(r["lFhi"], dx)) < TOL
+    assert s.status() == 0
+
+
+@pytest.mark.parametrize("dim,order", [(3, 5), (2, 3)])
+def test_batched_riemann_surface_update_cfl_vs_oracle(exa, torch, dim, order):
+    rng = np.random.default_rng(7)
+    n = order + 1
+    nd, nf = n ** dim, n ** (dim - 1)
+    ncells = 12
+    o = Oracle(dim, order)
+    s = exa.Solver(exa.PDE_EULER, dim, order)
+    dev = torch.device("cuda")
+    qhb = np.concatenate([euler_cells(rng, 2 * dim, nf, dim=dim).reshape(-1) for _ in range(ncells)])
+    fhb = rng.normal(size=ncells * 2 * dim * nf * 5)
+    left = np.array([0, 3, 5, 7, 11, 2], dtype=np.int32)
+    right = np.array([1, 4, 6, 8, 10, 9], dtype=np.int32)
+    dirs = np.array([0, 1, dim - 1, 0, 1, dim - 1], dtype=np.int8)
+    t_q = torch.from_numpy(qhb).to(dev)
+    t_f = torch.from_numpy(fhb.copy()).to(dev)
+    s.riemann(torch.from_numpy(left).to(dev), torch.from_numpy(right).to(dev), torch.from_numpy(dirs).to(dev), t_q, t_f)
+    got = t_f.cpu().numpy().reshape(ncells, 2 * dim, nf * 5)
+    exp = fhb.copy().reshape(ncells, 2 * dim, nf * 5)
+    qq = qhb.reshape(ncells, 2 * dim, nf * 5)
+    for L, R, d in zip(left, right, dirs):
+        FL, FR = o.riemann(exp[L, 2 * d + 1], exp[R, 2 * d], qq[L, 2 * d + 1], qq[R, 2 * d], 1.0, d)
+        exp[L, 2 * d + 1], exp[R, 2 * d] = FL, FR
+    assert rel(got, exp) < TOL
+    # surface integral + update, then CFL of the updated state
+    luh = euler_cells(rng, ncells, nd, dim=dim).reshape(-1)
+    lduh = rng.normal(size=ncells * nd * 5) * 0.01
+    dx = np.array([0.1, 0.07, 0.05])[:dim]
+    t_luh = torch.from_numpy(luh.copy()).to(dev)
+    s.surface_integral_and_update(t_luh, torch.from_numpy(lduh).to(dev), torch.from_numpy(fhb * 0.01).to(dev), dx, 1e-3)
+    new = t_luh.cpu().numpy().reshape(ncells, -1)
+    for c in range(ncells):
+        du = o.surface(lduh.reshape(ncells, -1)[c], (fhb * 0.01).reshape(ncells, -1)[c], dx)
+        ref = o.update(luh.reshape(ncells, -1)[c], du, 1e-3)
+        assert rel(new[c], ref) < TOL
+    cell_dt = torch.zeros(ncells, dtype=torch.float64, device=dev)
+    dtmin = s.stable_time_step_size(t_luh, dx, cell_dt=cell_dt)
+    ref_dt = np.array([o.dt(new[c], dx) for c in range(ncells)])
+    assert rel(cell_dt.cpu().numpy(), ref_dt) < 1e-15
+    assert dtmin == ref_dt.min()
+
+
+# ------------------------------------------------------------------------------------------
+# whole steps on device-resident patches vs the oracle's patch driver
+# ------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("dim,order,ncell,steps,walls", [
+    (2, 3, (27, 27), 20, False),      # 2D Euler entropy wave, the parity workload
+    (3, 3, (5, 4, 3), 4, False),
+    (3, 5, (4, 3, 3), 3, False),
+    (2, 3, (6, 5), 5, True),
+    (3, 3, (3, 3, 4), 3, True),
+])
+def test_patch_steps_vs_oracle(exa, dim, order, ncell, steps, walls):
+    import exa_scenarios as sc
+    if ncell == (27, 27):
+        luh0, _ = sc.euler_entropy_wave(ncell, order, seed=0)
+        size = [1.0, 1.0]
+    else:
+        rng = np.random.default_rng(3)
+        luh0 = euler_cells(rng, int(np.prod(ncell)), (order + 1) ** dim, amp=0.03, dim=dim).reshape(-1)
+        size = [1.0, 0.9, 0.8][:dim]
+    o = Oracle(dim, order)
+    ref = luh0.copy()
+    t_ref, dts, _ = o.run(ref, ncell, size, steps, walls=walls)
+    s = exa.Solver(exa.PDE_EULER, dim, order)
+    bc = exa.BC_WALL if walls else exa.BC_PERIODIC
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    p.set_solution(luh0)
+    p.step(steps)
+    got = p.get_solution()
+    t, dt = p.time()
+    assert abs(t[0] - t_ref) <= 1e-13 * t_ref
+    assert rel(got, ref) < TOL
+    assert p.status() == 0
+
+
+def test_patch_swe_walls_vs_oracle(exa):
+    """2D shallow water with bathymetry (NCP) and reflective walls."""
+    rng = np.random.default_rng(9)
+    order, ncell = 4, (7, 6)
+    n = order + 1
+    nc = ncell[0] * ncell[1]
+    Q = np.zeros((nc, n * n, 4))
+    Q[..., 0] = 1.0 + 0.2 * rng.uniform(0, 1, (nc, n * n))
+    Q[..., 1] = 0.05 * rng.normal(size=(nc, n * n))
+    Q[..., 2] = 0.05 * rng.normal(size=(nc, n * n))
+    Q[..., 3] = 0.1 * rng.uniform(0, 1, (nc, n * n))
+    luh0 = Q.reshape(-1)
+    o = Oracle(2, order, pde=PDE_SWE)
+    ref = luh0.copy()
+    t_ref, _, _ = o.run(ref, ncell, [1.0, 1.0], 4, walls=True)
+    s = exa.Solver(exa.PDE_SWE, 2, order)
+    p = exa.Patch(s, [dict(ncell=ncell, size=[1.0, 1.0], bc=exa.BC_WALL)])
+    p.set_solution(luh0)
+    p.step(4)
+    assert rel(p.get_solution(), ref) < TOL
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+
+
+def test_patch_many_grids_independent(exa):
+    """Several grids of different sizes in one patch advance exactly like separate patches."""
+    import exa_scenarios as sc
+    s = exa.Solver(exa.PDE_EULER, 2, 3)
+    specs = [dict(ncell=(9, 7), size=[1.0, 0.8]), dict(ncell=(5, 5), size=[0.5, 0.5], bc=exa.BC_WALL),
+             dict(ncell=(12, 4), size=[2.0, 1.0])]
+    rng = np.random.default_rng(2)
+    inits = [euler_cells(rng, int(np.prod(sp["ncell"])), 16, amp=0.04, dim=2).reshape(-1) for sp in specs]
+    multi = exa.Patch(s, specs)
+    multi.set_solution(np.concatenate(inits))
+    multi.step(3)
+    got = multi.get_solution()
+    t_multi, _ = multi.time()
+    off = 0
+    for g, (sp, init) in enumerate(zip(specs, inits)):
+        single = exa.Patch(s, [sp])
+        single.set_solution(init)
+        single.step(3)
+        ref = single.get_solution()
+        assert np.array_equal(got[off:off + ref.size], ref)
+        assert t_multi[g] == single.time()[0][0]
+        off += ref.size
