@@ -46,10 +46,26 @@ struct Shape {
   static constexpr int sizeQhb = 2 * DIM * nf * D;
   static constexpr int sizeFhb = 2 * DIM * nf * V;
   static constexpr int maxSweeps = 2 * n;
-  // dynamic shared memory of the predictor: lQi [cell][t][node][D] + flux/partials [cell][dir][V][node]
+  // flux/partials block of one (cell, dir, var): lines of n nodes, the x lines padded to n+1
+  // doubles so that neighbouring lines start in different shared-memory banks
+  static constexpr int BS = NL * (n + 1);
+  // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][D] + flux/partials
   static constexpr int smemQ = CPB * n * nd * D;
-  static constexpr int smemF = CPB * DIM * V * nd;
-  static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF);
+  static constexpr int smemF = CPB * DIM * V * BS;
+  static constexpr int items = CPB * DIM * V * NL;             // line contractions per time node
+  static constexpr int rounds = (items + TPB - 1) / TPB;       // per thread
+  static constexpr int smemU = CPB * nd * D;                   // luh of the CTA's cells
+  static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF + smemU);
+  // resident predictor CTAs per SM the register allocation is bounded for (shared memory
+  // allows two CTAs of 3D N=5 Euler cells: 2 x 77.8 KB)
+#ifndef EXA_PRED_MINBLOCKS
+#define EXA_PRED_MINBLOCKS 2
+#endif
+  static constexpr int MinBlocks = EXA_PRED_MINBLOCKS;
+  // registers are split over the SM's four 16K-register partitions: B blocks of W warps need
+  // ceil(B*W/4) warps' worth of registers in one partition
+  static constexpr int WarpsPerSmsp = (MinBlocks * (TPB / 32) + 3) / 4;
+  static constexpr int MaxRegs = (512 / WarpsPerSmsp) / 8 * 8 > 255 ? 255 : (512 / WarpsPerSmsp) / 8 * 8;
 };
 
 // Arguments shared by the cell kernels (device pointers).
@@ -128,410 +144,11 @@ __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
   atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-// ------------------------------------------------------------------------------------------
-// Fused predictor + volume integral
-// ------------------------------------------------------------------------------------------
-template <class PDE, int DIM, int N, int P>
-__global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB)
-predictor_kernel(CellArgs a) {
-  using S = Shape<PDE, DIM, N, P>;
-  using G = GL<N>;
-  constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, NL = S::NL, CPB = S::CPB;
-  constexpr bool NCP = PDE::kNCP;
-  extern __shared__ double smem[];
-  double* sQ = smem;                 // [CPB][n][nd][D]   lQi of the current iterate (time-major)
-  double* sF = smem + S::smemQ;      // [CPB][DIM][V][nd] fluxes, then contraction partials in place
-  __shared__ double s_w[n], s_Kxi[n * n], s_dudx[n * n], s_F0[n], s_F1[n];
-  __shared__ double s_dt[CPB], s_invdx[CPB][3], s_res[CPB];
-  __shared__ int s_active[CPB];
+}  // namespace exa
 
-  const int tid = threadIdx.x;
-  const bool inr = tid < CPB * nd;   // threads past the last cell only help in item loops
-  const int lc = inr ? tid / nd : 0; // cell within the CTA
-  const int p = inr ? tid % nd : 0;  // node within the cell
-  const long cell = (long)blockIdx.x * CPB + lc;
-  const bool live = inr && cell < a.ncells;
+#include "exa_predictor.cuh"
 
-  if (tid < n) {
-    s_w[tid] = G::weights(tid);
-    s_F0[tid] = G::F0(tid);
-    s_F1[tid] = G::F1(tid);
-  }
-  if (tid < n * n) {
-    s_Kxi[tid] = G::Kxi(tid / n, tid % n);
-    s_dudx[tid] = G::dudx(tid / n, tid % n);
-  }
-  if (tid < CPB) {
-    const long c = (long)blockIdx.x * CPB + tid;
-    const int g = (c < a.ncells && a.cell_grid) ? a.cell_grid[c] : 0;
-    s_dt[tid] = a.grid_dt ? a.grid_dt[g] : a.u_dt;
-#pragma unroll
-    for (int d = 0; d < 3; d++)
-      s_invdx[tid][d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
-    s_active[tid] = c < a.ncells;
-  }
-  __syncthreads();
-
-  int co[3];
-  node_coords<DIM, n>(p, co);
-  const double w_sp = DIM == 3 ? s_w[co[2]] * s_w[co[1]] * s_w[co[0]] : s_w[co[1]] * s_w[co[0]];
-  const double iweight = 1.0 / w_sp;
-  const double dt = s_dt[lc];
-  double invDx[3] = {s_invdx[lc][0], s_invdx[lc][1], s_invdx[lc][2]};
-
-  // luh of this node; the trivial initial guess lQi[., t] = luh (:71-82)
-  double u[D];
-  const double* luh = a.luh + (size_t)cell * nd * D + (size_t)p * D;
-#pragma unroll
-  for (int m = 0; m < D; m++) u[m] = live ? luh[m] : 1.0;
-  double* q_s = sQ + (size_t)lc * n * nd * D;
-  if (inr) {
-#pragma unroll
-    for (int t = 0; t < n; t++)
-#pragma unroll
-      for (int m = 0; m < D; m++) q_s[(t * nd + p) * D + m] = u[m];
-  }
-  double* f_s = sF + (size_t)lc * DIM * V * nd;
-
-  double qn[n][V];      // new iterate lQi[p][t][m], m < V
-  double fh[DIM][V];    // time-averaged flux of the current sweep (lFhi)
-  double sh[V];         // time-averaged source (lShi), NCP only
-  const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
-  int sweeps = 0;
-  bool done = false;
-
-  // Gradient of the iterate at time node ti and this node: gradQ[d][m] (:111-175), NCP only.
-  auto gradient = [&](int ti, double* gq) {
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      const int L = node_line<DIM, n>(p, d);
-      const int base = line_base<DIM, n>(d, L), st = line_stride<n>(d);
-      const int l = co[d];
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        double g = 0.0;
-#pragma unroll
-        for (int k = 0; k < n; k++)
-          g += 1.0 * invDx[d] * q_s[(ti * nd + base + k * st) * D + m] * s_dudx[l * n + k];
-        gq[d * V + m] = g;
-      }
-    }
-  };
-
-  // Phase 2: contractions along every line, in place on f_s. coef excludes/includes w_i.
-  auto contract = [&](double wi) {
-    for (int it = tid; it < CPB * DIM * V * NL; it += S::TPB) {
-      const int L = it % NL;
-      int r = it / NL;
-      const int m = r % V;
-      r /= V;
-      const int d = r % DIM;
-      const int c = r / DIM;
-      double* f = sF + ((size_t)(c * DIM + d) * V + m) * nd;
-      const int base = line_base<DIM, n>(d, L), st = line_stride<n>(d);
-      const double wt = DIM == 3 ? s_w[L / n] * s_w[L % n] : s_w[L];
-      const double coef = wi * wt * s_dt[c] * s_invdx[c][d];
-      double x[n];
-#pragma unroll
-      for (int k = 0; k < n; k++) x[k] = f[base + k * st];
-#pragma unroll
-      for (int l = 0; l < n; l++) {
-        double acc = 0.0;
-#pragma unroll
-        for (int k = 0; k < n; k++) acc = fma(x[k], G::Kxi(k, l), acc);
-        f[base + l * st] = coef * acc;
-      }
-    }
-  };
-
-  for (int s = 0; s < maxIter; s++) {
-    if (s_active[lc] == 0) done = true;  // phantom cells and converged cells idle
-    const bool work = live && !done;
-    // converged cells keep qn/fh/sh of their last sweep: only working cells reset and accumulate
-    if (work) {
-#pragma unroll
-      for (int t = 0; t < n; t++)
-#pragma unroll
-        for (int m = 0; m < V; m++) qn[t][m] = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; d++)
-#pragma unroll
-        for (int m = 0; m < V; m++) fh[d][m] = 0.0;
-#pragma unroll
-      for (int m = 0; m < V; m++) sh[m] = 0.0;
-    }
-
-    if (s == 0) {
-      // First sweep: the iterate is luh at every time node, so the flux, the gradient and the
-      // contractions are time-independent; compute them once and weight by w_i per time node.
-      double F[DIM * V];
-      double S0[V];
-      PDE::template flux<DIM>(u, F);
-      if (inr) {
-#pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) f_s[(d * V + m) * nd + p] = F[d * V + m];
-      }
-      if (NCP) {
-        double gq[DIM * V], B[V];
-        gradient(0, gq);
-        PDE::template ncp<DIM>(u, gq, B);
-#pragma unroll
-        for (int m = 0; m < V; m++) S0[m] = -B[m];
-      }
-      __syncthreads();
-      contract(1.0);
-      __syncthreads();
-      double o[V];
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        double acc = f_s[(0 * V + m) * nd + p];
-#pragma unroll
-        for (int d = 1; d < DIM; d++) acc += f_s[(d * V + m) * nd + p];
-        o[m] = acc;
-      }
-      if (a.ex_lFi && work) {
-        for (int i = 0; i < n; i++) {
-          double* e = a.ex_lFi + (size_t)cell * n * nd * (DIM + 1) * V + ((size_t)(i * nd + p) * (DIM + 1)) * V;
-          for (int d = 0; d < DIM; d++)
-            for (int m = 0; m < V; m++) e[d * V + m] = F[d * V + m];
-          if (NCP)
-            for (int m = 0; m < V; m++) e[DIM * V + m] = S0[m];
-        }
-      }
-      for (int i = 0; i < n && work; i++) {
-        const double wi = G::weights(i);
-        const double f0 = G::F0(i);
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          double rhs = w_sp * f0 * u[m] - wi * o[m];
-          if (NCP) rhs += wi * w_sp * dt * S0[m];
-          const double r = iweight * rhs;
-#pragma unroll
-          for (int t = 0; t < n; t++) qn[t][m] = fma(r, G::iK1(t, i), qn[t][m]);
-#pragma unroll
-          for (int d = 0; d < DIM; d++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
-          if (NCP) sh[m] = fma(S0[m], wi, sh[m]);
-        }
-      }
-      __syncthreads();
-    } else {
-      for (int i = 0; i < n; i++) {
-        // Phase 1: flux (and NCP source) of the iterate at time node i (:196-227, :323-367)
-        double q[D];
-#pragma unroll
-        for (int m = 0; m < D; m++) q[m] = q_s[(i * nd + p) * D + m];
-        double F[DIM * V];
-        double Si[V];
-        PDE::template flux<DIM>(q, F);
-        if (inr) {
-#pragma unroll
-          for (int d = 0; d < DIM; d++)
-#pragma unroll
-            for (int m = 0; m < V; m++) f_s[(d * V + m) * nd + p] = F[d * V + m];
-        }
-        if (NCP) {
-          double gq[DIM * V], B[V];
-          gradient(i, gq);
-          PDE::template ncp<DIM>(q, gq, B);
-#pragma unroll
-          for (int m = 0; m < V; m++) Si[m] = -B[m];
-        }
-        if (a.ex_lFi && work) {
-          double* e = a.ex_lFi + (size_t)cell * n * nd * (DIM + 1) * V + ((size_t)(i * nd + p) * (DIM + 1)) * V;
-          for (int d = 0; d < DIM; d++)
-            for (int m = 0; m < V; m++) e[d * V + m] = F[d * V + m];
-          if (NCP)
-            for (int m = 0; m < V; m++) e[DIM * V + m] = Si[m];
-        }
-        const double wi = G::weights(i);
-        __syncthreads();
-        // Phase 2: flux contractions with Kxi along x, y, z (:248-321)
-        contract(wi);
-        __syncthreads();
-        // Phase 3: rhs at time node i and the iK1 time solve (:231-246, :370-405)
-        const double f0 = G::F0(i);
-#pragma unroll
-        for (int m = 0; m < V && work; m++) {
-          double rhs = w_sp * f0 * u[m];
-#pragma unroll
-          for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * nd + p];
-          if (NCP) rhs += wi * w_sp * dt * Si[m];
-          const double r = iweight * rhs;
-#pragma unroll
-          for (int t = 0; t < n; t++) qn[t][m] = fma(r, G::iK1(t, i), qn[t][m]);
-#pragma unroll
-          for (int d = 0; d < DIM; d++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
-          if (NCP) sh[m] = fma(Si[m], wi, sh[m]);
-        }
-        __syncthreads();
-      }
-    }
-
-    // residual of this sweep and commit of the new iterate (:370-405)
-    double res = 0.0;
-    if (work) {
-#pragma unroll
-      for (int t = 0; t < n; t++)
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          double* o = &q_s[(t * nd + p) * D + m];
-          const double dlt = qn[t][m] - *o;
-          res = fma(dlt, dlt, res);
-          *o = qn[t][m];
-        }
-    }
-    // per-cell reduction: segmented warp tree, then one shared atomic per segment head
-    if (tid < CPB) s_res[tid] = 0.0;
-    __syncthreads();
-    {
-      const int lane = tid & 31;
-      const int seg_end = (lc + 1) * nd - 1;  // last thread of this cell
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double o = __shfl_down_sync(0xffffffffu, res, off);
-        if (lane + off < 32 && tid + off <= seg_end) res += o;
-      }
-      const bool head = (p == 0) || (lane == 0);
-      if (head && work) atomicAdd(&s_res[lc], res);
-    }
-    __syncthreads();
-    const bool was_active = !done;
-    if (work) {
-      sweeps = s + 1;
-      const double r = s_res[lc];
-      if (!finite(r)) {
-        if (a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
-      }
-      // exit test (:407-412): |res|^2 < 1e-7^2, unless a fixed sweep count is requested
-      if (a.max_picard <= 0 && r < 1e-7 * 1e-7) done = true;
-    }
-    (void)was_active;
-    // keep the block looping until every cell of the CTA has converged
-    __syncthreads();
-    if (p == 0 && live && done) s_active[lc] = 0;
-    __syncthreads();
-    bool any = false;
-#pragma unroll
-    for (int c = 0; c < CPB; c++) any |= s_active[c] != 0;
-    if (!any) break;
-    __syncthreads();
-  }
-  if (live && a.picard && p == 0) a.picard[cell] = sweeps;
-  if (live && p == 0 && a.max_picard <= 0 && !done && a.status) atomicOr(a.status, ST_PICARD_CAP);
-  __syncthreads();
-
-  // ---------------- time averaging (:441-515) ----------------
-  // lQhi[p][m] = sum_t w_t lQi[p][t][m]; parameters are constant in time.
-  double qh[D];
-#pragma unroll
-  for (int m = 0; m < D; m++) {
-    double acc = 0.0;
-#pragma unroll
-    for (int t = 0; t < n; t++) acc = fma(m < V ? q_s[(t * nd + p) * D + m] : u[m], G::weights(t), acc);
-    qh[m] = acc;
-  }
-  if (live && a.ex_lQi) {
-    double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
-    for (int t = 0; t < n; t++)
-      for (int m = 0; m < D; m++) e[t * D + m] = m < V ? q_s[(t * nd + p) * D + m] : u[m];
-  }
-  __syncthreads();
-  // stage lQhi [node][D] and lShi [node][V] in the lQi region, lFhi [dir][V][node] in the flux region
-  double* qh_s = q_s;
-  double* sh_s = q_s + nd * D;
-  if (inr) {
-#pragma unroll
-    for (int m = 0; m < D; m++) qh_s[p * D + m] = qh[m];
-#pragma unroll
-    for (int d = 0; d < DIM; d++)
-#pragma unroll
-      for (int m = 0; m < V; m++) f_s[(d * V + m) * nd + p] = fh[d][m];
-    if (NCP) {
-#pragma unroll
-      for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
-    }
-  }
-  if (live && a.ex_lQhi) {
-    for (int m = 0; m < D; m++) a.ex_lQhi[(size_t)cell * nd * D + p * D + m] = qh[m];
-  }
-  if (live && a.ex_lFhi) {
-    // reference lFhi blocks: x [z][y][x], y [z][x][y], z [y][x][z], source [z][y][x]
-    double* e = a.ex_lFhi + (size_t)cell * (DIM + 1) * nd * V;
-    for (int d = 0; d < DIM; d++) {
-      const int L = node_line<DIM, n>(p, d);
-      const int idx = L * n + co[d];
-      for (int m = 0; m < V; m++) e[(size_t)d * nd * V + idx * V + m] = fh[d][m];
-    }
-    for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = NCP ? sh[m] : 0.0;
-  }
-  __syncthreads();
-
-  // ---------------- volume integral (volumeIntegralNonlinear :133-223) ----------------
-  if (live) {
-    double* lduh = a.lduh + (size_t)cell * nd * V + (size_t)p * V;
-    double acc[V];
-#pragma unroll
-    for (int m = 0; m < V; m++) acc[m] = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      const int L = node_line<DIM, n>(p, d);
-      const int base = line_base<DIM, n>(d, L), st = line_stride<n>(d);
-      const double wt = DIM == 3 ? s_w[L / n] * s_w[L % n] : s_w[L];
-      const double us = wt * invDx[d];
-      const int k = co[d];
-#pragma unroll
-      for (int m = 0; m < V; m++)
-#pragma unroll
-        for (int mm = 0; mm < n; mm++)
-          acc[m] += s_Kxi[k * n + mm] * f_s[(d * V + m) * nd + base + mm * st] * us;
-    }
-    if (NCP) {
-#pragma unroll
-      for (int m = 0; m < V; m++) acc[m] += w_sp * sh_s[p * V + m];
-    }
-    bool ok = true;
-#pragma unroll
-    for (int m = 0; m < V; m++) {
-      lduh[m] = acc[m];
-      ok &= finite(acc[m]);
-    }
-    if (!ok && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
-  }
-
-  // ---------------- extrapolation to the faces (:517-687) ----------------
-  // lQhbnd[c][face][fn][D] then lFhbnd[c][face][fn][V]; item index runs over the output block
-  for (int j = tid; j < CPB * (S::sizeQhb + S::sizeFhb); j += S::TPB) {
-    const int c = j / (S::sizeQhb + S::sizeFhb);
-    const long gc = (long)blockIdx.x * CPB + c;
-    if (gc >= a.ncells) continue;
-    int r = j % (S::sizeQhb + S::sizeFhb);
-    const bool isQ = r < S::sizeQhb;
-    if (!isQ) r -= S::sizeQhb;
-    const int W = isQ ? D : V;
-    const int m = r % W;
-    const int fn = (r / W) % nf;
-    const int face = r / (W * nf);
-    const int d = face >> 1, o = face & 1;
-    const int base = line_base<DIM, n>(d, fn), st = line_stride<n>(d);
-    double acc = 0.0;
-    if (isQ) {
-      // 2D x faces extrapolate only the evolved variables (2d/spaceTimePredictorNonlinear.cpph:436-445)
-      if (!(DIM == 2 && d == 0 && m >= V)) {
-        const double* src = smem + (size_t)c * n * nd * D;
-#pragma unroll
-        for (int l = 0; l < n; l++) acc = fma(src[(base + l * st) * D + m], o ? G::F1(l) : G::F0(l), acc);
-      }
-      a.lQhbnd[(size_t)gc * S::sizeQhb + r] = acc;
-    } else {
-      const double* src = sF + ((size_t)(c * DIM + d) * V + m) * nd;
-#pragma unroll
-      for (int l = 0; l < n; l++) acc = fma(src[base + l * st], o ? G::F1(l) : G::F0(l), acc);
-      a.lFhbnd[(size_t)gc * S::sizeFhb + r] = acc;
-    }
-  }
-}
+namespace exa {
 
 // ------------------------------------------------------------------------------------------
 // Rusanov on interior faces: one warp per face, in place on lFhbnd

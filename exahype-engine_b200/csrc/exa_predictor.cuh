@@ -1,0 +1,506 @@
+// Fused space-time predictor + time averaging + face extrapolation + volume integral.
+//
+// Reference: ExaHyPE/kernels/aderdg/generic/c/3d/spaceTimePredictorNonlinear.cpph
+//   aderPicardLoopNonlinear :39-433, aderPredictorNonlinear :441-515,
+//   aderExtrapolatorNonlinear :517-687, entry :816-864 (2D: 2d/spaceTimePredictorNonlinear.cpph),
+// and 3d/volumeIntegralNonlinear.cpph:133-223 (time-averaged branch), as the generated glue
+// calls them in fusedSpaceTimePredictorVolumeIntegral (AbstractGenericADERDGSolverImplementation
+// .template:168-211).
+//
+// Work decomposition: one CTA per cell (several cells per CTA when a cell has fewer than 256
+// nodes), one thread per spatial node. A Picard sweep walks the n time nodes; per time node
+//   phase 1  each thread evaluates the flux (and the NCP source) of the old iterate at its node
+//            and writes it to shared memory,
+//   phase 2  every thread contracts whole lines (direction, variable, line) with Kxi, in place
+//            and already scaled by w_t w_a w_b dt/dx_d,
+//   phase 3  each thread forms its node's rhs and stores it, scaled by 1/w_xyz, as slice i.
+// The iK1 time solve runs once per sweep from the stored slices; the old iterate stays in
+// registers (the only per-node state carried across phases), the new one is staged in shared
+// memory until the per-cell residual decides whether the cell has converged.
+//
+// Sweep 0 starts from lQi[., t] = luh (:71-82), which is constant in time, so its flux and
+// contractions are computed once and weighted per time node (an exact identity, not an
+// approximation). For PDEs without NCP the time-averaged flux lFhi is re-evaluated from the final
+// old iterate after convergence instead of being carried through every sweep.
+#pragma once
+
+namespace exa {
+
+template <int DIM, int n>
+__device__ __forceinline__ int pline_base(int d, int L) {
+  // start of line L of direction d inside a padded (dir, var) block
+  if (d == 0) return L * (n + 1);
+  if (DIM == 3 && d == 1) return (L / n) * n * n + (L % n);
+  return L;
+}
+template <int DIM, int n>
+__device__ __forceinline__ int pnode_off(int d, int p) {
+  // offset of node p inside a padded (dir, var) block
+  return d == 0 ? p + p / n : p;
+}
+
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__((Shape<PDE, DIM, N, P>::TPB)) __maxnreg__((Shape<PDE, DIM, N, P>::MaxRegs))
+predictor_kernel(CellArgs a) {
+  using S = Shape<PDE, DIM, N, P>;
+  using G = GL<N>;
+  constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, NL = S::NL, CPB = S::CPB, BS = S::BS;
+  constexpr bool NCP = PDE::kNCP;
+  extern __shared__ double smem[];
+  double* sQ = smem;              // [CPB][n][nd][D]: old iterate (NCP), rhs slices, new iterate
+  double* sF = smem + S::smemQ;   // [CPB][DIM][V][BS]: fluxes, contracted in place
+  __shared__ double s_w[n], s_Kxi[n * n], s_dudx[n * n];
+  __shared__ double s_lw[CPB * DIM * NL];  // w_a w_b dt / dx_d of every line
+  __shared__ double s_dt[CPB], s_invdx[CPB][3], s_res[CPB];
+  __shared__ int s_active[CPB];
+
+  const int tid = threadIdx.x;
+  const bool inr = tid < CPB * nd;   // tail threads of the last warp only help in line loops
+  const int lc = inr ? tid / nd : 0;
+  const int p = inr ? tid % nd : 0;
+  const long cell = (long)blockIdx.x * CPB + lc;
+  const bool live = inr && cell < a.ncells;
+
+  if (tid < n) s_w[tid] = G::weights(tid);
+  if (tid < n * n) {
+    s_Kxi[tid] = G::Kxi(tid / n, tid % n);
+    s_dudx[tid] = G::dudx(tid / n, tid % n);
+  }
+  if (tid < CPB) {
+    const long c = (long)blockIdx.x * CPB + tid;
+    const int g = (c < a.ncells && a.cell_grid) ? a.cell_grid[c] : 0;
+    s_dt[tid] = a.grid_dt ? a.grid_dt[g] : a.u_dt;
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+      s_invdx[tid][d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
+    s_active[tid] = c < a.ncells;
+  }
+  __syncthreads();
+  for (int j = tid; j < CPB * DIM * NL; j += S::TPB) {
+    const int c = j / (DIM * NL), d = (j / NL) % DIM, L = j % NL;
+    const double wt = DIM == 3 ? s_w[L / n] * s_w[L % n] : s_w[L];
+    s_lw[j] = wt * s_dt[c] * s_invdx[c][d];
+  }
+
+  int co[3];
+  node_coords<DIM, n>(p, co);
+  const double w_sp = DIM == 3 ? s_w[co[2]] * s_w[co[1]] * s_w[co[0]] : s_w[co[1]] * s_w[co[0]];
+  const double iweight = 1.0 / w_sp;
+  const double dt = s_dt[lc];
+  int off[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) off[d] = pnode_off<DIM, n>(d, p);
+
+  // this thread's line contractions, packed: start offset in sF (bits 0-17), direction
+  // (bits 18-19), index of the line weight (bits 20-31); -1 when the thread has none
+  static_assert(S::smemF < (1 << 18) && CPB * DIM * NL < (1 << 12), "packed line descriptor overflow");
+  int it_pack[S::rounds];
+#pragma unroll
+  for (int r = 0; r < S::rounds; r++) {
+    const int it = tid + r * S::TPB;
+    if (it < S::items) {
+      const int L = it % NL;
+      const int m = (it / NL) % V;
+      const int d = (it / (NL * V)) % DIM;
+      const int c = it / (NL * V * DIM);
+      it_pack[r] = (((c * DIM + d) * V + m) * BS + pline_base<DIM, n>(d, L)) | (d << 18) |
+                   (((c * DIM + d) * NL + L) << 20);
+    } else {
+      it_pack[r] = -1;
+    }
+  }
+
+  // luh of this node, kept in shared memory (read once per phase, not worth 2*D registers);
+  // the old iterate starts as lQi[., t] = luh (:71-82)
+  double* u = sQ + S::smemQ + S::smemF + ((size_t)lc * nd + p) * D;
+  if (inr) {
+    const double* luh = a.luh + (size_t)cell * nd * D + (size_t)p * D;
+#pragma unroll
+    for (int m = 0; m < D; m++) u[m] = live ? luh[m] : 1.0;
+  }
+  double qo[n][V];  // old iterate; set to luh at the end of sweep 0, before the time solve
+  double* q_s = sQ + (size_t)lc * n * nd * D;
+  double* f_s = sF + (size_t)lc * DIM * V * BS;
+  if (NCP && inr) {  // neighbours' old iterate is read by the gradients
+#pragma unroll
+    for (int t = 0; t < n; t++)
+#pragma unroll
+      for (int m = 0; m < D; m++) q_s[(t * nd + p) * D + m] = u[m];
+  }
+  double fh[NCP ? DIM : 1][V];   // time-averaged flux / source of the sweep (NCP path only)
+  double sh[V];
+  (void)fh;
+  (void)sh;
+  __syncthreads();
+
+  // gradient of the old iterate at time node ti and this node (:111-175), NCP only
+  auto gradient = [&](int ti, double* gq) {
+    const double invDx[3] = {s_invdx[lc][0], s_invdx[lc][1], s_invdx[lc][2]};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const int st = d == 0 ? 1 : (d == 1 ? n : n * n);
+      const int base = p - co[d] * st;
+      const int l = co[d];
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        double g = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; k++) g += 1.0 * invDx[d] * q_s[(ti * nd + base + k * st) * D + m] * s_dudx[l * n + k];
+        gq[d * V + m] = g;
+      }
+    }
+  };
+  // phase 2: contraction of every line with Kxi, in place, scaled by wi * w_a w_b dt/dx_d (:248-321)
+  auto contract = [&](double wi) {
+#pragma unroll
+    for (int r = 0; r < S::rounds; r++) {
+      const int pk = it_pack[r];
+      if (pk < 0) continue;
+      double* f = sF + (pk & 0x3ffff);
+      const int dd = (pk >> 18) & 3;
+      const int st = dd == 0 ? 1 : (dd == 1 ? n : n * n);
+      const double coef = wi * s_lw[(unsigned)pk >> 20];
+      double x[n];
+#pragma unroll
+      for (int k = 0; k < n; k++) x[k] = f[k * st];
+#pragma unroll
+      for (int l = 0; l < n; l++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < n; k++) acc = fma(x[k], G::Kxi(k, l), acc);
+        f[l * st] = coef * acc;
+      }
+    }
+  };
+  auto store_flux = [&](const double* F) {
+    if (inr) {
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = F[d * V + m];
+    }
+  };
+  auto export_flux = [&](int i, const double* F, const double* Sv) {
+    double* e = a.ex_lFi + (size_t)cell * n * nd * (DIM + 1) * V + ((size_t)(i * nd + p) * (DIM + 1)) * V;
+    for (int d = 0; d < DIM; d++)
+      for (int m = 0; m < V; m++) e[d * V + m] = F[d * V + m];
+    for (int m = 0; m < V; m++) e[DIM * V + m] = NCP ? Sv[m] : 0.0;
+  };
+
+  const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
+  int sweeps = 0;
+  bool done = false;
+  for (int s = 0; s < maxIter; s++) {
+    if (s_active[lc] == 0) done = true;
+    const bool work = live && !done;
+    if (NCP && work) {
+#pragma unroll
+      for (int d = 0; d < (NCP ? DIM : 1); d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) fh[d][m] = 0.0;
+#pragma unroll
+      for (int m = 0; m < V; m++) sh[m] = 0.0;
+    }
+    if (s == 0) {
+      // the iterate is luh at every time node: one flux, one set of contractions
+      double F[DIM * V];
+      double S0[V];
+      PDE::template flux<DIM>(u, F);
+      store_flux(F);
+      if (NCP) {
+        double gq[DIM * V], B[V];
+        gradient(0, gq);
+        PDE::template ncp<DIM>(u, gq, B);
+#pragma unroll
+        for (int m = 0; m < V; m++) S0[m] = -B[m];
+        if (work) {
+          for (int i = 0; i < n; i++) {
+            const double wi = G::weights(i);
+#pragma unroll
+            for (int d = 0; d < (NCP ? DIM : 1); d++)
+#pragma unroll
+              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+#pragma unroll
+            for (int m = 0; m < V; m++) sh[m] = fma(S0[m], wi, sh[m]);
+          }
+        }
+      }
+      if (NCP && a.ex_lFi && work)
+        for (int i = 0; i < n; i++) export_flux(i, F, S0);
+      __syncthreads();
+      contract(1.0);
+      __syncthreads();
+      if (work) {
+        double o[V];
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          double acc = f_s[(0 * V + m) * BS + off[0]];
+#pragma unroll
+          for (int d = 1; d < DIM; d++) acc += f_s[(d * V + m) * BS + off[d]];
+          o[m] = acc;
+        }
+#pragma unroll
+        for (int i = 0; i < n; i++) {
+          const double wi = G::weights(i);
+          const double f0 = G::F0(i);
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            double rhs = w_sp * f0 * u[m] - wi * o[m];
+            if (NCP) rhs += wi * w_sp * dt * S0[m];
+            q_s[(i * nd + p) * D + m] = iweight * rhs;
+          }
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < n; t++)
+#pragma unroll
+        for (int m = 0; m < V; m++) qo[t][m] = u[m];
+    } else {
+      // The time loop is not unrolled: qo is rotated by one time node per iteration so that the
+      // current node always sits in qo[0] (compile-time register index), and after n
+      // iterations the rotation is back at its start.
+#pragma unroll
+      for (int i = 0; i < n; i++) {
+        // phase 1: flux (and NCP source) of the old iterate at time node i (:196-227, :323-367)
+        double q[D];
+#pragma unroll
+        for (int m = 0; m < D; m++) q[m] = m < V ? qo[i][m] : u[m];
+        double F[DIM * V];
+        double Si[V];
+        PDE::template flux<DIM>(q, F);
+        store_flux(F);
+        const double wi = G::weights(i);
+        if (NCP) {
+          double gq[DIM * V], B[V];
+          gradient(i, gq);
+          PDE::template ncp<DIM>(q, gq, B);
+#pragma unroll
+          for (int m = 0; m < V; m++) Si[m] = -B[m];
+          if (work) {
+#pragma unroll
+            for (int d = 0; d < (NCP ? DIM : 1); d++)
+#pragma unroll
+              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+#pragma unroll
+            for (int m = 0; m < V; m++) sh[m] = fma(Si[m], wi, sh[m]);
+          }
+          if (a.ex_lFi && work) export_flux(i, F, Si);
+        }
+        __syncthreads();
+        // phase 2
+        contract(wi);
+        __syncthreads();
+        // phase 3: rhs of time node i, scaled by 1/w_xyz, as slice i (:231-246, :323-367)
+        if (work) {
+          const double f0 = G::F0(i);
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            double rhs = w_sp * f0 * u[m];
+#pragma unroll
+            for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * BS + off[d]];
+            if (NCP) rhs += wi * w_sp * dt * Si[m];
+            q_s[(i * nd + p) * D + m] = iweight * rhs;
+          }
+        }
+        // no barrier: the next phase 1 rewrites only this thread's own flux slots, and the NCP
+        // gradients read slice i+1, which still holds the old iterate
+      }
+    }
+    __syncthreads();
+    // iK1 time solve (:370-405): new iterate, residual against the old one, staged in the slices
+    double res = 0.0;
+    if (work) {
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        double r[n];
+#pragma unroll
+        for (int i = 0; i < n; i++) r[i] = q_s[(i * nd + p) * D + m];
+#pragma unroll
+        for (int t = 0; t < n; t++) {
+          double qn = 0.0;
+#pragma unroll
+          for (int i = 0; i < n; i++) qn = fma(r[i], G::iK1(t, i), qn);
+          const double dl = qn - qo[t][m];
+          res = fma(dl, dl, res);
+          q_s[(t * nd + p) * D + m] = qn;
+        }
+      }
+    }
+    // per-cell residual: segmented warp tree, one shared atomic per segment head
+    if (tid < CPB) s_res[tid] = 0.0;
+    __syncthreads();
+    {
+      const int lane = tid & 31;
+      const int seg_end = (lc + 1) * nd - 1;
+#pragma unroll
+      for (int off2 = 16; off2 > 0; off2 >>= 1) {
+        const double o2 = __shfl_down_sync(0xffffffffu, res, off2);
+        if (lane + off2 < 32 && tid + off2 <= seg_end) res += o2;
+      }
+      if ((p == 0 || lane == 0) && work) atomicAdd(&s_res[lc], res);
+    }
+    __syncthreads();
+    if (work) {
+      sweeps = s + 1;
+      const double rr = s_res[lc];
+      if (!finite(rr) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+      // exit test (:407-412): |res|^2 < 1e-7^2, unless a fixed sweep count is requested
+      if (a.max_picard <= 0 && rr < 1e-7 * 1e-7) done = true;
+      if (!done) {
+        // the new iterate becomes the old one
+#pragma unroll
+        for (int t = 0; t < n; t++)
+#pragma unroll
+          for (int m = 0; m < V; m++) qo[t][m] = q_s[(t * nd + p) * D + m];
+      }
+    }
+    __syncthreads();
+    if (p == 0 && live && done) s_active[lc] = 0;
+    __syncthreads();
+    bool any = false;
+#pragma unroll
+    for (int c = 0; c < CPB; c++) any |= s_active[c] != 0;
+    if (!any) break;
+  }
+  if (live && a.picard && p == 0) a.picard[cell] = sweeps;
+  if (live && p == 0 && a.max_picard <= 0 && !done && a.status) atomicOr(a.status, ST_PICARD_CAP);
+
+  // ---------------- time averaging (:441-515) ----------------
+  // lQhi from the new iterate (staged in the slices); lFhi from the flux of the old iterate
+  double qh[D];
+#pragma unroll
+  for (int m = 0; m < D; m++) {
+    double acc = 0.0;
+#pragma unroll
+    for (int t = 0; t < n; t++) acc = fma(m < V ? q_s[(t * nd + p) * D + m] : u[m], G::weights(t), acc);
+    qh[m] = acc;
+  }
+  if (live && a.ex_lQi) {
+    double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
+    for (int t = 0; t < n; t++)
+      for (int m = 0; m < D; m++) e[t * D + m] = m < V ? q_s[(t * nd + p) * D + m] : u[m];
+  }
+  __syncthreads();
+  // stage lQhi [node][D] and lShi [node][V] in the slice region, lFhi in the flux blocks
+  double* qh_s = q_s;
+  double* sh_s = q_s + nd * D;
+  if (inr) {
+#pragma unroll
+    for (int m = 0; m < D; m++) qh_s[p * D + m] = qh[m];
+    if (NCP) {
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[NCP ? d : 0][m];
+#pragma unroll
+      for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
+    } else {
+      // lFhi = sum_t w_t F(old iterate at t), accumulated in this node's own flux slots
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = 0.0;
+#pragma unroll 1
+      for (int i = 0; i < n; i++) {
+        double q[D], F[DIM * V];
+#pragma unroll
+        for (int m = 0; m < D; m++) q[m] = m < V ? qo[0][m] : u[m];
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+          const double t0 = qo[0][m];
+#pragma unroll
+          for (int t = 0; t + 1 < n; t++) qo[t][m] = qo[t + 1][m];
+          qo[n - 1][m] = t0;
+        }
+        PDE::template flux<DIM>(q, F);
+        const double wi = G::weights(i);
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            double* slot = &f_s[(d * V + m) * BS + off[d]];
+            *slot = fma(F[d * V + m], wi, *slot);
+          }
+        if (live && a.ex_lFi) export_flux(i, F, nullptr);
+      }
+    }
+  }
+  if (live && a.ex_lQhi) {
+    for (int m = 0; m < D; m++) a.ex_lQhi[(size_t)cell * nd * D + p * D + m] = qh[m];
+  }
+  if (live && a.ex_lFhi) {
+    // reference lFhi blocks: x [z][y][x], y [z][x][y], z [y][x][z], source [z][y][x]
+    double* e = a.ex_lFhi + (size_t)cell * (DIM + 1) * nd * V;
+    for (int d = 0; d < DIM; d++) {
+      const int idx = node_line<DIM, n>(p, d) * n + co[d];
+      for (int m = 0; m < V; m++) e[(size_t)d * nd * V + idx * V + m] = f_s[(d * V + m) * BS + off[d]];
+    }
+    for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = NCP ? sh[m] : 0.0;
+  }
+  __syncthreads();
+
+  // ---------------- volume integral (volumeIntegralNonlinear :133-223) ----------------
+  if (live) {
+    double* lduh = a.lduh + (size_t)cell * nd * V + (size_t)p * V;
+    double acc[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) acc[m] = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const int L = node_line<DIM, n>(p, d);
+      const int base = pline_base<DIM, n>(d, L), st = d == 0 ? 1 : (d == 1 ? n : n * n);
+      const double wt = DIM == 3 ? s_w[L / n] * s_w[L % n] : s_w[L];
+      const double us = wt * s_invdx[lc][d];
+      const int k = co[d];
+#pragma unroll
+      for (int m = 0; m < V; m++)
+#pragma unroll
+        for (int mm = 0; mm < n; mm++) acc[m] += s_Kxi[k * n + mm] * f_s[(d * V + m) * BS + base + mm * st] * us;
+    }
+    if (NCP) {
+#pragma unroll
+      for (int m = 0; m < V; m++) acc[m] += w_sp * sh_s[p * V + m];
+    }
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      lduh[m] = acc[m];
+      ok &= finite(acc[m]);
+    }
+    if (!ok && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+  }
+
+  // ---------------- extrapolation to the faces (:517-687) ----------------
+  for (int j = tid; j < CPB * (S::sizeQhb + S::sizeFhb); j += S::TPB) {
+    const int c = j / (S::sizeQhb + S::sizeFhb);
+    const long gc = (long)blockIdx.x * CPB + c;
+    if (gc >= a.ncells) continue;
+    int r = j % (S::sizeQhb + S::sizeFhb);
+    const bool isQ = r < S::sizeQhb;
+    if (!isQ) r -= S::sizeQhb;
+    const int W = isQ ? D : V;
+    const int m = r % W;
+    const int fn = (r / W) % nf;
+    const int face = r / (W * nf);
+    const int d = face >> 1, o = face & 1;
+    const int st = d == 0 ? 1 : (d == 1 ? n : n * n);
+    double acc = 0.0;
+    if (isQ) {
+      // 2D x faces extrapolate only the evolved variables (2d/spaceTimePredictorNonlinear.cpph:436-445)
+      if (!(DIM == 2 && d == 0 && m >= V)) {
+        const double* src = smem + (size_t)c * n * nd * D;
+        const int base = line_base<DIM, n>(d, fn);
+#pragma unroll
+        for (int l = 0; l < n; l++) acc = fma(src[(base + l * st) * D + m], o ? G::F1(l) : G::F0(l), acc);
+      }
+      a.lQhbnd[(size_t)gc * S::sizeQhb + r] = acc;
+    } else {
+      const double* src = sF + ((size_t)(c * DIM + d) * V + m) * BS + pline_base<DIM, n>(d, fn);
+#pragma unroll
+      for (int l = 0; l < n; l++) acc = fma(src[l * st], o ? G::F1(l) : G::F0(l), acc);
+      a.lFhbnd[(size_t)gc * S::sizeFhb + r] = acc;
+    }
+  }
+}
+
+}  // namespace exa
