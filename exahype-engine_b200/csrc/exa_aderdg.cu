@@ -1,11 +1,12 @@
 // Host runtime and C ABI of the B200 ADER-DG cell update (include/exa_aderdg.h).
 //
 // One shared library, libexa_aderdg.so, compiled for sm_100a. The PDE functors, dimensions and
-// orders are template instantiations registered in make_ops(); the C ABI dispatches to them
+// orders are template instantiations registered in find_ops(); the C ABI dispatches to them
 // through the Ops interface. Everything device-side lives in exa_kernels.cuh.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -119,10 +120,14 @@ struct OpsImpl final : Ops {
   }
 };
 
-// The instantiations this library carries.
-std::unique_ptr<Ops> make_ops(int pde, int dim, int order, int npar) {
-#define EXA_CASE(PDEID, PDET, D_, N_, P_) \
-  if (pde == PDEID && dim == D_ && order == N_ && npar == P_) return std::unique_ptr<Ops>(new OpsImpl<PDET, D_, N_, P_>());
+// The instantiations this library carries: one function-local static launcher object each
+// (constructed on first use, never on the heap; shared by every solver handle).
+Ops* find_ops(int pde, int dim, int order, int npar) {
+#define EXA_CASE(PDEID, PDET, D_, N_, P_)                         \
+  if (pde == PDEID && dim == D_ && order == N_ && npar == P_) {    \
+    static OpsImpl<PDET, D_, N_, P_> inst;                         \
+    return &inst;                                                  \
+  }
   EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 5, 0)
   EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 3, 0)
   EXA_CASE(EXA_PDE_EULER, EulerPDE, 3, 3, 1)
@@ -140,7 +145,7 @@ std::unique_ptr<Ops> make_ops(int pde, int dim, int order, int npar) {
 // ------------------------------------------------------------------------------------------
 struct exa_solver {
   exa_solver_config cfg;
-  std::unique_ptr<exa::Ops> ops;
+  exa::Ops* ops = nullptr;  // static launcher object, not owned
   double cfl = 0.9, pnpm = 0.0;
   unsigned* d_status = nullptr;
   std::mutex mu;
@@ -174,7 +179,7 @@ int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
   if (cfg->max_picard < 0) return fail(EXA_ERR_INVALID, "max_picard must be >= 0");
   if (cfg->precision != EXA_PREC_FP64 && cfg->precision != EXA_PREC_MIXED)
     return fail(EXA_ERR_INVALID, "unknown precision");
-  auto ops = exa::make_ops(cfg->pde, cfg->dim, cfg->order, cfg->npar);
+  exa::Ops* ops = exa::find_ops(cfg->pde, cfg->dim, cfg->order, cfg->npar);
   if (!ops || cfg->precision != EXA_PREC_FP64)
     return fail(EXA_ERR_UNSUPPORTED, "no kernel instantiation for pde=" + std::to_string(cfg->pde) +
                                          " dim=" + std::to_string(cfg->dim) + " order=" +
@@ -182,7 +187,7 @@ int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
                                          " precision=" + std::to_string(cfg->precision));
   std::unique_ptr<exa_solver> s(new exa_solver());
   s->cfg = *cfg;
-  s->ops = std::move(ops);
+  s->ops = ops;
   s->cfl = cfg->cfl > 0 ? cfg->cfl : 0.9;
   s->pnpm = cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order);
   EXA_CUDA(cudaMalloc(&s->d_status, sizeof(unsigned)));
@@ -829,3 +834,80 @@ int exa_patch_status(exa_patch* p, unsigned* bits) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Allocation-free CFL time step (exa_stable_time_step_size_noalloc). No counterpart in the
+// reference. Its scratch -- the per-cell time steps, the minimum and a status word -- lives in
+// one file-scope device array instead of memory obtained from cudaMalloc. Every GPU that loads
+// this library holds the array (8 MiB + 256 B) until the process exits.
+// ------------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoallocHead = 32;  // doubles before the per-cell area: [0] minimum, [1] status bits
+static __device__ __align__(256) double g_exa_cfl_scratch[kNoallocHead + EXA_NOALLOC_MAX_CELLS];
+// device address of g_exa_cfl_scratch per device ordinal, looked up on the first call on a device
+std::atomic<double*> g_cfl_scratch_addr[64];
+
+int noalloc_scratch(double** out) {
+  int dev = 0;
+  EXA_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(EXA_ERR_INVALID, "device ordinal >= 64 not supported by the scratch table");
+  double* p = g_cfl_scratch_addr[dev].load();
+  if (!p) {
+    // the host-side name g_exa_cfl_scratch is only a stand-in: the kernels need the device address
+    void* addr = nullptr;
+    EXA_CUDA(cudaGetSymbolAddress(&addr, g_exa_cfl_scratch));
+    p = static_cast<double*>(addr);
+    g_cfl_scratch_addr[dev].store(p);
+  }
+  *out = p;
+  return EXA_OK;
+}
+
+}  // namespace
+
+extern "C" int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, int ncells, const double* luh,
+                                                 const double* dx, double* cell_dt, double* dt_min, void* stream) {
+  if (!cfg || !dx || (ncells > 0 && !luh)) return fail(EXA_ERR_INVALID, "null argument");
+  if (ncells < 0) return fail(EXA_ERR_INVALID, "ncells < 0");
+  if (ncells > EXA_NOALLOC_MAX_CELLS)
+    return fail(EXA_ERR_INVALID, "ncells = " + std::to_string(ncells) +
+                                     " exceeds EXA_NOALLOC_MAX_CELLS = " + std::to_string(EXA_NOALLOC_MAX_CELLS) +
+                                     "; use exa_stable_time_step_size for larger batches");
+  if (cfg->dim != 2 && cfg->dim != 3) return fail(EXA_ERR_INVALID, "dim must be 2 or 3");
+  exa::Ops* ops = exa::find_ops(cfg->pde, cfg->dim, cfg->order, cfg->npar);
+  if (!ops) return fail(EXA_ERR_UNSUPPORTED, "no kernel instantiation for this configuration");
+  double* scratch = nullptr;
+  if (int e = noalloc_scratch(&scratch)) return e;
+  cudaStream_t st = (cudaStream_t)stream;
+  double* d_min = scratch;
+  unsigned* d_status = reinterpret_cast<unsigned*>(scratch + 1);
+  double* d_cell = scratch + kNoallocHead;
+  // the array keeps the previous call's contents: reset the minimum and the status word
+  exa::fill_kernel<<<1, 32, 0, st>>>(1, d_min, INFINITY);
+  exa::fill_kernel<<<1, 32, 0, st>>>(1, scratch + 1, 0.0);
+  EXA_CUDA(cudaGetLastError());
+  if (ncells > 0) {
+    exa::CellArgs a;
+    memset(&a, 0, sizeof(a));
+    a.ncells = ncells;
+    a.luh = luh;
+    a.cell_dt = d_cell;
+    a.status = d_status;
+    a.cfl_pnpm = (cfg->cfl > 0 ? cfg->cfl : 0.9) * (cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order));
+    for (int d = 0; d < 3; d++) a.u_dx[d] = d < cfg->dim ? dx[d] : 1.0;
+    EXA_CUDA(ops->update(a, false, false, st));
+    exa::min_reduce_kernel<<<1, 1024, 0, st>>>(ncells, d_cell, d_min);
+    EXA_CUDA(cudaGetLastError());
+    if (cell_dt) EXA_CUDA(cudaMemcpyAsync(cell_dt, d_cell, sizeof(double) * ncells, cudaMemcpyDeviceToDevice, st));
+  }
+  unsigned bits = 0;
+  if (dt_min) {
+    EXA_CUDA(cudaMemcpyAsync(dt_min, d_min, sizeof(double), cudaMemcpyDeviceToHost, st));
+    EXA_CUDA(cudaMemcpyAsync(&bits, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    EXA_CUDA(cudaStreamSynchronize(st));
+    if (bits) return fail(EXA_ERR_NUMERICS, "non-finite state or non-positive dt (status bits " +
+                                                std::to_string(bits) + ")");
+  }
+  return EXA_OK;
+}

@@ -141,6 +141,31 @@ int exa_solution_update(exa_solver* s, int ncells, double* luh, const double* lu
 int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
                               double* dt_min, void* stream);
 
+/* Allocation-free variant of exa_stable_time_step_size. It has no counterpart in the reference.
+ *
+ * Who needs it: callers that cannot call cudaMalloc. One case is a host program whose device
+ * memory is owned by another runtime, such as a framework allocator that has reserved the whole
+ * pool. Another is a step loop that must not pay the device-wide synchronisation an allocation
+ * can imply. exa_solver_create allocates (its status word), so this entry point takes the solver
+ * configuration directly and needs no handle. It calls no cudaMalloc, cudaFree or other
+ * allocating routine.
+ *
+ * Inputs and outputs belong to the caller, as in exa_stable_time_step_size: luh and cell_dt are
+ * device arrays of ncells cells (cell_dt nullable); *dt_min is a host double (nullable;
+ * requesting it synchronises the stream).
+ * Its scratch -- every cell's time step, the minimum and a status word -- is one file-scope
+ * device array of the library sized for EXA_NOALLOC_MAX_CELLS cells (8 MiB). Every GPU that loads
+ * the library holds the array until the process exits.
+ *   - ncells > EXA_NOALLOC_MAX_CELLS is rejected with EXA_ERR_INVALID before any device work.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) and
+ *     caches it for that device; make that first call before any stream capture.
+ *   - All calls share the one array and each call resets what it reads, but calls that overlap
+ *     on the GPU (other streams, other host threads) race on it: serialise them.
+ * Returns EXA_ERR_NUMERICS when a cell's state is non-finite or gives dt <= 0 (dt_min requested). */
+#define EXA_NOALLOC_MAX_CELLS 1048576
+int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, int ncells, const double* luh, const double* dx,
+                                      double* cell_dt, double* dt_min, void* stream);
+
 /* ---- per-cell compatibility shims: the exact generic-kernel signatures on HOST pointers ----
  * One cell per call, synchronous; for conformance tests and glue that has not been batched yet. */
 

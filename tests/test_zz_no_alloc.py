@@ -1,0 +1,82 @@
+"""The allocation-free CFL entry point, exa_stable_time_step_size_noalloc.
+
+It serves callers that cannot call cudaMalloc (device memory owned by another runtime, or a step
+loop that must not pay an allocation's synchronisation). It keeps its scratch in a file-scope
+device array of the library instead. This test drives it through the C ABI on the GPU and checks
+it against the allocating entry point, exa_stable_time_step_size, on two calls in a row. The
+second call runs on a state with a larger time step, so a stale minimum left in the shared array
+would show. The file is named so that pytest collects it last.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-15  # same kernel arithmetic: the per-cell values are expected to be bit-identical
+
+
+def _cells(rng, ncells, nd, scale):
+    rho = 1.0 + 0.05 * rng.uniform(-1, 1, (ncells, nd))
+    u = scale * rng.uniform(-1, 1, (ncells, nd, 3))
+    p = 1.0 + 0.05 * rng.uniform(-1, 1, (ncells, nd))
+    Q = np.zeros((ncells, nd, 5))
+    Q[..., 0] = rho
+    Q[..., 1:4] = rho[..., None] * u
+    Q[..., 4] = p / 0.4 + 0.5 * rho * (u ** 2).sum(-1)
+    return Q.reshape(-1)
+
+
+def test_noalloc_cfl_matches_allocating_entry_point():
+    import torch
+    import exa_aderdg as exa
+
+    lib = exa.load_library()
+    f = lib.exa_stable_time_step_size_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.POINTER(exa._Config), ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                  ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    order, nd = 5, 216
+    cfg = exa._Config(3, order, 0, exa.PDE_EULER, 0.9, 0.0, 0, exa.PREC_FP64)
+    solver = exa.Solver(exa.PDE_EULER, 3, order)
+    dx3 = (ctypes.c_double * 3)(1.0 / 81, 1.0 / 81, 1.0 / 81)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rng = np.random.default_rng(4)
+    previous = None
+    for call, (ncells, speed) in enumerate(((3001, 0.6), (1777, 0.1))):
+        luh = torch.from_numpy(_cells(rng, ncells, nd, speed)).cuda()
+        want_cells = torch.zeros(ncells, dtype=torch.float64, device="cuda")
+        want_min = solver.stable_time_step_size(luh, [1.0 / 81] * 3, cell_dt=want_cells)
+        got_cells = torch.full((ncells,), -1.0, dtype=torch.float64, device="cuda")
+        got_min = ctypes.c_double(-1.0)
+        rc = f(ctypes.byref(cfg), ncells, ctypes.c_void_p(luh.data_ptr()), dx3, ctypes.c_void_p(got_cells.data_ptr()),
+               ctypes.byref(got_min), stream)
+        assert rc == 0, lib.exa_last_error()
+        torch.cuda.synchronize()
+        w, g = want_cells.cpu().numpy(), got_cells.cpu().numpy()
+        assert np.all(w > 0)
+        assert np.max(np.abs(g - w) / w) <= TOL
+        assert abs(got_min.value - want_min) <= TOL * want_min
+        assert got_min.value == w.min()
+        if previous is not None:
+            assert got_min.value > previous  # the slower state has the larger step: no stale minimum
+        previous = got_min.value
+
+
+def test_noalloc_cfl_rejects_oversized_batches():
+    import torch
+    import exa_aderdg as exa
+
+    lib = exa.load_library()
+    f = lib.exa_stable_time_step_size_noalloc
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.POINTER(exa._Config), ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                  ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]
+    cfg = exa._Config(3, 5, 0, exa.PDE_EULER, 0.9, 0.0, 0, exa.PREC_FP64)
+    dx3 = (ctypes.c_double * 3)(0.1, 0.1, 0.1)
+    dummy = torch.zeros(8, dtype=torch.float64, device="cuda")
+    out = ctypes.c_double(0.0)
+    rc = f(ctypes.byref(cfg), 1048576 + 1, ctypes.c_void_p(dummy.data_ptr()), dx3, None, ctypes.byref(out), None)
+    assert rc == 1  # EXA_ERR_INVALID, before any device work
+    assert b"EXA_NOALLOC_MAX_CELLS" in lib.exa_last_error()
