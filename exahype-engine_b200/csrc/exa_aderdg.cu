@@ -55,7 +55,8 @@ struct Ops {
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
   bool ncp;
   virtual ~Ops() {}
-  virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st) = 0;
+  bool mixed_ok = false;  // mixed-precision predictor instantiated
+  virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed = false) = 0;
   virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
   virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
   virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
@@ -64,8 +65,24 @@ struct Ops {
 template <class PDE, int DIM, int N, int P>
 struct OpsImpl final : Ops {
   using S = Shape<PDE, DIM, N, P>;
-  bool smem_set = false;
+  bool smem_set = false, smem_set_mixed = false;
+  static constexpr bool kMixed = !PDE::kNCP;
+  template <bool M>
+  cudaError_t launch_predictor(const CellArgs& a, cudaStream_t st, bool& set) {
+    constexpr bool MM = M && kMixed;
+    const size_t smem = MM ? S::predictor_smem_mixed : S::predictor_smem;
+    if (!set) {
+      cudaError_t e = cudaFuncSetAttribute(predictor_kernel<PDE, DIM, N, P, MM>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      set = true;
+    }
+    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
+    predictor_kernel<PDE, DIM, N, P, MM><<<blocks, S::TPB, smem, st>>>(a);
+    return cudaGetLastError();
+  }
   OpsImpl() {
+    mixed_ok = kMixed;
     dim = DIM;
     order = N;
     nvar = S::V;
@@ -83,17 +100,13 @@ struct OpsImpl final : Ops {
     sz_lQhi = (size_t)S::nd * S::D;
     sz_lFhi = (size_t)(DIM + 1) * S::nd * S::V;
   }
-  cudaError_t predictor(const CellArgs& a, cudaStream_t st) override {
+  cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed) override {
     if (a.ncells <= 0) return cudaSuccess;
-    if (!smem_set) {
-      cudaError_t e = cudaFuncSetAttribute(predictor_kernel<PDE, DIM, N, P>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::predictor_smem);
-      if (e != cudaSuccess) return e;
-      smem_set = true;
+    if (mixed) {
+      if (!kMixed) return cudaErrorNotSupported;
+      return launch_predictor<true>(a, st, smem_set_mixed);
     }
-    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
-    predictor_kernel<PDE, DIM, N, P><<<blocks, S::TPB, S::predictor_smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_predictor<false>(a, st, smem_set);
   }
   cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
     if (a.ncells <= 0) return cudaSuccess;
@@ -180,7 +193,7 @@ int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
   if (cfg->precision != EXA_PREC_FP64 && cfg->precision != EXA_PREC_MIXED)
     return fail(EXA_ERR_INVALID, "unknown precision");
   exa::Ops* ops = exa::find_ops(cfg->pde, cfg->dim, cfg->order, cfg->npar);
-  if (!ops || cfg->precision != EXA_PREC_FP64)
+  if (!ops || (cfg->precision == EXA_PREC_MIXED && !ops->mixed_ok))
     return fail(EXA_ERR_UNSUPPORTED, "no kernel instantiation for pde=" + std::to_string(cfg->pde) +
                                          " dim=" + std::to_string(cfg->dim) + " order=" +
                                          std::to_string(cfg->order) + " npar=" + std::to_string(cfg->npar) +
@@ -250,7 +263,7 @@ int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double*
   a.lFhbnd = lFhbnd;
   a.picard = picard_sweeps;
   set_uniform(a, s, dx, dt);
-  EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream));
+  EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream, s->cfg.precision == EXA_PREC_MIXED));
   return EXA_OK;
 }
 
@@ -383,7 +396,7 @@ int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbn
   double dx[3] = {1.0, 1.0, 1.0};
   for (int k = 0; k < s->cfg.dim; k++) dx[k] = 1.0 / invDx[k];
   set_uniform(a, s, dx, dt);
-  cudaError_t e = s->ops->predictor(a, 0);
+  cudaError_t e = s->ops->predictor(a, 0, s->cfg.precision == EXA_PREC_MIXED);
   if (e != cudaSuccess) {
     cuda_fail(e, "predictor");
     return -1;
@@ -569,7 +582,7 @@ static exa::FaceArgs patch_faces(exa_patch* p) {
 // enqueue one step on p->stream (used for capture)
 static int patch_enqueue_step(exa_patch* p, bool cfl) {
   exa::CellArgs a = patch_args(p);
-  EXA_CUDA(p->s->ops->predictor(a, p->stream));
+  EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
   exa::FaceArgs f = patch_faces(p);
   EXA_CUDA(p->s->ops->riemann(f, p->stream));
   if (p->nbfaces > 0) {

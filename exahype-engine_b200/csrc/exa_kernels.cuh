@@ -55,7 +55,9 @@ struct Shape {
   static constexpr int items = CPB * DIM * V * NL;             // line contractions per time node
   static constexpr int rounds = (items + TPB - 1) / TPB;       // per thread
   static constexpr int smemU = CPB * nd * D;                   // luh of the CTA's cells
+  static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
   static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF + smemU);
+  static constexpr size_t predictor_smem_mixed = sizeof(double) * (smemQ + smemF + smemU + smemO);
   // resident predictor CTAs per SM the register allocation is bounded for (shared memory
   // allows two CTAs of 3D N=5 Euler cells: 2 x 77.8 KB)
 #ifndef EXA_PRED_MINBLOCKS

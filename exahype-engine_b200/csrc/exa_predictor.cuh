@@ -39,13 +39,14 @@ __device__ __forceinline__ int pnode_off(int d, int p) {
   return d == 0 ? p + p / n : p;
 }
 
-template <class PDE, int DIM, int N, int P>
+template <class PDE, int DIM, int N, int P, bool MIXED>
 __global__ void __launch_bounds__((Shape<PDE, DIM, N, P>::TPB)) __maxnreg__((Shape<PDE, DIM, N, P>::MaxRegs))
 predictor_kernel(CellArgs a) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, NL = S::NL, CPB = S::CPB, BS = S::BS;
   constexpr bool NCP = PDE::kNCP;
+  static_assert(!(MIXED && NCP), "the mixed-precision sweeps are built for PDEs without NCP");
   extern __shared__ double smem[];
   double* sQ = smem;              // [CPB][n][nd][D]: old iterate (NCP), rhs slices, new iterate
   double* sF = smem + S::smemQ;   // [CPB][DIM][V][BS]: fluxes, contracted in place
@@ -118,6 +119,8 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
     for (int m = 0; m < D; m++) u[m] = live ? luh[m] : 1.0;
   }
+  // mixed precision: the sweep-0 contraction of F(luh), per node and variable (summed over d)
+  double* o_s = sQ + S::smemQ + S::smemF + S::smemU + ((size_t)lc * nd + p) * V;
   double qo[n][V];  // old iterate; set to luh at the end of sweep 0, before the time solve
   double* q_s = sQ + (size_t)lc * n * nd * D;
   double* f_s = sF + (size_t)lc * DIM * V * BS;
@@ -168,6 +171,30 @@ predictor_kernel(CellArgs a) {
         double acc = 0.0;
 #pragma unroll
         for (int k = 0; k < n; k++) acc = fma(x[k], G::Kxi(k, l), acc);
+        f[l * st] = coef * acc;
+      }
+    }
+  };
+  // mixed precision, phase 2: the same contractions on the FP32 flux corrections F(q) - F(luh),
+  // stored as floats in the first half of the flux region
+  auto contractf = [&](float wi) {
+    float* sFf = reinterpret_cast<float*>(sF);
+#pragma unroll
+    for (int r = 0; r < S::rounds; r++) {
+      const int pk = it_pack[r];
+      if (pk < 0) continue;
+      float* f = sFf + (pk & 0x3ffff);
+      const int dd = (pk >> 18) & 3;
+      const int st = dd == 0 ? 1 : (dd == 1 ? n : n * n);
+      const float coef = wi * (float)s_lw[(unsigned)pk >> 20];
+      float x[n];
+#pragma unroll
+      for (int k = 0; k < n; k++) x[k] = f[k * st];
+#pragma unroll
+      for (int l = 0; l < n; l++) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int k = 0; k < n; k++) acc = fmaf(x[k], G::Kxif(k, l), acc);
         f[l * st] = coef * acc;
       }
     }
@@ -238,6 +265,7 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
           for (int d = 1; d < DIM; d++) acc += f_s[(d * V + m) * BS + off[d]];
           o[m] = acc;
+          if (MIXED) o_s[m] = acc;
         }
 #pragma unroll
         for (int i = 0; i < n; i++) {
@@ -268,7 +296,20 @@ predictor_kernel(CellArgs a) {
         double F[DIM * V];
         double Si[V];
         PDE::template flux<DIM>(q, F);
-        store_flux(F);
+        if (MIXED) {
+          // flux correction relative to luh, exact in FP64, then rounded to FP32
+          double Fu[DIM * V];
+          PDE::template flux<DIM>(u, Fu);
+          if (inr) {
+            float* sFf = reinterpret_cast<float*>(f_s);
+#pragma unroll
+            for (int d = 0; d < DIM; d++)
+#pragma unroll
+              for (int m = 0; m < V; m++) sFf[(d * V + m) * BS + off[d]] = (float)(F[d * V + m] - Fu[d * V + m]);
+          }
+        } else {
+          store_flux(F);
+        }
         const double wi = G::weights(i);
         if (NCP) {
           double gq[DIM * V], B[V];
@@ -288,7 +329,10 @@ predictor_kernel(CellArgs a) {
         }
         __syncthreads();
         // phase 2
-        contract(wi);
+        if (MIXED)
+          contractf((float)wi);
+        else
+          contract(wi);
         __syncthreads();
         // phase 3: rhs of time node i, scaled by 1/w_xyz, as slice i (:231-246, :323-367)
         if (work) {
@@ -296,8 +340,17 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
           for (int m = 0; m < V; m++) {
             double rhs = w_sp * f0 * u[m];
+            if (MIXED) {
+              const float* sFf = reinterpret_cast<const float*>(f_s);
+              float c = 0.0f;
 #pragma unroll
-            for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * BS + off[d]];
+              for (int d = 0; d < DIM; d++) c += sFf[(d * V + m) * BS + off[d]];
+              rhs -= wi * o_s[m];
+              rhs -= (double)c;
+            } else {
+#pragma unroll
+              for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * BS + off[d]];
+            }
             if (NCP) rhs += wi * w_sp * dt * Si[m];
             q_s[(i * nd + p) * D + m] = iweight * rhs;
           }

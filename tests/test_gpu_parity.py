@@ -284,3 +284,33 @@ def test_patch_many_grids_independent(exa):
         assert np.array_equal(got[off:off + ref.size], ref)
         assert t_multi[g] == single.time()[0][0]
         off += ref.size
+
+
+@pytest.mark.parametrize("dim,order,ncell,steps", [(3, 5, (4, 3, 3), 3), (2, 3, (27, 27), 10)])
+def test_mixed_precision_patch_vs_fp64_oracle(exa, dim, order, ncell, steps):
+    """Mixed mode: FP32 contractions of the flux corrections F(q) - F(luh) inside FP64 sweeps.
+    The iterate, the residual test, the time solve, the update and the CFL stay FP64, so the state
+    stays within 1e-9 (relative) of the FP64 oracle and the Picard counts are unchanged."""
+    import exa_scenarios as sc
+    if dim == 2:
+        luh0, _ = sc.euler_entropy_wave(ncell, order, seed=0)
+    else:
+        rng = np.random.default_rng(3)
+        luh0 = euler_cells(rng, int(np.prod(ncell)), (order + 1) ** dim, amp=0.03, dim=dim).reshape(-1)
+    size = [1.0] * dim
+    ref = luh0.copy()
+    t_ref, _, pic = Oracle(dim, order).run(ref, ncell, size, steps, want_picard=True)
+    s = exa.Solver(exa.PDE_EULER, dim, order, precision=exa.PREC_MIXED)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size)])
+    p.set_solution(luh0)
+    p.step(steps)
+    got = p.get_solution()
+    assert rel(got, ref) < 1e-9
+    assert abs(p.time()[0][0] - t_ref) <= 1e-9 * t_ref
+    assert p.stats()["picard_mean"] == pytest.approx(pic[-1].mean())
+    assert p.status() == 0
+
+
+def test_mixed_precision_rejected_for_ncp(exa):
+    with pytest.raises(exa.ExaError):
+        exa.Solver(exa.PDE_SWE, 2, 4, precision=exa.PREC_MIXED)
