@@ -40,6 +40,9 @@ def parse():
     ap.add_argument("--ncell", type=int, default=81, help="cells per axis (81 = the benchmark workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "swe_batched"],
+                    help="euler3d: the headline workload; swe_batched: 512 wall-bounded 2D SWE grids, N=4")
     return ap.parse_args()
 
 
@@ -157,10 +160,70 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def swe_cpu_sample(specs, states, steps=1):
+    """Reference generic kernels (oracle/_ref, SWE N=4, walls) on the first 8 grids, OpenMP."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    from pyoracle import Oracle, RefKernels, PDE_SWE
+    kind = "reference"
+    try:
+        runner = RefKernels(2, 4, pde="swe")
+    except Exception:
+        runner, kind = Oracle(2, 4, pde=PDE_SWE), "port"
+    cores = os.cpu_count()
+    cells = 0
+    t0 = time.perf_counter()
+    for sp, st in list(zip(specs, states))[:8]:
+        runner.run(st.copy(), sp["ncell"], sp["size"], steps, walls=True, nthreads=cores)
+        cells += sp["ncell"][0] * sp["ncell"][1]
+    el = time.perf_counter() - t0
+    return {"value": cells * 4 * 25 * steps / el, "unit": "DoF-updates/s", "cores": cores, "kind": kind,
+            "sample": "first 8 of the 512 grids (%d cells), %d step(s), %.1f s" % (cells, steps, el)}
+
+
+def run_swe_batched(args):
+    """512 independent wall-bounded 2D shallow-water grids (16^2..128^2 cells, N=4), each with its
+    own CFL time step, advanced together: one CUDA graph launch per step."""
+    import torch
+    import exa_aderdg as exa
+    import exa_scenarios as sc
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    specs, states = sc.swe_batched()
+    cells = sum(sp["ncell"][0] * sp["ncell"][1] for sp in specs)
+    dof_step = cells * 4 * 25
+    solver = exa.Solver(exa.PDE_SWE, 2, 4)
+    patch = exa.Patch(solver, specs)
+    patch.set_solution(np.concatenate(states))
+    stream = torch.cuda.ExternalStream(patch.stream)
+    W, K = args.warmup, args.steps
+    patch.step(W)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        ev0.record(stream)
+        patch.step(K)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / K
+    line = {"metric": "ADER-DG DoF-updates/s (batched 2D SWE N=4, 512 grids)", "value": dof_step / (ms * 1e-3),
+            "unit": "DoF-updates/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "512 2D shallow-water grids (h,hu,hv,b; NCP), sides U{16..128}, N=4, "
+                                   "reflective walls, per-grid CFL dt, one CUDA graph per step",
+                       "cells": cells, "dof_per_step": dof_step},
+            "picard_sweeps_mean": patch.stats()["picard_mean"], "status_bits": patch.status(),
+            "gpu_launches": K * 5, "clocks": clocks.summary()}
+    if not args.no_cpu:
+        line["cpu_baseline"] = swe_cpu_sample(specs, states)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "swe_batched":
+        run_swe_batched(args)
         return
     import torch
     import torch.distributed as dist
@@ -179,11 +242,18 @@ def main():
     cells = int(np.prod(ncell))
     dof_step = cells * NVAR * (ORDER + 1) ** 3
 
-    solver = exa.Solver(exa.PDE_EULER, 3, ORDER)
-    patch = exa.Patch(solver, [dict(ncell=ncell, size=[1.0, 1.0, 1.0])])
-    luh0, wave = sc.euler_entropy_wave(ncell, ORDER, seed=0)
-    patch.set_solution(luh0)
-    stream = torch.cuda.ExternalStream(patch.stream)
+    precision = exa.PREC_MIXED if args.precision == "mixed" else exa.PREC_FP64
+    solver = exa.Solver(exa.PDE_EULER, 3, ORDER, precision=precision)
+    # every rank owns one 81^3 slab of an 81 x 81 x (81 N) periodic grid (dx = 1/81 everywhere)
+    from exa_distributed import SlabPatch
+    slab = SlabPatch(solver, (ncell[0], ncell[1], ncell[2] * world), [1.0, 1.0, float(world)], rank=rank,
+                     world=world)
+    patch = slab.patch
+    lnc, lsize, loff = slab.local_grid()
+    wave = sc.EntropyWave(3, 0)
+    luh0 = wave.state(sc.nodal_positions(lnc, lsize, ORDER, offset=loff)).reshape(-1)
+    slab.set_local_solution(luh0)
+    stream = slab.stream
 
     def barrier():
         if world > 1:
@@ -191,13 +261,13 @@ def main():
         torch.cuda.synchronize()
 
     # ---- device-resident steps (graph per step), CUDA events on the patch's stream ----
-    patch.step(W)
+    slab.step(W)
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         barrier()
         ev0.record(stream)
-        patch.step(K)
+        slab.step(K)
         ev1.record(stream)
         ev1.synchronize()
         barrier()
@@ -209,6 +279,42 @@ def main():
     stats = patch.stats()
     status = patch.status()
     t_now, dt_now = patch.time()
+    # accuracy after W+K steps: rho against the exact entropy wave on every 37th cell
+    sol = patch.get_solution().reshape(cells, -1)
+    pick = np.arange(0, cells, 37)
+    xs = sc.nodal_positions(lnc, lsize, ORDER, offset=loff).reshape(cells, -1, 3)[pick]
+    exact = wave.state(xs, float(t_now[0]))
+    l2_exact, linf_exact = sc.l2_linf_error(sol[pick], exact, ORDER, 3)
+
+    # the other precision on the same state and step count, for the mixed-vs-FP64 comparison
+    other = None
+    if rank == 0:
+        oprec = exa.PREC_FP64 if precision == exa.PREC_MIXED else exa.PREC_MIXED
+        s2 = exa.Solver(exa.PDE_EULER, 3, ORDER, precision=oprec)
+        p2 = exa.Patch(s2, [dict(ncell=ncell, size=[1.0, 1.0, 1.0])])
+        p2.set_solution(luh0)
+        st2 = torch.cuda.ExternalStream(p2.stream)
+        p2.step(W)
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(st2)
+        p2.step(K)
+        a1.record(st2)
+        a1.synchronize()
+        ms2 = a0.elapsed_time(a1) / K
+        sol2 = p2.get_solution().reshape(cells, -1)
+        d = sol2 - sol
+        l2o, linfo = sc.l2_linf_error(sol2[pick], exact, ORDER, 3)
+        other = {"precision": "fp64" if oprec == exa.PREC_FP64 else "mixed",
+                 "value": dof_step / (ms2 * 1e-3), "ms_per_step": ms2,
+                 "speedup_of_mixed_over_fp64": (ms2 / ms) if oprec == exa.PREC_FP64 else (ms / ms2),
+                 "l2_rho_vs_exact": l2o, "linf_rho_vs_exact": linfo,
+                 "max_abs_diff_vs_this_run": float(np.max(np.abs(d))),
+                 "l2_rel_diff_vs_this_run": float(np.linalg.norm(d) / np.linalg.norm(sol)),
+                 "status_bits": p2.status()}
+        p2.close()
+        s2.close()
+        del sol2, d
 
     # ---- dominant kernel (predictor) timed alone, events on the same stream ----
     import ctypes
@@ -257,9 +363,9 @@ def main():
         host_out = torch.empty_like(host_in).pin_memory()
         nbytes = host_in.numel() * 8
         def e2e_step():
-            patch.set_solution(host_in.numpy())  # H2D + CFL dt of the uploaded state
-            patch.step(1)
-            patch.get_solution(host_out.numpy())  # D2H of the result
+            slab.set_local_solution(host_in.numpy())  # H2D + CFL dt of the uploaded state
+            slab.step(1)
+            slab.get_solution(host_out.numpy())  # D2H of the result
         e2e_step()
         barrier()
         t0 = time.perf_counter()
@@ -280,12 +386,17 @@ def main():
         "metric": METRIC, "value": world * dof_step / (ms * 1e-3), "unit": "DoF-updates/s", "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "3D Euler N=5 (6^3 nodes, nVar=5) entropy wave, %d^3 periodic cells, CFL 0.9, "
-                               "FP64 Picard predictor + Rusanov + update, one CUDA graph per step" % ncell[0],
+        "config": {"workload": "3D Euler N=5 (6^3 nodes, nVar=5) entropy wave, %d^3 periodic cells per GPU "
+                               "(slab of %dx%dx%d), CFL 0.9, Picard predictor + Rusanov + update, one CUDA graph "
+                               "per step on 1 GPU; halo exchange + dt all-reduce over NCCL on N GPUs"
+                               % (ncell[0], ncell[0], ncell[1], ncell[2] * world),
                    "cells": cells, "dof_per_step": dof_step, "l2": "inputs 4.6 GB > L2, no flush needed",
-                   "precision": "fp64"},
+                   "precision": args.precision},
         "cell_updates_per_s": world * cells / (ms * 1e-3),
         "picard_sweeps_mean": stats["picard_mean"], "status_bits": status,
+        "accuracy": {"t": float(t_now[0]), "l2_rho_vs_exact": l2_exact, "linf_rho_vs_exact": linf_exact,
+                     "sample": "every 37th cell, exact entropy wave at t"},
+        "other_precision": other,
         "roofline": {"bound": "tensor", "kernel": "predictor_kernel (fused Picard + volume integral)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
@@ -304,7 +415,7 @@ def main():
             line["cpu_baseline"] = {"value": None, "error": str(ex)}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    patch.close()
+    slab.close()
     if world > 1:
         dist.destroy_process_group()
 

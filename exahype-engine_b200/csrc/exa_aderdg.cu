@@ -538,6 +538,11 @@ struct exa_patch {
   cudaGraphExec_t graph_cfl = nullptr, graph_fixed = nullptr;
   bool track_picard = false;
   double fixed_dt = -1.0;
+  // halo (slab decomposition): ghost cells appended after the real cells, face traces only
+  long long nghost = 0;      // 2 * layer cells, or 0
+  int halo_axis = -1;        // axis with EXA_BC_HALO
+  long long layer = 0;       // cells per layer normal to the halo axis
+  long long halo_lo_first = 0, halo_hi_first = 0;  // first real cell of the low / high boundary layer
 };
 
 static void patch_free(exa_patch* p) {
@@ -621,6 +626,114 @@ static int patch_graph(exa_patch* p, bool cfl, cudaGraphExec_t* out) {
   return EXA_OK;
 }
 
+namespace {
+struct FaceBuild {
+  long long ncells = 0, nghost = 0, layer = 0;
+  int halo_axis = -1;
+  std::vector<int> cell_grid, fL, fR, bc;
+  std::vector<int8_t> fd, bf;
+  std::vector<double> dx;
+  std::vector<long long> first;
+};
+
+// Face lists of a batch of uniform grids: interior faces (left cell, right cell, axis), domain
+// faces with a wall (cell, face 2*axis+orientation), and, for EXA_BC_HALO on the last axis of a
+// single grid, faces joining the boundary layers to ghost cells appended after the real cells
+// (low ghost layer first, then the high one; cell index within a layer as in the grid).
+int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) {
+  fb.dx.assign(3 * ngrids, 1.0);
+  long long c0 = 0;
+  for (int g = 0; g < ngrids; g++) {
+    const exa_grid_desc& G = grids[g];
+    int nc[3] = {G.ncell[0], G.ncell[1], dim == 3 ? G.ncell[2] : 1};
+    for (int d = 0; d < dim; d++) {
+      if (nc[d] <= 0 || !(G.size[d] > 0)) return fail(EXA_ERR_INVALID, "grid extents must be positive");
+      if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL && G.bc[d] != EXA_BC_HALO)
+        return fail(EXA_ERR_INVALID, "unknown boundary");
+      if (G.bc[d] == EXA_BC_HALO && (d != dim - 1 || ngrids != 1))
+        return fail(EXA_ERR_INVALID, "EXA_BC_HALO is supported on the last axis of a single-grid patch");
+      fb.dx[3 * g + d] = G.size[d] / nc[d];
+    }
+    const long long n = (long long)nc[0] * nc[1] * nc[2];
+    fb.first.push_back(c0);
+    c0 += n;
+  }
+  fb.ncells = c0;
+  const bool halo = grids[0].bc[dim - 1] == EXA_BC_HALO;
+  if (halo) {
+    fb.halo_axis = dim - 1;
+    fb.layer = dim == 3 ? (long long)grids[0].ncell[0] * grids[0].ncell[1] : grids[0].ncell[0];
+    fb.nghost = 2 * fb.layer;
+  }
+  if (fb.ncells + fb.nghost > 0x7fffffffLL) return fail(EXA_ERR_INVALID, "too many cells for 32-bit face indices");
+  for (int g = 0; g < ngrids; g++) {
+    const exa_grid_desc& G = grids[g];
+    const long long c0g = fb.first[g];
+    int nc[3] = {G.ncell[0], G.ncell[1], dim == 3 ? G.ncell[2] : 1};
+    auto idx = [&](int x, int y, int z) { return c0g + ((long long)z * nc[1] + y) * nc[0] + x; };
+    auto lidx = [&](int x, int y) { return dim == 3 ? (long long)y * nc[0] + x : (long long)x; };
+    for (int d = 0; d < dim; d++)
+      for (int z = 0; z < nc[2]; z++)
+        for (int y = 0; y < nc[1]; y++)
+          for (int x = 0; x < nc[0]; x++) {
+            int j[3] = {x, y, z};
+            const int i_d = j[d];
+            j[d] += 1;
+            const long long c = idx(x, y, z);
+            if (j[d] == nc[d]) {
+              if (G.bc[d] == EXA_BC_PERIODIC) {
+                j[d] = 0;
+              } else if (G.bc[d] == EXA_BC_WALL) {
+                fb.bc.push_back((int)c);
+                fb.bf.push_back((int8_t)(2 * d + 1));
+              } else {  // halo: the high ghost cell of this column is the right cell
+                fb.fL.push_back((int)c);
+                fb.fR.push_back((int)(fb.ncells + fb.layer + lidx(x, y)));
+                fb.fd.push_back((int8_t)d);
+              }
+            }
+            if (j[d] < nc[d]) {
+              fb.fL.push_back((int)c);
+              fb.fR.push_back((int)idx(j[0], j[1], j[2]));
+              fb.fd.push_back((int8_t)d);
+            }
+            if (i_d == 0 && G.bc[d] == EXA_BC_WALL) {
+              fb.bc.push_back((int)c);
+              fb.bf.push_back((int8_t)(2 * d));
+            }
+            if (i_d == 0 && G.bc[d] == EXA_BC_HALO) {  // the low ghost cell is the left cell
+              fb.fL.push_back((int)(fb.ncells + lidx(x, y)));
+              fb.fR.push_back((int)c);
+              fb.fd.push_back((int8_t)d);
+            }
+          }
+    if (ngrids > 1) fb.cell_grid.insert(fb.cell_grid.end(), (size_t)(nc[0] * (long long)nc[1] * nc[2]), g);
+  }
+  return EXA_OK;
+}
+}  // namespace
+
+extern "C" int exa_build_face_lists(int dim, int ngrids, const exa_grid_desc* grids, exa_face_lists* out) {
+  if (!grids || !out || ngrids <= 0 || (dim != 2 && dim != 3)) return fail(EXA_ERR_INVALID, "bad argument");
+  FaceBuild fb;
+  if (int r = build_faces(dim, ngrids, grids, fb)) return r;
+  const bool fill = out->left != nullptr;
+  if (fill && (out->nfaces < (int)fb.fL.size() || out->nbfaces < (int)fb.bc.size()))
+    return fail(EXA_ERR_INVALID, "face arrays too small");
+  out->ncells = fb.ncells;
+  out->nghost = fb.nghost;
+  out->nfaces = (int)fb.fL.size();
+  out->nbfaces = (int)fb.bc.size();
+  if (fill) {
+    std::copy(fb.fL.begin(), fb.fL.end(), out->left);
+    std::copy(fb.fR.begin(), fb.fR.end(), out->right);
+    std::copy(fb.fd.begin(), fb.fd.end(), reinterpret_cast<int8_t*>(out->dir));
+    if (out->bcell) std::copy(fb.bc.begin(), fb.bc.end(), out->bcell);
+    if (out->bface) std::copy(fb.bf.begin(), fb.bf.end(), reinterpret_cast<int8_t*>(out->bface));
+  }
+  return EXA_OK;
+}
+
 extern "C" {
 
 int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_patch** out) {
@@ -630,53 +743,24 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   std::unique_ptr<exa_patch> p(new exa_patch());
   p->s = s;
   p->grids.assign(grids, grids + ngrids);
-  std::vector<int> hcell_grid;
-  std::vector<int> fL, fR, bc;
-  std::vector<int8_t> fd, bf;
-  std::vector<double> hdx(3 * ngrids);
-  long long c0 = 0;
-  for (int g = 0; g < ngrids; g++) {
-    const exa_grid_desc& G = grids[g];
-    int nc[3] = {G.ncell[0], G.ncell[1], dim == 3 ? G.ncell[2] : 1};
-    for (int d = 0; d < dim; d++) {
-      if (nc[d] <= 0 || !(G.size[d] > 0)) return fail(EXA_ERR_INVALID, "grid extents must be positive");
-      if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL) return fail(EXA_ERR_INVALID, "unknown boundary");
-      hdx[3 * g + d] = G.size[d] / nc[d];
-    }
-    for (int d = dim; d < 3; d++) hdx[3 * g + d] = 1.0;
-    const long long n = (long long)nc[0] * nc[1] * nc[2];
-    p->grid_first.push_back(c0);
-    auto idx = [&](int x, int y, int z) { return c0 + ((long long)z * nc[1] + y) * nc[0] + x; };
-    for (int d = 0; d < dim; d++)
-      for (int z = 0; z < nc[2]; z++)
-        for (int y = 0; y < nc[1]; y++)
-          for (int x = 0; x < nc[0]; x++) {
-            int j[3] = {x, y, z};
-            const int i_d = j[d];
-            j[d] += 1;
-            if (j[d] == nc[d]) {
-              if (G.bc[d] == EXA_BC_PERIODIC) {
-                j[d] = 0;
-              } else {
-                bc.push_back((int)idx(x, y, z));
-                bf.push_back((int8_t)(2 * d + 1));
-              }
-            }
-            if (j[d] < nc[d]) {
-              fL.push_back((int)idx(x, y, z));
-              fR.push_back((int)idx(j[0], j[1], j[2]));
-              fd.push_back((int8_t)d);
-            }
-            if (i_d == 0 && G.bc[d] == EXA_BC_WALL) {
-              bc.push_back((int)idx(x, y, z));
-              bf.push_back((int8_t)(2 * d));
-            }
-          }
-    if (ngrids > 1) hcell_grid.insert(hcell_grid.end(), (size_t)n, g);
-    c0 += n;
+  FaceBuild fb;
+  if (int r = build_faces(dim, ngrids, grids, fb)) return r;
+  std::vector<int>& hcell_grid = fb.cell_grid;
+  std::vector<int>& fL = fb.fL;
+  std::vector<int>& fR = fb.fR;
+  std::vector<int>& bc = fb.bc;
+  std::vector<int8_t>& fd = fb.fd;
+  std::vector<int8_t>& bf = fb.bf;
+  std::vector<double>& hdx = fb.dx;
+  p->grid_first = fb.first;
+  p->ncells = fb.ncells;
+  p->nghost = fb.nghost;
+  p->halo_axis = fb.halo_axis;
+  p->layer = fb.layer;
+  if (fb.halo_axis >= 0) {
+    p->halo_lo_first = 0;
+    p->halo_hi_first = fb.ncells - fb.layer;
   }
-  if (c0 > 0x7fffffffLL) return fail(EXA_ERR_INVALID, "too many cells for 32-bit face indices");
-  p->ncells = c0;
   p->nfaces = (int)fL.size();
   p->nbfaces = (int)bc.size();
   const exa::Ops& o = *s->ops;
@@ -694,8 +778,8 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   }
   EXA_ALLOC(p->luh, nc * o.sz_luh * sizeof(double));
   EXA_ALLOC(p->lduh, nc * o.sz_lduh * sizeof(double));
-  EXA_ALLOC(p->lQhbnd, nc * o.sz_qhb * sizeof(double));
-  EXA_ALLOC(p->lFhbnd, nc * o.sz_fhb * sizeof(double));
+  EXA_ALLOC(p->lQhbnd, (nc + p->nghost) * o.sz_qhb * sizeof(double));
+  EXA_ALLOC(p->lFhbnd, (nc + p->nghost) * o.sz_fhb * sizeof(double));
   EXA_ALLOC(p->picard, nc * sizeof(int));
   EXA_ALLOC(p->grid_dx, 3 * ngrids * sizeof(double));
   EXA_ALLOC(p->grid_t, ngrids * sizeof(double));
@@ -783,6 +867,8 @@ int exa_patch_get_solution(exa_patch* p, double* luh, int on_device) {
 
 int exa_patch_step(exa_patch* p, int nsteps, double fixed_dt) {
   if (!p || nsteps < 0) return fail(EXA_ERR_INVALID, "bad argument");
+  if (p->halo_axis >= 0)
+    return fail(EXA_ERR_INVALID, "a patch with EXA_BC_HALO steps through exa_patch_step_phase and a halo exchange");
   const bool cfl = !(fixed_dt > 0);
   if (!cfl && fixed_dt != p->fixed_dt) {
     const int ng = (int)p->grids.size();
@@ -843,6 +929,123 @@ int exa_patch_status(exa_patch* p, unsigned* bits) {
   EXA_CUDA(cudaMemcpyAsync(bits, p->status, sizeof(unsigned), cudaMemcpyDeviceToHost, p->stream));
   EXA_CUDA(cudaMemsetAsync(p->status, 0, sizeof(unsigned), p->stream));
   EXA_CUDA(cudaStreamSynchronize(p->stream));
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// step phases and halo exchange support (slab decomposition across devices)
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  const bool cfl = !(fixed_dt > 0);
+  const int ng = (int)p->grids.size();
+  if (!cfl && fixed_dt != p->fixed_dt) {
+    exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, fixed_dt);
+    EXA_CUDA(cudaGetLastError());
+    p->fixed_dt = fixed_dt;
+  }
+  switch (phase) {
+    case EXA_PHASE_PREDICTOR: {
+      exa::CellArgs a = patch_args(p);
+      EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+      return EXA_OK;
+    }
+    case EXA_PHASE_FACES: {
+      exa::FaceArgs f = patch_faces(p);
+      EXA_CUDA(p->s->ops->riemann(f, p->stream));
+      if (p->nbfaces > 0) {
+        exa::FaceArgs b = f;
+        b.nfaces = p->nbfaces;
+        EXA_CUDA(p->s->ops->boundary(b, p->stream));
+      }
+      return EXA_OK;
+    }
+    case EXA_PHASE_UPDATE: {
+      exa::CellArgs u = patch_args(p);
+      if (cfl) u.grid_dt_next = p->grid_dt_next;
+      EXA_CUDA(p->s->ops->update(u, true, true, p->stream));
+      return EXA_OK;
+    }
+    case EXA_PHASE_ADVANCE: {
+      exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt,
+                                                                   cfl ? p->grid_dt_next : p->grid_dt, p->steps);
+      EXA_CUDA(cudaGetLastError());
+      return EXA_OK;
+    }
+    default:
+      return fail(EXA_ERR_INVALID, "unknown phase");
+  }
+}
+
+long long exa_patch_halo_doubles(const exa_patch* p) {
+  if (!p || p->halo_axis < 0) return 0;
+  const exa::Ops& o = *p->s->ops;
+  const int nfaces = 2 * o.dim;
+  return p->layer * (long long)(o.sz_qhb / nfaces + o.sz_fhb / nfaces);
+}
+
+// one side's face traces: [Q of every layer cell][F of every layer cell]; 2D-pitched copies
+static int halo_copy(exa_patch* p, long long first_cell, int face, double* buf, bool to_buf) {
+  const exa::Ops& o = *p->s->ops;
+  const size_t fq = o.sz_qhb / (2 * o.dim), ff = o.sz_fhb / (2 * o.dim);
+  double* q = p->lQhbnd + first_cell * o.sz_qhb + face * fq;
+  double* f = p->lFhbnd + first_cell * o.sz_fhb + face * ff;
+  double* bq = buf;
+  double* bfl = buf + p->layer * fq;
+  if (to_buf) {
+    EXA_CUDA(cudaMemcpy2DAsync(bq, fq * sizeof(double), q, o.sz_qhb * sizeof(double), fq * sizeof(double),
+                               (size_t)p->layer, cudaMemcpyDeviceToDevice, p->stream));
+    EXA_CUDA(cudaMemcpy2DAsync(bfl, ff * sizeof(double), f, o.sz_fhb * sizeof(double), ff * sizeof(double),
+                               (size_t)p->layer, cudaMemcpyDeviceToDevice, p->stream));
+  } else {
+    EXA_CUDA(cudaMemcpy2DAsync(q, o.sz_qhb * sizeof(double), bq, fq * sizeof(double), fq * sizeof(double),
+                               (size_t)p->layer, cudaMemcpyDeviceToDevice, p->stream));
+    EXA_CUDA(cudaMemcpy2DAsync(f, o.sz_fhb * sizeof(double), bfl, ff * sizeof(double), ff * sizeof(double),
+                               (size_t)p->layer, cudaMemcpyDeviceToDevice, p->stream));
+  }
+  return EXA_OK;
+}
+
+int exa_patch_halo_pack(exa_patch* p, double* send_lo, double* send_hi) {
+  if (!p || p->halo_axis < 0) return fail(EXA_ERR_INVALID, "patch has no halo");
+  if (!send_lo || !send_hi) return fail(EXA_ERR_INVALID, "null buffer");
+  const int a = p->halo_axis;
+  // low real layer, its low face 2a; high real layer, its high face 2a+1
+  if (int r = halo_copy(p, p->halo_lo_first, 2 * a, send_lo, true)) return r;
+  return halo_copy(p, p->halo_hi_first, 2 * a + 1, send_hi, true);
+}
+
+int exa_patch_halo_unpack(exa_patch* p, const double* recv_lo, const double* recv_hi) {
+  if (!p || p->halo_axis < 0) return fail(EXA_ERR_INVALID, "patch has no halo");
+  if (!recv_lo || !recv_hi) return fail(EXA_ERR_INVALID, "null buffer");
+  const int a = p->halo_axis;
+  // recv_lo: the lower neighbour's high layer (face 2a+1) -> low ghost cells, face 2a+1
+  // recv_hi: the upper neighbour's low layer (face 2a)    -> high ghost cells, face 2a
+  if (int r = halo_copy(p, p->ncells, 2 * a + 1, const_cast<double*>(recv_lo), false)) return r;
+  return halo_copy(p, p->ncells + p->layer, 2 * a, const_cast<double*>(recv_hi), false);
+}
+
+int exa_patch_dt_copy(exa_patch* p, double* dev_buf, int to_patch) {
+  if (!p || !dev_buf) return fail(EXA_ERR_INVALID, "null argument");
+  const size_t bytes = p->grids.size() * sizeof(double);
+  if (to_patch)
+    EXA_CUDA(cudaMemcpyAsync(p->grid_dt, dev_buf, bytes, cudaMemcpyDeviceToDevice, p->stream));
+  else
+    EXA_CUDA(cudaMemcpyAsync(dev_buf, p->grid_dt, bytes, cudaMemcpyDeviceToDevice, p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_dt_next_copy(exa_patch* p, double* dev_buf, int to_patch) {
+  if (!p || !dev_buf) return fail(EXA_ERR_INVALID, "null argument");
+  const size_t bytes = p->grids.size() * sizeof(double);
+  if (to_patch)
+    EXA_CUDA(cudaMemcpyAsync(p->grid_dt_next, dev_buf, bytes, cudaMemcpyDeviceToDevice, p->stream));
+  else
+    EXA_CUDA(cudaMemcpyAsync(dev_buf, p->grid_dt_next, bytes, cudaMemcpyDeviceToDevice, p->stream));
   return EXA_OK;
 }
 

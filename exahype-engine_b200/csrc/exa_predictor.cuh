@@ -183,7 +183,10 @@ predictor_kernel(CellArgs a) {
     for (int r = 0; r < S::rounds; r++) {
       const int pk = it_pack[r];
       if (pk < 0) continue;
-      float* f = sFf + (pk & 0x3ffff);
+      // the packed offset counts doubles; the float view of cell c's flux block starts at float
+      // index 2*c*DIM*V*BS (the floats of every cell sit in the first half of its own block)
+      const int bd = pk & 0x3ffff;
+      float* f = sFf + bd + (bd / (DIM * V * BS)) * (DIM * V * BS);
       const int dd = (pk >> 18) & 3;
       const int st = dd == 0 ? 1 : (dd == 1 ? n : n * n);
       const float coef = wi * (float)s_lw[(unsigned)pk >> 20];

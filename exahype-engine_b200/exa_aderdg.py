@@ -49,6 +49,16 @@ class GridDesc(ctypes.Structure):
                 ("bc", ctypes.c_int * 3)]
 
 
+class FaceLists(ctypes.Structure):
+    _fields_ = [("ncells", ctypes.c_longlong), ("nghost", ctypes.c_longlong), ("nfaces", ctypes.c_int),
+                ("nbfaces", ctypes.c_int), ("left", ctypes.c_void_p), ("right", ctypes.c_void_p),
+                ("dir", ctypes.c_void_p), ("bcell", ctypes.c_void_p), ("bface", ctypes.c_void_p)]
+
+
+PHASE_PREDICTOR, PHASE_FACES, PHASE_UPDATE, PHASE_ADVANCE = 0, 1, 2, 3
+BC_HALO = 2
+
+
 class _PatchStats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_longlong), ("picard_mean", ctypes.c_double), ("picard_hist", ctypes.c_int * 32)]
 
@@ -92,6 +102,12 @@ def load_library(path=None):
         "exa_patch_time": [vp, dp, dp],
         "exa_patch_stats_get": [vp, ctypes.POINTER(_PatchStats)],
         "exa_patch_status": [vp, ctypes.POINTER(ctypes.c_uint)],
+        "exa_patch_step_phase": [vp, i, d],
+        "exa_patch_halo_pack": [vp, vp, vp],
+        "exa_patch_halo_unpack": [vp, vp, vp],
+        "exa_patch_dt_next_copy": [vp, vp, i],
+        "exa_patch_dt_copy": [vp, vp, i],
+        "exa_build_face_lists": [i, i, ctypes.POINTER(GridDesc), ctypes.POINTER(FaceLists)],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -103,6 +119,8 @@ def load_library(path=None):
     lib.exa_patch_luh.restype = ctypes.c_void_p
     lib.exa_patch_stream.argtypes = [vp]
     lib.exa_patch_stream.restype = ctypes.c_void_p
+    lib.exa_patch_halo_doubles.argtypes = [vp]
+    lib.exa_patch_halo_doubles.restype = ctypes.c_longlong
     _lib = lib
     return lib
 
@@ -245,6 +263,42 @@ class Solver:
         return out.value
 
 
+def grid_descs(grids):
+    """ctypes array of exa_grid_desc from dicts {ncell, size, offset=0, bc=periodic (or per axis)}."""
+    arr = (GridDesc * len(grids))()
+    for g, spec in zip(arr, grids):
+        nc = list(spec["ncell"]) + [1] * (3 - len(spec["ncell"]))
+        sz = list(spec["size"]) + [1.0] * (3 - len(spec["size"]))
+        off = list(spec.get("offset", [0.0] * 3)) + [0.0] * 3
+        bc = spec.get("bc", BC_PERIODIC)
+        bcs = list(bc) if hasattr(bc, "__len__") else [bc] * 3
+        bcs = bcs + [BC_PERIODIC] * (3 - len(bcs))
+        for k in range(3):
+            g.ncell[k] = int(nc[k])
+            g.size[k] = float(sz[k])
+            g.offset[k] = float(off[k])
+            g.bc[k] = int(bcs[k])
+    return arr
+
+
+def build_face_lists(dim, grids):
+    """Host-only: the face lists exa_patch_create builds for these grids (numpy arrays)."""
+    lib = load_library()
+    arr = grid_descs(grids)
+    fl = FaceLists()
+    _check(lib.exa_build_face_lists(dim, len(grids), arr, ctypes.byref(fl)), "exa_build_face_lists")
+    left = np.zeros(fl.nfaces, dtype=np.int32)
+    right = np.zeros(fl.nfaces, dtype=np.int32)
+    d = np.zeros(fl.nfaces, dtype=np.int8)
+    bcell = np.zeros(max(fl.nbfaces, 1), dtype=np.int32)
+    bface = np.zeros(max(fl.nbfaces, 1), dtype=np.int8)
+    fl.left, fl.right, fl.dir = _np_ptr(left), _np_ptr(right), _np_ptr(d)
+    fl.bcell, fl.bface = _np_ptr(bcell), _np_ptr(bface)
+    _check(lib.exa_build_face_lists(dim, len(grids), arr, ctypes.byref(fl)), "exa_build_face_lists")
+    return {"ncells": fl.ncells, "nghost": fl.nghost, "left": left, "right": right, "dir": d,
+            "bcell": bcell[:fl.nbfaces], "bface": bface[:fl.nbfaces]}
+
+
 class Patch:
     """Device-resident uniform grid(s); the step is one CUDA graph launch."""
 
@@ -252,24 +306,30 @@ class Patch:
         """grids: list of dicts {ncell, size, offset=0, bc=periodic} (bc per axis)."""
         self.solver = solver
         self.lib = solver.lib
-        arr = (GridDesc * len(grids))()
-        for g, spec in zip(arr, grids):
-            nc = list(spec["ncell"]) + [1] * (3 - len(spec["ncell"]))
-            sz = list(spec["size"]) + [1.0] * (3 - len(spec["size"]))
-            off = list(spec.get("offset", [0.0] * 3)) + [0.0] * 3
-            bc = spec.get("bc", BC_PERIODIC)
-            bcs = list(bc) if hasattr(bc, "__len__") else [bc] * 3
-            bcs = bcs + [BC_PERIODIC] * (3 - len(bcs))
-            for k in range(3):
-                g.ncell[k] = int(nc[k])
-                g.size[k] = float(sz[k])
-                g.offset[k] = float(off[k])
-                g.bc[k] = int(bcs[k])
+        arr = grid_descs(grids)
         h = ctypes.c_void_p()
         _check(self.lib.exa_patch_create(solver.h, len(grids), arr, ctypes.byref(h)), "exa_patch_create")
         self.h = h
         self.ngrids = len(grids)
         self.ncells = int(self.lib.exa_patch_num_cells(self.h))
+
+    def step_phase(self, phase, fixed_dt=0.0):
+        _check(self.lib.exa_patch_step_phase(self.h, int(phase), float(fixed_dt)), "exa_patch_step_phase")
+
+    def halo_doubles(self):
+        return int(self.lib.exa_patch_halo_doubles(self.h))
+
+    def halo_pack(self, send_lo, send_hi):
+        _check(self.lib.exa_patch_halo_pack(self.h, _ptr(send_lo), _ptr(send_hi)), "exa_patch_halo_pack")
+
+    def halo_unpack(self, recv_lo, recv_hi):
+        _check(self.lib.exa_patch_halo_unpack(self.h, _ptr(recv_lo), _ptr(recv_hi)), "exa_patch_halo_unpack")
+
+    def dt_next_copy(self, buf, to_patch):
+        _check(self.lib.exa_patch_dt_next_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_next_copy")
+
+    def dt_copy(self, buf, to_patch):
+        _check(self.lib.exa_patch_dt_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_copy")
 
     def close(self):
         if getattr(self, "h", None):

@@ -120,3 +120,45 @@ def l2_linf_error(luh, exact, order, dim, nvar_out=1, nvar=5):
     ncells = a.shape[0]
     e2 = ((a - b) ** 2 * wn[None, :, None]).sum() / ncells
     return float(np.sqrt(e2)), float(np.max(np.abs(a - b)))
+
+
+# ------------------------------------------------------------------------------------------
+# Batched shallow water: many independent grids of uneven sizes
+# ------------------------------------------------------------------------------------------
+
+def swe_grid_specs(ngrids=512, seed=0, nmin=16, nmax=128):
+    """Per-grid square sizes drawn uniformly from nmin..nmax cells per side, unit square each."""
+    rng = np.random.default_rng(seed)
+    sides = rng.integers(nmin, nmax + 1, size=ngrids)
+    return [dict(ncell=(int(s), int(s)), size=[1.0, 1.0]) for s in sides]
+
+
+def swe_bumps_state(ncell, order, rng):
+    """h = 1 + 1..5 circular bumps (height U[0.2,1], radius U[0.05,0.2]), zero velocity,
+    bathymetry b = 0.1 * a smooth random field; (h, hu, hv, b) per node."""
+    x = nodal_positions(ncell, [1.0, 1.0], order)  # [cells][nodes][2]
+    nb = int(rng.integers(1, 6))
+    h = np.ones(x.shape[:-1])
+    for _ in range(nb):
+        c = rng.uniform(0.2, 0.8, 2)
+        hgt = rng.uniform(0.2, 1.0)
+        rad = rng.uniform(0.05, 0.2)
+        r2 = ((x - c) ** 2).sum(-1)
+        h += hgt * np.exp(-r2 / (rad * rad))
+    kx, ky = rng.integers(1, 4, 2)
+    ph = rng.uniform(0, 2 * np.pi, 2)
+    b = 0.1 * 0.5 * (np.cos(2 * np.pi * kx * x[..., 0] + ph[0]) * np.cos(2 * np.pi * ky * x[..., 1] + ph[1]) + 1.0)
+    Q = np.zeros(x.shape[:-1] + (4,))
+    Q[..., 0] = h
+    Q[..., 3] = b
+    return Q.reshape(-1)
+
+
+def swe_batched(ngrids=512, order=4, seed=0, nmin=16, nmax=128):
+    """Grid specs (reflective walls) and the concatenated initial state of every grid."""
+    specs = swe_grid_specs(ngrids, seed, nmin, nmax)
+    rng = np.random.default_rng(seed + 1)
+    states = [swe_bumps_state(sp["ncell"], order, rng) for sp in specs]
+    for sp in specs:
+        sp["bc"] = 1  # reflective walls on every side
+    return specs, states

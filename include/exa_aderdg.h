@@ -59,7 +59,10 @@ typedef enum {
   EXA_PREC_MIXED = 1  /* early Picard sweeps in FP32, final sweep + residual test + update in FP64 */
 } exa_precision;
 
-typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1 } exa_bc;
+/* EXA_BC_HALO (last axis of a single-grid patch only): the two boundary layers face ghost
+ * cells whose face traces a neighbouring subdomain supplies (slab decomposition, see
+ * exa_patch_halo_pack / exa_patch_halo_unpack). */
+typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1, EXA_BC_HALO = 2 } exa_bc;
 
 /* Compile-time constants of the reference's generated solver (AbstractGenericADERDGSolverHeader
  * .template:34-68), here runtime fields of a solver handle. */
@@ -225,6 +228,42 @@ int exa_patch_track_picard(exa_patch* p, int on);
 int exa_patch_stats_get(exa_patch* p, exa_patch_stats* st);
 int exa_patch_status(exa_patch* p, unsigned* bits);       /* reads and clears (synchronises) */
 void* exa_patch_stream(exa_patch* p);                     /* the cudaStream_t the patch runs on */
+
+/* ---- one step in phases, for subdomains that exchange face traces ---------------------------
+ * The reference exchanges the face data of cells next to a remote rank by MPI
+ * (ADERDGSolver::sendDataToNeighbour / mergeWithNeighbourData, ADERDGSolver.cpp:1946-2010) and
+ * reduces the admissible time step over ranks. Here a rank's patch carries EXA_BC_HALO on its last
+ * axis; one step is
+ *   PREDICTOR -> halo_pack -> (exchange with the two neighbours) -> halo_unpack -> FACES ->
+ *   UPDATE -> (all-reduce min of dt_next, exa_patch_dt_next_copy) -> ADVANCE.
+ * exa_patch_step refuses halo patches. All calls enqueue on the patch stream. */
+enum { EXA_PHASE_PREDICTOR = 0, EXA_PHASE_FACES = 1, EXA_PHASE_UPDATE = 2, EXA_PHASE_ADVANCE = 3 };
+int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt);
+/* doubles in one side's exchange buffer: [lQhbnd face blocks of the layer][lFhbnd face blocks] */
+long long exa_patch_halo_doubles(const exa_patch* p);
+/* send_lo: the low boundary layer's low faces; send_hi: the high layer's high faces (device) */
+int exa_patch_halo_pack(exa_patch* p, double* send_lo, double* send_hi);
+/* recv_lo: what the lower neighbour packed as send_hi; recv_hi: the upper neighbour's send_lo */
+int exa_patch_halo_unpack(exa_patch* p, const double* recv_lo, const double* recv_hi);
+/* copy the per-grid CFL minimum of the last UPDATE phase to (to_patch=0) or from (1) a device buffer */
+int exa_patch_dt_next_copy(exa_patch* p, double* dev_buf, int to_patch);
+/* the same for the time step in use (after exa_patch_set_solution: the local CFL minimum) */
+int exa_patch_dt_copy(exa_patch* p, double* dev_buf, int to_patch);
+
+/* Host-only (no device work): the face lists a patch of these grids uses. With out->left == NULL
+ * only the counts are filled; otherwise the caller's arrays (nfaces / nbfaces entries, sizes given
+ * in out->nfaces / out->nbfaces) receive the lists. Ghost cells of a halo axis are numbered after
+ * the real cells: the low ghost layer, then the high one. */
+typedef struct {
+  long long ncells, nghost;
+  int nfaces, nbfaces;
+  int* left;
+  int* right;
+  signed char* dir;
+  int* bcell;
+  signed char* bface;
+} exa_face_lists;
+int exa_build_face_lists(int dim, int ngrids, const exa_grid_desc* grids, exa_face_lists* out);
 
 #ifdef __cplusplus
 }

@@ -314,3 +314,86 @@ def test_mixed_precision_patch_vs_fp64_oracle(exa, dim, order, ncell, steps):
 def test_mixed_precision_rejected_for_ncp(exa):
     with pytest.raises(exa.ExaError):
         exa.Solver(exa.PDE_SWE, 2, 4, precision=exa.PREC_MIXED)
+
+
+def test_swe_batched_grids_vs_oracle(exa):
+    """Batched shallow water: several wall-bounded grids of uneven sizes in one patch, each with
+    its own CFL time step, against the oracle run grid by grid."""
+    import exa_scenarios as sc
+    specs, states = sc.swe_batched(ngrids=5, order=4, seed=3, nmin=6, nmax=14)
+    s = exa.Solver(exa.PDE_SWE, 2, 4)
+    p = exa.Patch(s, specs)
+    p.set_solution(np.concatenate(states))
+    p.step(4)
+    got = p.get_solution()
+    t, _ = p.time()
+    o = Oracle(2, 4, pde=PDE_SWE)
+    off = 0
+    for g, (sp, st) in enumerate(zip(specs, states)):
+        ref = st.copy()
+        t_ref, _, _ = o.run(ref, sp["ncell"], sp["size"], 4, walls=True)
+        assert rel(got[off:off + ref.size], ref) < TOL, g
+        assert abs(t[g] - t_ref) <= 1e-13 * t_ref
+        off += ref.size
+    assert p.status() == 0
+
+
+@pytest.mark.parametrize("nz,split", [(6, 3), (5, 2)])
+def test_two_slabs_with_halo_match_whole_grid(exa, torch, nz, split):
+    """The slab-decomposition path on one GPU: two halo patches (lower and upper slab of a periodic
+    grid) advanced phase by phase, with the host copying the exchange buffers between them, give
+    the same state as one whole-grid patch (the exchange a multi-GPU run does with NCCL)."""
+    rng = np.random.default_rng(8)
+    order, nx, ny = 3, 3, 4
+    nd = (order + 1) ** 3
+    size = [1.0, 0.9, 1.1]
+    hz = size[2] / nz
+    luh0 = euler_cells(rng, nx * ny * nz, nd, amp=0.04).reshape(-1)
+    s = exa.Solver(exa.PDE_EULER, 3, order)
+    whole = exa.Patch(s, [dict(ncell=(nx, ny, nz), size=size)])
+    whole.set_solution(luh0)
+    whole.step(3)
+    ref = whole.get_solution()
+    layer = nx * ny * nd * 5
+    slabs = []
+    for first, count in ((0, split), (split, nz - split)):
+        p = exa.Patch(s, [dict(ncell=(nx, ny, count), size=[size[0], size[1], count * hz],
+                               offset=[0, 0, first * hz], bc=[exa.BC_PERIODIC, exa.BC_PERIODIC, exa.BC_HALO])])
+        p.set_solution(luh0[first * layer:(first + count) * layer])
+        nh = p.halo_doubles()
+        bufs = {k: torch.zeros(nh, dtype=torch.float64, device="cuda") for k in ("slo", "shi", "rlo", "rhi")}
+        slabs.append((p, bufs))
+    dtb = [torch.zeros(1, dtype=torch.float64, device="cuda") for _ in slabs]
+    with pytest.raises(exa.ExaError):
+        slabs[0][0].step(1)  # halo patches refuse the single-device step
+    for (p, _), b in zip(slabs, dtb):
+        p.dt_copy(b, 0)
+    torch.cuda.synchronize()
+    m = torch.minimum(dtb[0], dtb[1])
+    for (p, _), b in zip(slabs, dtb):
+        b.copy_(m)
+        p.dt_copy(b, 1)
+    for _ in range(3):
+        for p, bf in slabs:
+            p.step_phase(exa.PHASE_PREDICTOR)
+            p.halo_pack(bf["slo"], bf["shi"])
+        torch.cuda.synchronize()
+        (pa, a), (pb, b) = slabs
+        a["rlo"].copy_(b["shi"]); a["rhi"].copy_(b["slo"])  # periodic: each slab is the other's both neighbours
+        b["rlo"].copy_(a["shi"]); b["rhi"].copy_(a["slo"])
+        torch.cuda.synchronize()
+        for p, bf in slabs:
+            p.halo_unpack(bf["rlo"], bf["rhi"])
+            p.step_phase(exa.PHASE_FACES)
+            p.step_phase(exa.PHASE_UPDATE)
+        for (p, _), bb in zip(slabs, dtb):
+            p.dt_next_copy(bb, 0)
+        torch.cuda.synchronize()
+        m = torch.minimum(dtb[0], dtb[1])
+        for (p, _), bb in zip(slabs, dtb):
+            bb.copy_(m)
+            p.dt_next_copy(bb, 1)
+            p.step_phase(exa.PHASE_ADVANCE)
+    got = np.concatenate([p.get_solution() for p, _ in slabs])
+    assert rel(got, ref) < TOL
+    assert slabs[0][0].time()[0][0] == whole.time()[0][0]
