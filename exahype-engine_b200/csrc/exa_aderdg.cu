@@ -66,7 +66,9 @@ template <class PDE, int DIM, int N, int P>
 struct OpsImpl final : Ops {
   using S = Shape<PDE, DIM, N, P>;
   bool smem_set = false, smem_set_mixed = false;
-  static constexpr bool kMixed = !PDE::kNCP;
+  // the mixed form needs PDEs without NCP and its larger shared-memory footprint must fit a CTA
+  static constexpr bool kMixed = !PDE::kNCP && S::predictor_smem_mixed + 4096 <= 227 * 1024;
+  static_assert(S::predictor_smem + 4096 <= 227 * 1024, "predictor shared memory exceeds one CTA");
   template <bool M>
   cudaError_t launch_predictor(const CellArgs& a, cudaStream_t st, bool& set) {
     constexpr bool MM = M && kMixed;
@@ -147,6 +149,9 @@ Ops* find_ops(int pde, int dim, int order, int npar) {
   EXA_CASE(EXA_PDE_EULER, EulerPDE, 2, 3, 0)
   EXA_CASE(EXA_PDE_EULER, EulerPDE, 2, 3, 1)
   EXA_CASE(EXA_PDE_SWE, SWEPDE, 2, 4, 0)
+  EXA_CASE(EXA_PDE_ACOUSTIC, AcousticPDE, 3, 4, 2)
+  EXA_CASE(EXA_PDE_ELASTIC, ElasticPDE, 3, 3, 3)
+  EXA_CASE(EXA_PDE_ELASTIC, ElasticPDE, 3, 4, 3)
 #undef EXA_CASE
   return nullptr;
 }
@@ -538,6 +543,10 @@ struct exa_patch {
   cudaGraphExec_t graph_cfl = nullptr, graph_fixed = nullptr;
   bool track_picard = false;
   double fixed_dt = -1.0;
+  double* grid_geo = nullptr;       // [grid][6]: lower corner, cells per axis
+  long long* grid_first_d = nullptr; // [grid] first cell
+  double* src = nullptr;            // point source parameters (8 doubles), nullptr when unset
+  int8_t* btype = nullptr;          // boundary type of every domain face
   // halo (slab decomposition): ghost cells appended after the real cells, face traces only
   long long nghost = 0;      // 2 * layer cells, or 0
   int halo_axis = -1;        // axis with EXA_BC_HALO
@@ -549,7 +558,8 @@ static void patch_free(exa_patch* p) {
   if (p->graph_cfl) cudaGraphExecDestroy(p->graph_cfl);
   if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
   void* ptrs[] = {p->luh, p->lduh, p->lQhbnd, p->lFhbnd, p->picard, p->cell_grid, p->grid_dx, p->grid_t,
-                  p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status};
+                  p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status,
+                  p->grid_geo, p->grid_first_d, p->src, p->btype};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -567,6 +577,10 @@ static exa::CellArgs patch_args(exa_patch* p) {
   a.cell_grid = p->grids.size() > 1 ? p->cell_grid : nullptr;
   a.grid_dx = p->grid_dx;
   a.grid_dt = p->grid_dt;
+  a.grid_t = p->grid_t;
+  a.grid_geo = p->grid_geo;
+  a.grid_first = p->grid_first_d;
+  a.src = p->src;
   return a;
 }
 
@@ -581,6 +595,7 @@ static exa::FaceArgs patch_faces(exa_patch* p) {
   f.lFhbnd = p->lFhbnd;
   f.bcell = p->bcell;
   f.bface = p->bface;
+  f.btype = p->btype;
   return f;
 }
 
@@ -631,7 +646,7 @@ struct FaceBuild {
   long long ncells = 0, nghost = 0, layer = 0;
   int halo_axis = -1;
   std::vector<int> cell_grid, fL, fR, bc;
-  std::vector<int8_t> fd, bf;
+  std::vector<int8_t> fd, bf, bt;
   std::vector<double> dx;
   std::vector<long long> first;
 };
@@ -648,7 +663,8 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
     int nc[3] = {G.ncell[0], G.ncell[1], dim == 3 ? G.ncell[2] : 1};
     for (int d = 0; d < dim; d++) {
       if (nc[d] <= 0 || !(G.size[d] > 0)) return fail(EXA_ERR_INVALID, "grid extents must be positive");
-      if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL && G.bc[d] != EXA_BC_HALO)
+      if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL && G.bc[d] != EXA_BC_HALO &&
+          G.bc[d] != EXA_BC_OUTFLOW)
         return fail(EXA_ERR_INVALID, "unknown boundary");
       if (G.bc[d] == EXA_BC_HALO && (d != dim - 1 || ngrids != 1))
         return fail(EXA_ERR_INVALID, "EXA_BC_HALO is supported on the last axis of a single-grid patch");
@@ -683,9 +699,10 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
             if (j[d] == nc[d]) {
               if (G.bc[d] == EXA_BC_PERIODIC) {
                 j[d] = 0;
-              } else if (G.bc[d] == EXA_BC_WALL) {
+              } else if (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW) {
                 fb.bc.push_back((int)c);
                 fb.bf.push_back((int8_t)(2 * d + 1));
+                fb.bt.push_back((int8_t)G.bc[d]);
               } else {  // halo: the high ghost cell of this column is the right cell
                 fb.fL.push_back((int)c);
                 fb.fR.push_back((int)(fb.ncells + fb.layer + lidx(x, y)));
@@ -697,9 +714,10 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
               fb.fR.push_back((int)idx(j[0], j[1], j[2]));
               fb.fd.push_back((int8_t)d);
             }
-            if (i_d == 0 && G.bc[d] == EXA_BC_WALL) {
+            if (i_d == 0 && (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW)) {
               fb.bc.push_back((int)c);
               fb.bf.push_back((int8_t)(2 * d));
+              fb.bt.push_back((int8_t)G.bc[d]);
             }
             if (i_d == 0 && G.bc[d] == EXA_BC_HALO) {  // the low ghost cell is the left cell
               fb.fL.push_back((int)(fb.ncells + lidx(x, y)));
@@ -793,6 +811,9 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   EXA_ALLOC(p->bcell, bc.size() * sizeof(int));
   EXA_ALLOC(p->bface, bf.size());
   if (ngrids > 1) EXA_ALLOC(p->cell_grid, hcell_grid.size() * sizeof(int));
+  EXA_ALLOC(p->grid_geo, 6 * ngrids * sizeof(double));
+  EXA_ALLOC(p->grid_first_d, ngrids * sizeof(long long));
+  EXA_ALLOC(p->btype, fb.bt.size() + 1);
 #undef EXA_ALLOC
   cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
@@ -800,7 +821,17 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
     return cuda_fail(e, "cudaStreamCreate");
   }
   std::vector<double> zeros(ngrids, 0.0);
-  bool ok = cudaMemcpy(p->grid_dx, hdx.data(), hdx.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+  std::vector<double> geo(6 * ngrids);
+  for (int g = 0; g < ngrids; g++)
+    for (int k = 0; k < 3; k++) {
+      geo[6 * g + k] = grids[g].offset[k];
+      geo[6 * g + 3 + k] = (k < dim) ? grids[g].ncell[k] : 1;
+    }
+  bool ok = cudaMemcpy(p->grid_geo, geo.data(), geo.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
+            cudaMemcpy(p->grid_first_d, fb.first.data(), ngrids * sizeof(long long), cudaMemcpyHostToDevice) ==
+                cudaSuccess &&
+            (fb.bt.empty() || cudaMemcpy(p->btype, fb.bt.data(), fb.bt.size(), cudaMemcpyHostToDevice) == cudaSuccess);
+  ok = ok && cudaMemcpy(p->grid_dx, hdx.data(), hdx.size() * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(p->grid_t, zeros.data(), ngrids * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemcpy(p->grid_dt, zeros.data(), ngrids * sizeof(double), cudaMemcpyHostToDevice) == cudaSuccess &&
             cudaMemset(p->steps, 0, sizeof(long long)) == cudaSuccess &&
@@ -1027,6 +1058,29 @@ int exa_patch_halo_unpack(exa_patch* p, const double* recv_lo, const double* rec
   // recv_hi: the upper neighbour's low layer (face 2a)    -> high ghost cells, face 2a
   if (int r = halo_copy(p, p->ncells, 2 * a + 1, const_cast<double*>(recv_lo), false)) return r;
   return halo_copy(p, p->ncells + p->layer, 2 * a, const_cast<double*>(recv_hi), false);
+}
+
+int exa_patch_set_point_source(exa_patch* p, const exa_point_source* src) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  if (!src) {
+    EXA_CUDA(cudaStreamSynchronize(p->stream));
+    if (p->src) cudaFree(p->src);
+    p->src = nullptr;
+  } else {
+    if (src->variable < 0 || src->variable >= p->s->ops->nvar) return fail(EXA_ERR_INVALID, "source variable");
+    if (!(src->width > 0)) return fail(EXA_ERR_INVALID, "source width must be positive");
+    if (!p->src) EXA_CUDA(cudaMalloc(&p->src, 8 * sizeof(double)));
+    const double h[8] = {src->x[0], src->x[1], src->x[2], src->f0, src->t0, src->amplitude, src->width,
+                         (double)src->variable};
+    // ordered after any step still running on the patch's stream
+    EXA_CUDA(cudaMemcpyAsync(p->src, h, sizeof(h), cudaMemcpyHostToDevice, p->stream));
+    EXA_CUDA(cudaStreamSynchronize(p->stream));
+  }
+  // the captured step graphs hold the old pointer: rebuild them on the next step
+  if (p->graph_cfl) cudaGraphExecDestroy(p->graph_cfl);
+  if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
+  p->graph_cfl = p->graph_fixed = nullptr;
+  return EXA_OK;
 }
 
 int exa_patch_dt_copy(exa_patch* p, double* dev_buf, int to_patch) {

@@ -58,12 +58,9 @@ struct Shape {
   static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
   static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF + smemU);
   static constexpr size_t predictor_smem_mixed = sizeof(double) * (smemQ + smemF + smemU + smemO);
-  // resident predictor CTAs per SM the register allocation is bounded for (shared memory
-  // allows two CTAs of 3D N=5 Euler cells: 2 x 77.8 KB)
-#ifndef EXA_PRED_MINBLOCKS
-#define EXA_PRED_MINBLOCKS 2
-#endif
-  static constexpr int MinBlocks = EXA_PRED_MINBLOCKS;
+  // two resident CTAs per SM when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
+  static constexpr int MinBlocks =
+      2 * (sizeof(double) * (smemQ + smemF + smemU + smemO) + 3 * 1024) <= 228 * 1024 ? 2 : 1;
   // registers are split over the SM's four 16K-register partitions: B blocks of W warps need
   // ceil(B*W/4) warps' worth of registers in one partition
   static constexpr int WarpsPerSmsp = (MinBlocks * (TPB / 32) + 3) / 4;
@@ -89,6 +86,12 @@ struct CellArgs {
   unsigned* status;         // error bits (nullable)
   int max_picard;           // 0: residual test, 2(N+1) cap; > 0: fixed sweep count
   double cfl_pnpm;          // CFL * PNPM
+  // point source (nullable): {x, y, z, f0, t0, amplitude, width, variable}; needs the geometry
+  const double* src;
+  const double* grid_geo;        // [grid][6]: lower corner xyz, cells per axis xyz
+  const long long* grid_first;   // [grid] first cell of the grid in the batch
+  const double* grid_t;          // [grid] time at the start of the step (nullable: u_t)
+  double u_t;
   // optional export of the predictor's internals, reference layouts (per-cell shims, tests)
   double* ex_lQi;
   double* ex_lFi;
@@ -141,6 +144,44 @@ __device__ __forceinline__ int node_line(int p, int dir) {
 template <class T>
 __device__ __forceinline__ bool finite(T x) { return isfinite(x); }
 
+// Regularised point source S_var(x, t) = A r(t - t0) exp(-|x - xs|^2 / (2 w^2)) / ((2 pi)^(d/2) w^d)
+// with the Ricker wavelet r(s) = (1 - 2 pi^2 f0^2 s^2) exp(-pi^2 f0^2 s^2); the pointwise
+// algebraicSource(x, t, Q, S) of the reference's solver API for a source at xs.
+template <int DIM>
+__device__ __forceinline__ double point_source(const double* src, const double* x, double t) {
+  const double pi = 3.14159265358979323846;
+  double r2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) r2 += (x[d] - src[d]) * (x[d] - src[d]);
+  const double w = src[6];
+  const double a = pi * src[3] * (t - src[4]);
+  const double ricker = (1.0 - 2.0 * a * a) * exp(-a * a);
+  const double norm = DIM == 3 ? 1.0 / (15.749609945722419 * w * w * w) : 1.0 / (6.283185307179586 * w * w);
+  return src[5] * ricker * exp(-0.5 * r2 / (w * w)) * norm;
+}
+// The source acts on cells whose centre lies within 6 widths plus a cell diagonal of xs.
+template <int DIM>
+__device__ __forceinline__ bool source_near(const double* src, const double* centre, const double* dx) {
+  double r2 = 0.0, h2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    r2 += (centre[d] - src[d]) * (centre[d] - src[d]);
+    h2 += dx[d] * dx[d];
+  }
+  const double reach = 6.0 * src[6] + sqrt(h2);
+  return r2 <= reach * reach;
+}
+// centre of cell `cell` of grid g from the grid geometry
+__device__ __forceinline__ void cell_centre(const CellArgs& a, long cell, int g, const double* dx, double* c) {
+  const double* G = a.grid_geo + 6 * g;
+  const long long loc = cell - (a.grid_first ? a.grid_first[g] : 0);
+  const long long nx = (long long)G[3], ny = (long long)G[4];
+  const long long ix = loc % nx, iy = (loc / nx) % ny, iz = loc / (nx * ny);
+  c[0] = G[0] + (ix + 0.5) * dx[0];
+  c[1] = G[1] + (iy + 0.5) * dx[1];
+  c[2] = G[2] + (iz + 0.5) * dx[2];
+}
+
 __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
   // non-negative doubles order like their bit patterns
   atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
@@ -155,6 +196,18 @@ namespace exa {
 // ------------------------------------------------------------------------------------------
 // Rusanov on interior faces: one warp per face, in place on lFhbnd
 // ------------------------------------------------------------------------------------------
+// Ghost state of a domain face (boundaryValues): a reflective wall mirrors the normal velocity;
+// normal < 0 selects outflow, the inner state itself (transparent / absorbing for normal waves).
+template <class PDE, int DIM, int D>
+__device__ __forceinline__ void ghost_state(const double* qin, int normal, double* qout) {
+  if (normal < 0) {
+#pragma unroll
+    for (int m = 0; m < D; m++) qout[m] = qin[m];
+  } else {
+    PDE::template wall<DIM>(qin, normal, qout);
+  }
+}
+
 template <class PDE, int DIM, int N, int P>
 __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR, double* FL, double* FR, int d,
                                              int lane, bool ghostL, bool ghostR, int ghost_normal) {
@@ -173,8 +226,8 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
       ql[m] = QL[fn * D + m];
       qr[m] = QR[fn * D + m];
     }
-    if (ghostL) PDE::template wall<DIM>(qr, ghost_normal, ql);
-    if (ghostR) PDE::template wall<DIM>(ql, ghost_normal, qr);
+    if (ghostL) ghost_state<PDE, DIM, D>(qr, ghost_normal, ql);
+    if (ghostR) ghost_state<PDE, DIM, D>(ql, ghost_normal, qr);
     if (ghostL || ghostR) {
 #pragma unroll
       for (int m = V; m < D; m++) {
@@ -213,8 +266,8 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
       ql[m] = QL[fn * D + m];
       qr[m] = QR[fn * D + m];
     }
-    if (ghostL) PDE::template wall<DIM>(qr, ghost_normal, ql);
-    if (ghostR) PDE::template wall<DIM>(ql, ghost_normal, qr);
+    if (ghostL) ghost_state<PDE, DIM, D>(qr, ghost_normal, ql);
+    if (ghostR) ghost_state<PDE, DIM, D>(ql, ghost_normal, qr);
     if (ghostL || ghostR) {
 #pragma unroll
       for (int m = V; m < D; m++) {
@@ -226,8 +279,12 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
       PDE::template flux<DIM>(ghostL ? ql : qr, Fg);
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        fl[m] = ghostL ? Fg[d * V + m] : FL[fn * V + m];
-        fr[m] = ghostR ? Fg[d * V + m] : FR[fn * V + m];
+        double fg = Fg[m];
+#pragma unroll
+        for (int k = 1; k < DIM; k++)
+          if (k == d) fg = Fg[k * V + m];
+        fl[m] = ghostL ? fg : FL[fn * V + m];
+        fr[m] = ghostR ? fg : FR[fn * V + m];
       }
     } else {
 #pragma unroll
@@ -240,9 +297,9 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
     if (PDE::kNCP) {
       double gq[DIM * V], qa[D];
 #pragma unroll
-      for (int k = 0; k < DIM * V; k++) gq[k] = 0.0;
+      for (int k = 0; k < DIM; k++)
 #pragma unroll
-      for (int m = 0; m < V; m++) gq[d * V + m] = qr[m] - ql[m];
+        for (int m = 0; m < V; m++) gq[k * V + m] = k == d ? qr[m] - ql[m] : 0.0;
 #pragma unroll
       for (int m = 0; m < D; m++) qa[m] = 0.5 * (qr[m] + ql[m]);
       PDE::template ncp<DIM>(qa, gq, ncp);
@@ -290,10 +347,11 @@ __global__ void __launch_bounds__(256) boundary_kernel(FaceArgs f) {
   const double* Q = f.lQhbnd + c * S::sizeQhb + face * S::nf * S::D;
   double* F = f.lFhbnd + c * S::sizeFhb + face * S::nf * S::V;
   // orientation 0: the cell is on the right of the face (ghost left); 1: ghost right
+  const bool outflow = f.btype && f.btype[warp] == 3;  // EXA_BC_OUTFLOW: ghost = inner state
   if (o == 0)
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, d);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, outflow ? -1 : d);
   else
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, d);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, outflow ? -1 : d);
 }
 
 // ------------------------------------------------------------------------------------------

@@ -8,6 +8,7 @@
 //   eigenvalues<DIM>(Q, d, lambda)   lambda[V]
 //   ncp<DIM>(Q, gradQ, BgradQ)       gradQ[d*V + m]  (only when kNCP)
 //   wall<DIM>(QIn, normal, QOut)     ghost state of a reflective wall (boundaryValues)
+//   static constexpr bool kSource;   the patch's point source (algebraicSource) may act on it
 //
 // The bodies restate the reference applications' formulas in the same operation order so that
 // the FP64 path agrees with the reference to rounding.
@@ -20,6 +21,7 @@ namespace exa {
 struct EulerPDE {
   static constexpr int V = 5;
   static constexpr bool kNCP = false;
+  static constexpr bool kSource = false;  // no algebraicSource
   static constexpr int id = 0;
 
   template <int DIM, class T>
@@ -46,7 +48,8 @@ struct EulerPDE {
     const double irho = 1. / Q[0];
     const double j2 = DIM == 3 ? Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3] : Q[1] * Q[1] + Q[2] * Q[2];
     const double p = (gamma - 1) * (Q[4] - 0.5 * irho * j2);
-    const double u_n = Q[d + 1] * irho;
+    // Q[d + 1] written as a select so that register-resident Q is never indexed at run time
+    const double u_n = (d == 0 ? Q[1] : (d == 1 ? Q[2] : Q[3])) * irho;
     const double c = sqrt(gamma * p * irho);
 #pragma unroll
     for (int m = 0; m < 5; m++) lambda[m] = u_n;
@@ -62,7 +65,9 @@ struct EulerPDE {
   static __device__ __forceinline__ void wall(const double* Qin, int normal, double* Qout) {
 #pragma unroll
     for (int m = 0; m < 5; m++) Qout[m] = Qin[m];
-    Qout[1 + normal] = -Qout[1 + normal];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      if (k == normal) Qout[1 + k] = -Qout[1 + k];
   }
 };
 
@@ -71,6 +76,7 @@ struct EulerPDE {
 struct SWEPDE {
   static constexpr int V = 4;
   static constexpr bool kNCP = true;
+  static constexpr bool kSource = false;
   static constexpr int id = 1;
   static constexpr double grav = 9.81;
 
@@ -95,7 +101,7 @@ struct SWEPDE {
   static __device__ __forceinline__ void eigenvalues(const double* Q, int d, double* lambda) {
     const double c = sqrt(grav * Q[0]);
     const double ih = 1. / Q[0];
-    const double u_n = Q[d + 1] * ih;
+    const double u_n = (d == 0 ? Q[1] : Q[2]) * ih;
     lambda[0] = u_n + c;
     lambda[1] = u_n - c;
     lambda[2] = u_n;
@@ -112,7 +118,129 @@ struct SWEPDE {
   static __device__ __forceinline__ void wall(const double* Qin, int normal, double* Qout) {
 #pragma unroll
     for (int m = 0; m < 4; m++) Qout[m] = Qin[m];
-    Qout[1 + normal] = -Qout[1 + normal];
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+      if (k == normal) Qout[1 + k] = -Qout[1 + k];
+  }
+};
+
+}  // namespace exa
+
+namespace exa {
+
+// Linear acoustics with material parameters carried per node (V = 4: p, u, v, w; P = 2: rho, c),
+// written in flux form for the nonlinear ADER-DG path (the reference's acoustic and elastic apps
+// use the linear kernels; these functors are new):
+//   dp/dt + div(rho c^2 u) = 0,   du_d/dt + d(p / rho)/dx_d = 0.
+// Inside a cell the parameters are constant, so the flux form equals the usual non-conservative
+// form; across cells the Rusanov flux couples them. Eigenvalues -c, 0, 0, +c.
+struct AcousticPDE {
+  static constexpr int V = 4;
+  static constexpr int P = 2;
+  static constexpr bool kNCP = false;
+  static constexpr bool kSource = true;  // regularised point source (Ricker)
+  static constexpr int id = 2;
+
+  template <int DIM, class T>
+  static __device__ __forceinline__ void flux(const T* Q, T* F) {
+    const T rho = Q[4], c = Q[5];
+    const T K = rho * c * c;
+    const T pr = Q[0] / rho;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      T* f = F + 4 * d;
+      f[0] = K * Q[1 + d];
+      f[1] = d == 0 ? pr : T(0);
+      f[2] = d == 1 ? pr : T(0);
+      f[3] = d == 2 ? pr : T(0);
+    }
+  }
+  template <int DIM>
+  static __device__ __forceinline__ void eigenvalues(const double* Q, int, double* lambda) {
+    const double c = Q[5];
+    lambda[0] = -c;
+    lambda[1] = 0.0;
+    lambda[2] = 0.0;
+    lambda[3] = c;
+  }
+  template <int DIM, class T>
+  static __device__ __forceinline__ void ncp(const T*, const T*, T* B) {
+#pragma unroll
+    for (int m = 0; m < 4; m++) B[m] = T(0);
+  }
+  template <int DIM>
+  static __device__ __forceinline__ void wall(const double* Qin, int normal, double* Qout) {
+#pragma unroll
+    for (int m = 0; m < 6; m++) Qout[m] = Qin[m];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      if (k == normal) Qout[1 + k] = -Qout[1 + k];
+  }
+};
+
+// Linear elasticity, velocity-stress form with per-node parameters (V = 9: v1 v2 v3 s11 s22 s33
+// s12 s13 s23; P = 3: rho, cp, cs; lambda = rho (cp^2 - 2 cs^2), mu = rho cs^2), in flux form:
+//   dv_i/dt - d(s_ij / rho)/dx_j = 0,
+//   ds_ij/dt - d(lambda delta_ij v_k + mu (delta_ik v_j + delta_jk v_i))/dx_k = 0.
+// Eigenvalues -cp, -cs, -cs, 0, 0, 0, cs, cs, cp.
+struct ElasticPDE {
+  static constexpr int V = 9;
+  static constexpr int P = 3;
+  static constexpr bool kNCP = false;
+  static constexpr bool kSource = true;  // regularised point source (Ricker)
+  static constexpr int id = 3;
+
+  template <int DIM, class T>
+  static __device__ __forceinline__ void flux(const T* Q, T* F) {
+    const T rho = Q[9], cp = Q[10], cs = Q[11];
+    const T mu = rho * cs * cs;
+    const T lam = rho * cp * cp - T(2) * mu;
+    const T ir = T(1) / rho;
+    // stress tensor entries by (i, j)
+    const T s[3][3] = {{Q[3], Q[6], Q[7]}, {Q[6], Q[4], Q[8]}, {Q[7], Q[8], Q[5]}};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      T* f = F + 9 * d;
+      f[0] = -s[0][d] * ir;
+      f[1] = -s[1][d] * ir;
+      f[2] = -s[2][d] * ir;
+      const T vd = Q[d];
+      // diagonal stresses: -(lambda v_d + 2 mu v_d delta_id)
+      f[3] = -(lam * vd + (d == 0 ? T(2) * mu * vd : T(0)));
+      f[4] = -(lam * vd + (d == 1 ? T(2) * mu * vd : T(0)));
+      f[5] = -(lam * vd + (d == 2 ? T(2) * mu * vd : T(0)));
+      // shear stresses s12, s13, s23: -mu (delta_1d v_2 + delta_2d v_1), ...
+      f[6] = -mu * ((d == 0 ? Q[1] : T(0)) + (d == 1 ? Q[0] : T(0)));
+      f[7] = -mu * ((d == 0 ? Q[2] : T(0)) + (d == 2 ? Q[0] : T(0)));
+      f[8] = -mu * ((d == 1 ? Q[2] : T(0)) + (d == 2 ? Q[1] : T(0)));
+    }
+  }
+  template <int DIM>
+  static __device__ __forceinline__ void eigenvalues(const double* Q, int, double* lambda) {
+    const double cp = Q[10], cs = Q[11];
+    lambda[0] = -cp;
+    lambda[1] = -cs;
+    lambda[2] = -cs;
+    lambda[3] = 0.0;
+    lambda[4] = 0.0;
+    lambda[5] = 0.0;
+    lambda[6] = cs;
+    lambda[7] = cs;
+    lambda[8] = cp;
+  }
+  template <int DIM, class T>
+  static __device__ __forceinline__ void ncp(const T*, const T*, T* B) {
+#pragma unroll
+    for (int m = 0; m < 9; m++) B[m] = T(0);
+  }
+  template <int DIM>
+  static __device__ __forceinline__ void wall(const double* Qin, int normal, double* Qout) {
+    // rigid wall: mirrored velocity
+#pragma unroll
+    for (int m = 0; m < 12; m++) Qout[m] = Qin[m];
+#pragma unroll
+    for (int k = 0; k < 3; k++) Qout[k] = -Qout[k];
+    (void)normal;
   }
 };
 

@@ -92,6 +92,31 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
   for (int d = 0; d < DIM; d++) off[d] = pnode_off<DIM, n>(d, p);
 
+  // point source (algebraicSource at x_p, t + node_i dt, :323-337): only cells near the source
+  bool srcOn = false;
+  double tcell = 0.0;
+  if (PDE::kSource && a.src && live) {
+    const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+    const double dxv[3] = {1.0 / s_invdx[lc][0], DIM > 1 ? 1.0 / s_invdx[lc][1] : 1.0,
+                           DIM > 2 ? 1.0 / s_invdx[lc][2] : 1.0};
+    double cc[3];
+    cell_centre(a, cell, g, dxv, cc);
+    srcOn = source_near<DIM>(a.src, cc, dxv);
+    tcell = a.grid_t ? a.grid_t[g] : a.u_t;
+  }
+  // source value of this node at time node i (evaluated only where srcOn)
+  auto src_at = [&](int i) -> double {
+    const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+    const double dxv[3] = {1.0 / s_invdx[lc][0], DIM > 1 ? 1.0 / s_invdx[lc][1] : 1.0,
+                           DIM > 2 ? 1.0 / s_invdx[lc][2] : 1.0};
+    double cc[3], x[3];
+    cell_centre(a, cell, g, dxv, cc);
+#pragma unroll
+    for (int d = 0; d < 3; d++) x[d] = cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5);
+    return point_source<DIM>(a.src, x, tcell + G::nodes(i) * s_dt[lc]);
+  };
+  const int srcVar = (PDE::kSource && a.src) ? (int)a.src[7] : -1;
+
   // this thread's line contractions, packed: start offset in sF (bits 0-17), direction
   // (bits 18-19), index of the line weight (bits 20-31); -1 when the thread has none
   static_assert(S::smemF < (1 << 18) && CPB * DIM * NL < (1 << 12), "packed line descriptor overflow");
@@ -274,10 +299,12 @@ predictor_kernel(CellArgs a) {
         for (int i = 0; i < n; i++) {
           const double wi = G::weights(i);
           const double f0 = G::F0(i);
+          const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
 #pragma unroll
           for (int m = 0; m < V; m++) {
             double rhs = w_sp * f0 * u[m] - wi * o[m];
             if (NCP) rhs += wi * w_sp * dt * S0[m];
+            if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
             q_s[(i * nd + p) * D + m] = iweight * rhs;
           }
         }
@@ -340,9 +367,11 @@ predictor_kernel(CellArgs a) {
         // phase 3: rhs of time node i, scaled by 1/w_xyz, as slice i (:231-246, :323-367)
         if (work) {
           const double f0 = G::F0(i);
+          const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
 #pragma unroll
           for (int m = 0; m < V; m++) {
             double rhs = w_sp * f0 * u[m];
+            if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
             if (MIXED) {
               const float* sFf = reinterpret_cast<const float*>(f_s);
               float c = 0.0f;
@@ -516,6 +545,13 @@ predictor_kernel(CellArgs a) {
     if (NCP) {
 #pragma unroll
       for (int m = 0; m < V; m++) acc[m] += w_sp * sh_s[p * V + m];
+    }
+    if (PDE::kSource && srcOn) {  // time-averaged point source lShi (volumeIntegralNonlinear :211-221)
+      double sa = 0.0;
+      for (int i = 0; i < n; i++) sa = fma(src_at(i), G::weights(i), sa);
+#pragma unroll
+      for (int m = 0; m < V; m++)
+        if (m == srcVar) acc[m] += w_sp * sa;
     }
     bool ok = true;
 #pragma unroll

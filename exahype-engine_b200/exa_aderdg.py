@@ -20,11 +20,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libexa_aderdg.so")
 
 EXA_OK = 0
-PDE_EULER, PDE_SWE = 0, 1
+PDE_EULER, PDE_SWE, PDE_ACOUSTIC, PDE_ELASTIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 BC_PERIODIC, BC_WALL = 0, 1
 ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT = 1, 2, 4, 8
-NVAR = {PDE_EULER: 5, PDE_SWE: 4}
+NVAR = {PDE_EULER: 5, PDE_SWE: 4, PDE_ACOUSTIC: 4, PDE_ELASTIC: 9}
+NPAR = {PDE_EULER: 0, PDE_SWE: 0, PDE_ACOUSTIC: 2, PDE_ELASTIC: 3}
 
 
 class ExaError(RuntimeError):
@@ -56,7 +57,12 @@ class FaceLists(ctypes.Structure):
 
 
 PHASE_PREDICTOR, PHASE_FACES, PHASE_UPDATE, PHASE_ADVANCE = 0, 1, 2, 3
-BC_HALO = 2
+BC_HALO, BC_OUTFLOW = 2, 3
+
+
+class PointSource(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_double * 3), ("f0", ctypes.c_double), ("t0", ctypes.c_double),
+                ("amplitude", ctypes.c_double), ("width", ctypes.c_double), ("variable", ctypes.c_int)]
 
 
 class _PatchStats(ctypes.Structure):
@@ -108,6 +114,7 @@ def load_library(path=None):
         "exa_patch_dt_next_copy": [vp, vp, i],
         "exa_patch_dt_copy": [vp, vp, i],
         "exa_build_face_lists": [i, i, ctypes.POINTER(GridDesc), ctypes.POINTER(FaceLists)],
+        "exa_patch_set_point_source": [vp, ctypes.POINTER(PointSource)],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -327,6 +334,15 @@ class Patch:
 
     def dt_next_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_next_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_next_copy")
+
+    def set_point_source(self, x, f0=0.0, t0=0.0, amplitude=0.0, width=1.0, variable=0):
+        """Ricker point source on `variable` (acoustic / elastic solvers); x=None removes it."""
+        if x is None:
+            _check(self.lib.exa_patch_set_point_source(self.h, None), "exa_patch_set_point_source")
+            return
+        ps = PointSource((ctypes.c_double * 3)(*list(x) + [0.0] * (3 - len(x))), f0, t0, amplitude, width,
+                         int(variable))
+        _check(self.lib.exa_patch_set_point_source(self.h, ctypes.byref(ps)), "exa_patch_set_point_source")
 
     def dt_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_copy")

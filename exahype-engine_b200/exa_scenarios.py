@@ -162,3 +162,52 @@ def swe_batched(ngrids=512, order=4, seed=0, nmin=16, nmax=128):
     for sp in specs:
         sp["bc"] = 1  # reflective walls on every side
     return specs, states
+
+
+# ------------------------------------------------------------------------------------------
+# Linear waves in a layered medium, driven by a point source
+# ------------------------------------------------------------------------------------------
+
+def layered_medium(pde, ncell, size, order, seed=0, offset=None):
+    """Initial state of the acoustic (V=4, P=2) or elastic (V=9, P=3) system with material
+    parameters constant per cell: two layers split at mid-height of the last axis (upper layer
+    slower), with a +-5 % seeded random perturbation per cell. Acoustic: a Gaussian pressure pulse
+    (width 0.08 of the box) at 0.3 of the box; elastic: at rest. Returns luh [cells*nodes*D]."""
+    rng = np.random.default_rng(seed)
+    dim = len(ncell)
+    x = nodal_positions(ncell, size, order, offset)          # [cells][nodes][dim]
+    ncells, nd = x.shape[0], x.shape[1]
+    off = np.zeros(dim) if offset is None else np.asarray(offset, dtype=float)
+    size = np.asarray(size, dtype=float)
+    cz = x.mean(axis=1)[:, -1]                               # cell-centre height
+    upper = cz > off[-1] + 0.5 * size[-1]
+    jitter = 1.0 + 0.05 * rng.uniform(-1, 1, ncells)
+    if pde == "acoustic":
+        rho = np.where(upper, 1.0, 1.5)
+        c = np.where(upper, 1.0, 1.6) * jitter
+        Q = np.zeros((ncells, nd, 6))
+        r2 = (((x - (off + 0.3 * size)) / (0.08 * size)) ** 2).sum(-1)
+        Q[..., 0] = np.exp(-r2)
+        Q[..., 4] = rho[:, None]
+        Q[..., 5] = c[:, None]
+        return Q.reshape(-1)
+    if pde == "elastic":
+        rho = np.where(upper, 1.0, 1.4)
+        cp = np.where(upper, 1.7, 2.4) * jitter
+        cs = np.where(upper, 1.0, 1.4) * jitter
+        Q = np.zeros((ncells, nd, 12))
+        Q[..., 9] = rho[:, None]
+        Q[..., 10] = cp[:, None]
+        Q[..., 11] = cs[:, None]
+        return Q.reshape(-1)
+    raise ValueError(pde)
+
+
+def ricker_source(dim, size, offset=None, f0=4.0, amplitude=1.0, width=None, variable=0, at=0.5):
+    """(x, y, z, f0, t0, amplitude, width, variable) of a point source at fraction `at` of the box,
+    delayed by t0 = 1.2 / f0 so that the wavelet starts from (near) zero."""
+    off = np.zeros(dim) if offset is None else np.asarray(offset, dtype=float)
+    size = np.asarray(size, dtype=float)
+    pos = list(off + at * size) + [0.0] * (3 - dim)
+    w = float(width) if width is not None else float(0.04 * size.min())
+    return tuple(pos) + (float(f0), 1.2 / float(f0), float(amplitude), w, float(variable))

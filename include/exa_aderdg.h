@@ -51,7 +51,9 @@ typedef enum {
  * nonConservativeProduct / boundaryValues of AbstractGenericADERDGSolverHeader.template:220-338). */
 typedef enum {
   EXA_PDE_EULER = 0, /* compressible Euler, gamma 1.4, V=5 (Euler_ADERDG/EulerSolver_ADERDG.cpp:61-146) */
-  EXA_PDE_SWE = 1    /* shallow water h,hu,hv,b with NCP, V=4 (SWE_ADERDG/MySWESolver.cpp:103-152) */
+  EXA_PDE_SWE = 1,   /* shallow water h,hu,hv,b with NCP, V=4 (SWE_ADERDG/MySWESolver.cpp:103-152) */
+  EXA_PDE_ACOUSTIC = 2, /* linear acoustics p,u,v,w with per-node rho,c (nPar=2), flux form; new */
+  EXA_PDE_ELASTIC = 3   /* linear elasticity v,sigma (V=9) with per-node rho,cp,cs (nPar=3), flux form; new */
 } exa_pde;
 
 typedef enum {
@@ -62,7 +64,9 @@ typedef enum {
 /* EXA_BC_HALO (last axis of a single-grid patch only): the two boundary layers face ghost
  * cells whose face traces a neighbouring subdomain supplies (slab decomposition, see
  * exa_patch_halo_pack / exa_patch_halo_unpack). */
-typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1, EXA_BC_HALO = 2 } exa_bc;
+/* EXA_BC_OUTFLOW: the ghost state is the inner state (boundaryValues copying stateIn), which
+ * lets waves leave the domain (the absorbing boundary of the elastic configuration). */
+typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1, EXA_BC_HALO = 2, EXA_BC_OUTFLOW = 3 } exa_bc;
 
 /* Compile-time constants of the reference's generated solver (AbstractGenericADERDGSolverHeader
  * .template:34-68), here runtime fields of a solver handle. */
@@ -228,6 +232,19 @@ int exa_patch_track_picard(exa_patch* p, int on);
 int exa_patch_stats_get(exa_patch* p, exa_patch_stats* st);
 int exa_patch_status(exa_patch* p, unsigned* bits);       /* reads and clears (synchronises) */
 void* exa_patch_stream(exa_patch* p);                     /* the cudaStream_t the patch runs on */
+
+/* Point source of the patch: the user's algebraicSource hook evaluated at every node x and
+ * time t + node_i*dt (3d/spaceTimePredictorNonlinear.cpph:323-337) as
+ *   S_var(x, t) = amplitude * r(t - t0) * exp(-|x - xs|^2 / (2 width^2)) / ((2 pi)^(d/2) width^d),
+ *   r(s) = (1 - 2 pi^2 f0^2 s^2) exp(-pi^2 f0^2 s^2)  (Ricker wavelet),
+ * on variable `variable`. Only PDEs built with a source (acoustic, elastic) use it; cells farther
+ * than 6 widths plus a cell diagonal from xs are skipped. NULL removes the source. */
+typedef struct {
+  double x[3];
+  double f0, t0, amplitude, width;
+  int variable;
+} exa_point_source;
+int exa_patch_set_point_source(exa_patch* p, const exa_point_source* src);
 
 /* ---- one step in phases, for subdomains that exchange face traces ---------------------------
  * The reference exchanges the face data of cells next to a remote rank by MPI

@@ -190,10 +190,48 @@ static void swe_ncp(const double* Q, const double* gradQ /*[d][4]*/, double* Bgr
   BgradQ[3] = 0.0;
 }
 
+/* Linear acoustics in flux form with per-node parameters Q[4] = rho, Q[5] = c (new functor;
+ * the reference's acoustic app uses the linear kernels): F_d = (rho c^2 u_d, p/rho e_d). */
+static void acoustic_flux(int dim, const double* Q, double* F) {
+  const double rho = Q[4], cc = Q[5];
+  const double K = rho * cc * cc;
+  const double pr = Q[0] / rho;
+  for (int d = 0; d < dim; d++) {
+    double* f = F + 4 * d;
+    f[0] = K * Q[1 + d];
+    f[1] = d == 0 ? pr : 0.0;
+    f[2] = d == 1 ? pr : 0.0;
+    f[3] = d == 2 ? pr : 0.0;
+  }
+}
+/* Linear elasticity, velocity-stress form, per-node rho, cp, cs (Q[9..11]) in flux form. */
+static void elastic_flux(int dim, const double* Q, double* F) {
+  const double rho = Q[9], cp = Q[10], cs = Q[11];
+  const double mu = rho * cs * cs;
+  const double lam = rho * cp * cp - 2.0 * mu;
+  const double ir = 1.0 / rho;
+  const double sg[3][3] = {{Q[3], Q[6], Q[7]}, {Q[6], Q[4], Q[8]}, {Q[7], Q[8], Q[5]}};
+  for (int d = 0; d < dim; d++) {
+    double* f = F + 9 * d;
+    f[0] = -sg[0][d] * ir;
+    f[1] = -sg[1][d] * ir;
+    f[2] = -sg[2][d] * ir;
+    const double vd = Q[d];
+    f[3] = -(lam * vd + (d == 0 ? 2.0 * mu * vd : 0.0));
+    f[4] = -(lam * vd + (d == 1 ? 2.0 * mu * vd : 0.0));
+    f[5] = -(lam * vd + (d == 2 ? 2.0 * mu * vd : 0.0));
+    f[6] = -mu * ((d == 0 ? Q[1] : 0.0) + (d == 1 ? Q[0] : 0.0));
+    f[7] = -mu * ((d == 0 ? Q[2] : 0.0) + (d == 2 ? Q[0] : 0.0));
+    f[8] = -mu * ((d == 1 ? Q[2] : 0.0) + (d == 2 ? Q[1] : 0.0));
+  }
+}
+
 void exo_flux(const exo_cfg* c, const double* Q, double* F) {
   switch (c->pde) {
     case EXO_PDE_EULER: euler_flux(c->dim, Q, F); break;
     case EXO_PDE_SWE: swe_flux(c->dim, Q, F); break;
+    case EXO_PDE_ACOUSTIC: acoustic_flux(c->dim, Q, F); break;
+    case EXO_PDE_ELASTIC: elastic_flux(c->dim, Q, F); break;
     default: memset(F, 0, sizeof(double) * c->dim * c->nvar);
   }
 }
@@ -201,8 +239,40 @@ void exo_eigenvalues(const exo_cfg* c, const double* Q, int d, double* lambda) {
   switch (c->pde) {
     case EXO_PDE_EULER: euler_eig(c->dim, Q, d, lambda); break;
     case EXO_PDE_SWE: swe_eig(Q, d, lambda); break;
+    case EXO_PDE_ACOUSTIC:
+      lambda[0] = -Q[5]; lambda[1] = 0.0; lambda[2] = 0.0; lambda[3] = Q[5];
+      break;
+    case EXO_PDE_ELASTIC: {
+      const double cp = Q[10], cs = Q[11];
+      const double l[9] = {-cp, -cs, -cs, 0.0, 0.0, 0.0, cs, cs, cp};
+      memcpy(lambda, l, sizeof(l));
+      break;
+    }
     default: memset(lambda, 0, sizeof(double) * c->nvar);
   }
+}
+
+/* Regularised point source on variable src[7]: amplitude * Ricker(t - t0; f0) * Gaussian of
+ * width src[6] around (src[0..2]), normalised to unit mass; cells whose centre is farther than
+ * 6 widths plus a cell diagonal receive none (the same truncation as the device kernels). */
+static double point_source(const exo_cfg* c, const double* x, double t) {
+  const double pi = 3.14159265358979323846;
+  double r2 = 0.0;
+  for (int d = 0; d < c->dim; d++) r2 += (x[d] - c->src[d]) * (x[d] - c->src[d]);
+  const double w = c->src[6];
+  const double a = pi * c->src[3] * (t - c->src[4]);
+  const double ricker = (1.0 - 2.0 * a * a) * exp(-a * a);
+  const double norm = c->dim == 3 ? 1.0 / (15.749609945722419 * w * w * w) : 1.0 / (6.283185307179586 * w * w);
+  return c->src[5] * ricker * exp(-0.5 * r2 / (w * w)) * norm;
+}
+static int source_near(const exo_cfg* c, const double* centre, const double* dx) {
+  double r2 = 0.0, h2 = 0.0;
+  for (int d = 0; d < c->dim; d++) {
+    r2 += (centre[d] - c->src[d]) * (centre[d] - c->src[d]);
+    h2 += dx[d] * dx[d];
+  }
+  const double reach = 6.0 * c->src[6] + sqrt(h2);
+  return r2 <= reach * reach;
 }
 static void exo_ncp(const exo_cfg* c, const double* Q, const double* gradQ, double* BgradQ) {
   switch (c->pde) {
@@ -216,7 +286,19 @@ void exo_boundary_wall(const exo_cfg* c, double* FOut, double* QOut, const doubl
   const int D = c->nvar + c->npar;
   double F[3 * MAXV];
   memcpy(QOut, QIn, sizeof(double) * D);
-  QOut[1 + normal] = -QOut[1 + normal];
+  if (c->pde == EXO_PDE_ELASTIC) {
+    for (int k = 0; k < 3; k++) QOut[k] = -QOut[k];
+  } else {
+    QOut[1 + normal] = -QOut[1 + normal];
+  }
+  exo_flux(c, QOut, F);
+  memcpy(FOut, F + normal * c->nvar, sizeof(double) * c->nvar);
+}
+/* outflow: boundaryValues returning the inner state and its flux */
+static void exo_boundary_outflow(const exo_cfg* c, double* FOut, double* QOut, const double* QIn, int normal) {
+  const int D = c->nvar + c->npar;
+  double F[3 * MAXV];
+  memcpy(QOut, QIn, sizeof(double) * D);
   exo_flux(c, QOut, F);
   memcpy(FOut, F + normal * c->nvar, sizeof(double) * c->nvar);
 }
@@ -277,17 +359,19 @@ static inline int lfhi_index(const geo* g, int dir, const int* co) {
 /* ------------------------------------------------------------------------------------------ */
 /* Space-time predictor: 3d/spaceTimePredictorNonlinear.cpph:39-433 (Picard loop), :441-515    */
 /* (time averaging), :517-687 (extrapolation), :816-864 (entry); 2D analogue 2d/...:38-597.    */
-/* Source term: zero for the PDEs here (algebraicSource returns 0), so S = -NCP (fusedMethods  */
-/* .cpph:65-80 sign convention).                                                               */
+/* Source term (:323-367): S = algebraicSource(x_node, t + node_i dt) - NCP; the point source   */
+/* of the acoustic / elastic systems is the only algebraicSource here (zero for Euler / SWE).  */
 /* ------------------------------------------------------------------------------------------ */
 int exo_predictor(const exo_cfg* c, const double* luh, const double* centre, const double* dx, double t,
                   double dt, double* lQi, double* lFi, double* lQhi, double* lFhi, double* lQhbnd,
                   double* lFhbnd, int* sweeps) {
-  (void)centre; (void)t;
   geo g;
   geo_init(&g, c);
   const int n = g.n, v = g.v, D = g.D, nd = g.nd, dim = g.dim, nf = g.nf;
   const int useNCP = c->use_ncp;
+  const int useSource = c->has_src; /* the lFi source block exists (zero far from the source) */
+  const int srcOn = c->has_src && source_near(c, centre, dx);
+  const int srcVar = (int)c->src[7];
   double invDx[3];
   for (int d = 0; d < dim; d++) invDx[d] = 1.0 / dx[d];
   const int maxIter = c->max_picard > 0 ? c->max_picard : 2 * n;
@@ -353,18 +437,25 @@ int exo_predictor(const exo_cfg* c, const double* luh, const double* centre, con
         }
       }
       /* source / NCP (:323-367) */
-      if (useNCP) {
+      if (useNCP || useSource) {
         for (int p = 0; p < nd; p++) {
           int co[3];
           node_coords(&g, p, co);
           const double weight = dim == 3 ? g.w[i] * g.w[co[2]] * g.w[co[1]] * g.w[co[0]]
                                          : g.w[i] * g.w[co[1]] * g.w[co[0]];
           const double updateSize = weight * dt;
-          double ncp[MAXV];
           double* S = &LFI(i, p, dim, 0);
           for (int m = 0; m < v; m++) S[m] = 0.0;
-          exo_ncp(c, &LQI(p, i, 0), &gradQ[p * dim * v], ncp);
-          for (int m = 0; m < v; m++) S[m] -= ncp[m];
+          if (srcOn) {
+            double x[3];
+            for (int dd = 0; dd < dim; dd++) x[dd] = centre[dd] + dx[dd] * (g.x[co[dd]] - 0.5);
+            S[srcVar] = point_source(c, x, t + g.x[i] * dt);
+          }
+          if (useNCP) {
+            double ncp[MAXV];
+            exo_ncp(c, &LQI(p, i, 0), &gradQ[p * dim * v], ncp);
+            for (int m = 0; m < v; m++) S[m] -= ncp[m];
+          }
           for (int m = 0; m < v; m++) RHS(i, p, m) += updateSize * S[m];
         }
       }
@@ -404,7 +495,7 @@ int exo_predictor(const exo_cfg* c, const double* luh, const double* centre, con
       for (int tt = 0; tt < n; tt++) {
         for (int dd = 0; dd < dim; dd++)
           lFhi[dd * nd * v + lfhi_index(&g, dd, co) * v + m] += LFI(tt, p, dd, m) * g.w[tt];
-        if (useNCP) lFhi[dim * nd * v + p * v + m] += LFI(tt, p, dim, m) * g.w[tt];
+        if (useNCP || useSource) lFhi[dim * nd * v + p * v + m] += LFI(tt, p, dim, m) * g.w[tt];
       }
     for (int m = 0; m < D; m++)
       for (int tt = 0; tt < n; tt++) lQhi[p * D + m] += LQI(p, tt, m) * g.w[tt];
@@ -468,7 +559,7 @@ void exo_volume(const exo_cfg* c, double* lduh, const double* lFhi, const double
         }
     }
   }
-  if (c->use_ncp) {
+  if (c->use_ncp || c->has_src) {
     for (int p = 0; p < nd; p++) {
       int co[3];
       node_coords(&g, p, co);
@@ -670,7 +761,12 @@ int exo_run(const exo_cfg* c, const int* ncell, const double* offset, const doub
         double QOut[MAXN * MAXN * MAXV], FOut[MAXN * MAXN * MAXV];
         if (j[d] == lim) {
           if (walls) {
-            for (int f = 0; f < nf; f++) exo_boundary_wall(c, FOut + f * v, QOut + f * D, QL + f * D, d);
+            for (int f = 0; f < nf; f++) {
+              if (walls == 3)
+                exo_boundary_outflow(c, FOut + f * v, QOut + f * D, QL + f * D, d);
+              else
+                exo_boundary_wall(c, FOut + f * v, QOut + f * D, QL + f * D, d);
+            }
             exo_riemann(c, FL, FOut, QL, QOut, dx, d);
           } else {
             j[d] = 0;
@@ -684,7 +780,12 @@ int exo_run(const exo_cfg* c, const int* ncell, const double* offset, const doub
         if (walls && k == 0) {
           double* FRb = lFhbnd + ci * sF + 2 * d * nf * v;
           const double* QRb = lQhbnd + ci * sQ + 2 * d * nf * D;
-          for (int f = 0; f < nf; f++) exo_boundary_wall(c, FOut + f * v, QOut + f * D, QRb + f * D, d);
+          for (int f = 0; f < nf; f++) {
+            if (walls == 3)
+              exo_boundary_outflow(c, FOut + f * v, QOut + f * D, QRb + f * D, d);
+            else
+              exo_boundary_wall(c, FOut + f * v, QOut + f * D, QRb + f * D, d);
+          }
           exo_riemann(c, FOut, FRb, QOut, QRb, dx, d);
         }
       }

@@ -33,6 +33,8 @@ typedef struct {
   double cfl;   /* CFL safety factor (0.9) */
   double pnpm;  /* ADER-DG PNPM factor for this order */
   int max_picard; /* 0: 2(N+1) with the residual test; >0: that fixed count, no test */
+  int has_src;    /* point source active (algebraicSource of the acoustic / elastic systems) */
+  double src[8];  /* x, y, z, f0, t0, amplitude, width, variable */
 } exo_cfg;
 
 /* DG operator tables on [0,1] for order N (arrays of n and n*n doubles, [row][col]). */
@@ -57,8 +59,8 @@ void exo_boundary_wall(const exo_cfg* c, double* FOut, double* QOut, const doubl
 void exo_flux(const exo_cfg* c, const double* Q, double* F /* [d][nvar] */);
 void exo_eigenvalues(const exo_cfg* c, const double* Q, int direction, double* lambda);
 
-/* Uniform patch in the global non-fused order (dt from CFL unless fixed_dt > 0). Periodic, or
- * reflective walls on every domain face when walls != 0. luh: all cells, cell-major,
+/* Uniform patch in the global non-fused order (dt from CFL unless fixed_dt > 0). walls selects
+ * the domain faces: 0 periodic, 1 reflective walls, 3 outflow (ghost = inner state). luh: all cells, cell-major,
  * c = (iz*ny+iy)*nx+ix. Optional outputs: dts[nsteps], picard[nsteps*ncells] (sweeps). */
 int exo_run(const exo_cfg* c, const int* ncell, const double* offset, const double* size, int walls,
             double* luh, int nsteps, double t0, double fixed_dt, double* t_out, double* dts, int* picard,

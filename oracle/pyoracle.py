@@ -22,7 +22,11 @@ PNPM = [1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015]
 class ExoCfg(ctypes.Structure):
     _fields_ = [("dim", ctypes.c_int), ("order", ctypes.c_int), ("nvar", ctypes.c_int), ("npar", ctypes.c_int),
                 ("pde", ctypes.c_int), ("use_ncp", ctypes.c_int), ("cfl", ctypes.c_double),
-                ("pnpm", ctypes.c_double), ("max_picard", ctypes.c_int)]
+                ("pnpm", ctypes.c_double), ("max_picard", ctypes.c_int), ("has_src", ctypes.c_int),
+                ("src", ctypes.c_double * 8)]
+
+NVAR = {PDE_EULER: 5, PDE_SWE: 4, PDE_ACOUSTIC: 4, PDE_ELASTIC: 9}
+NPAR = {PDE_EULER: 0, PDE_SWE: 0, PDE_ACOUSTIC: 2, PDE_ELASTIC: 3}
 
 
 def _p(a):
@@ -36,7 +40,8 @@ def _f64(a):
 class Oracle:
     """The C restatement, one configuration (dim, order, PDE) per instance."""
 
-    def __init__(self, dim, order, pde=PDE_EULER, nvar=None, npar=0, cfl=0.9, max_picard=0):
+    def __init__(self, dim, order, pde=PDE_EULER, nvar=None, npar=None, cfl=0.9, max_picard=0, source=None):
+        """source: (x, y, z, f0, t0, amplitude, width, variable) of the point source, or None."""
         path = os.path.join(HERE, "liboracle.so")
         if not os.path.exists(path):
             raise RuntimeError("oracle/liboracle.so missing: run make -C oracle")
@@ -44,8 +49,12 @@ class Oracle:
         self.lib.exo_predictor.restype = ctypes.c_int
         self.lib.exo_dt.restype = ctypes.c_double
         if nvar is None:
-            nvar = {PDE_EULER: 5, PDE_SWE: 4}[pde]
-        self.cfg = ExoCfg(dim, order, nvar, npar, pde, 1 if pde == PDE_SWE else 0, cfl, PNPM[order], max_picard)
+            nvar = NVAR[pde]
+        if npar is None:
+            npar = NPAR[pde]
+        src = (ctypes.c_double * 8)(*(list(source) if source is not None else [0.0] * 8))
+        self.cfg = ExoCfg(dim, order, nvar, npar, pde, 1 if pde == PDE_SWE else 0, cfl, PNPM[order], max_picard,
+                          1 if source is not None else 0, src)
         self.dim, self.n, self.v, self.D = dim, order + 1, nvar, nvar + npar
         self.nd = self.n ** dim
         self.nf = self.n ** (dim - 1)
@@ -116,7 +125,9 @@ class Oracle:
 
     def run(self, luh, ncell, size, nsteps, offset=(0.0, 0.0, 0.0), walls=False, t0=0.0, fixed_dt=0.0,
             nthreads=0, want_picard=False):
-        """Advance a uniform patch in place; returns (t, dts, picard sweeps per step and cell)."""
+        """Advance a uniform patch in place; returns (t, dts, picard sweeps per step and cell).
+
+        walls: False / 0 periodic, True / 1 reflective walls, 3 outflow on every domain face."""
         luh = np.ascontiguousarray(luh, dtype=np.float64)
         nc = int(np.prod(ncell))
         dts = np.zeros(nsteps)
@@ -133,7 +144,9 @@ class Oracle:
 class RefKernels:
     """The reference's own generic kernels (oracle/_ref), one instantiation per instance."""
 
-    def __init__(self, dim, order, pde="euler", npar=0):
+    def __init__(self, dim, order, pde="euler", npar=0, source=None):
+        """source: point source (x, y, z, f0, t0, amplitude, width, variable) for the acoustic and
+        elastic instantiations (process-wide setting of the library), or None."""
         path = os.path.join(HERE, "_ref", "libexaref%dd.so" % dim)
         if not os.path.exists(path):
             raise FileNotFoundError(path)
@@ -142,7 +155,9 @@ class RefKernels:
         if not hasattr(self.lib, self.prefix + "_predictor"):
             raise AttributeError("instantiation %s not built" % self.prefix)
         self.dim, self.n = dim, order + 1
-        self.v = {"euler": 5, "swe": 4}[pde]
+        self.v = {"euler": 5, "swe": 4, "acoustic": 4, "elastic": 9}[pde]
+        src = (ctypes.c_double * 8)(*(list(source) if source is not None else [0, 0, 0, 0, 0, 0, 1, 0]))
+        self.lib.exaref_set_source(src, 1 if source is not None else 0)
         self.D = self.v + npar
         self.nd, self.nf = self.n ** dim, self.n ** (dim - 1)
         getattr(self.lib, self.prefix + "_predictor").restype = ctypes.c_int

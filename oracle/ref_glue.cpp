@@ -123,6 +123,107 @@ struct SWEPDE {
   }
 };
 
+// Linear acoustics in flux form with per-node parameters rho = Q[4], c = Q[5]; the nonlinear
+// functors the GPU path uses for this system (the reference's acoustic app is linear-only).
+struct AcousticPDE {
+  static constexpr int NumberOfVariables = 4;
+  static constexpr bool HasSource = true;
+  static void flux(const double* const Q, double** const F) {
+    const double rho = Q[4], c = Q[5];
+    const double K = rho * c * c;
+    const double pr = Q[0] / rho;
+    for (int d = 0; d < DIMENSIONS; d++) {
+      F[d][0] = K * Q[1 + d];
+      F[d][1] = d == 0 ? pr : 0.0;
+      F[d][2] = d == 1 ? pr : 0.0;
+      F[d][3] = d == 2 ? pr : 0.0;
+    }
+  }
+  static void eigenvalues(const double* const Q, const int, double* const lambda) {
+    lambda[0] = -Q[5];
+    lambda[1] = 0.0;
+    lambda[2] = 0.0;
+    lambda[3] = Q[5];
+  }
+  static void nonConservativeProduct(const double* const, const double* const, double* const B) {
+    std::fill_n(B, 4, 0.0);
+  }
+  static void wall(const double* QIn, int normal, double* QOut) {
+    std::copy_n(QIn, 4, QOut);
+    QOut[1 + normal] = -QOut[1 + normal];
+  }
+};
+
+// Linear elasticity, velocity-stress form (v1 v2 v3 s11 s22 s33 s12 s13 s23), per-node
+// rho, cp, cs = Q[9..11], in flux form.
+struct ElasticPDE {
+  static constexpr int NumberOfVariables = 9;
+  static constexpr bool HasSource = true;
+  static void flux(const double* const Q, double** const F) {
+    const double rho = Q[9], cp = Q[10], cs = Q[11];
+    const double mu = rho * cs * cs;
+    const double lam = rho * cp * cp - 2.0 * mu;
+    const double ir = 1.0 / rho;
+    const double sg[3][3] = {{Q[3], Q[6], Q[7]}, {Q[6], Q[4], Q[8]}, {Q[7], Q[8], Q[5]}};
+    for (int d = 0; d < DIMENSIONS; d++) {
+      double* f = F[d];
+      f[0] = -sg[0][d] * ir;
+      f[1] = -sg[1][d] * ir;
+      f[2] = -sg[2][d] * ir;
+      const double vd = Q[d];
+      f[3] = -(lam * vd + (d == 0 ? 2.0 * mu * vd : 0.0));
+      f[4] = -(lam * vd + (d == 1 ? 2.0 * mu * vd : 0.0));
+      f[5] = -(lam * vd + (d == 2 ? 2.0 * mu * vd : 0.0));
+      f[6] = -mu * ((d == 0 ? Q[1] : 0.0) + (d == 1 ? Q[0] : 0.0));
+      f[7] = -mu * ((d == 0 ? Q[2] : 0.0) + (d == 2 ? Q[0] : 0.0));
+      f[8] = -mu * ((d == 1 ? Q[2] : 0.0) + (d == 2 ? Q[1] : 0.0));
+    }
+  }
+  static void eigenvalues(const double* const Q, const int, double* const lambda) {
+    const double cp = Q[10], cs = Q[11];
+    const double l[9] = {-cp, -cs, -cs, 0.0, 0.0, 0.0, cs, cs, cp};
+    std::copy_n(l, 9, lambda);
+  }
+  static void nonConservativeProduct(const double* const, const double* const, double* const B) {
+    std::fill_n(B, 9, 0.0);
+  }
+  static void wall(const double* QIn, int, double* QOut) {
+    std::copy_n(QIn, 9, QOut);
+    for (int k = 0; k < 3; k++) QOut[k] = -QOut[k];
+  }
+};
+
+// Point source of the acoustic / elastic solvers (x, y, z, f0, t0, amplitude, width, variable):
+// a unit-mass Gaussian of the given width times a Ricker wavelet, acting only on cells whose
+// centre is within 6 widths plus a cell diagonal (the per-cell truncation the GPU path and the
+// C restatement use). algebraicSource sees only the node, so the cell's verdict is handed to it
+// through a thread-local flag set before each predictor call.
+double g_src[8] = {0, 0, 0, 0, 0, 0, 1, 0};
+int g_src_active = 0;
+int g_bc_mode = 1;  // 1 reflective wall, 3 outflow
+thread_local int tl_src_on = 0;
+
+inline bool source_near(const double* centre, const double* dx) {
+  if (!g_src_active) return false;
+  double r2 = 0.0, h2 = 0.0;
+  for (int d = 0; d < DIMENSIONS; d++) {
+    r2 += (centre[d] - g_src[d]) * (centre[d] - g_src[d]);
+    h2 += dx[d] * dx[d];
+  }
+  const double reach = 6.0 * g_src[6] + std::sqrt(h2);
+  return r2 <= reach * reach;
+}
+inline double point_source(const double* x, double t) {
+  const double pi = 3.14159265358979323846;
+  double r2 = 0.0;
+  for (int d = 0; d < DIMENSIONS; d++) r2 += (x[d] - g_src[d]) * (x[d] - g_src[d]);
+  const double w = g_src[6];
+  const double a = pi * g_src[3] * (t - g_src[4]);
+  const double ricker = (1.0 - 2.0 * a * a) * std::exp(-a * a);
+  const double norm = DIMENSIONS == 3 ? 1.0 / (15.749609945722419 * w * w * w) : 1.0 / (6.283185307179586 * w * w);
+  return g_src[5] * ricker * std::exp(-0.5 * r2 / (w * w)) * norm;
+}
+
 template <class PDE, int ORDER, int NPAR>
 struct RefSolver {
   static constexpr int Order = ORDER;
@@ -145,19 +246,28 @@ struct RefSolver {
   void nonConservativeProduct(const double* const Q, const double* const g, double* const b) {
     PDE::nonConservativeProduct(Q, g, b);
   }
-  void algebraicSource(const tarch::la::Vector<DIMENSIONS, double>&, double, const double* const,
+  void algebraicSource(const tarch::la::Vector<DIMENSIONS, double>& x, double t, const double* const,
                        double* S) {
     std::fill_n(S, NumberOfVariables, 0.0);
+    if (tl_src_on) {
+      double xs[3] = {0, 0, 0};
+      for (int d = 0; d < DIMENSIONS; d++) xs[d] = x[d];
+      S[(int)g_src[7]] = point_source(xs, t);
+    }
   }
   void viscousFlux(const double* const, const double* const, double**) {}
   void viscousEigenvalues(const double* const, const int, double* const l) {
     std::fill_n(l, NumberOfVariables, 0.0);
   }
-  // Reflective wall: mirrored normal momentum, flux of the mirrored state.
+  // Reflective wall (mirrored normal momentum) or outflow (the inner state), and the flux of
+  // that ghost state.
   void boundaryValues(const double* const, const double, const double, const int, const int normal,
                       const double* const, const double* const stateIn, const double* const,
                       double* const fluxOut, double* const stateOut) {
-    PDE::wall(stateIn, normal, stateOut);
+    if (g_bc_mode == 3)
+      std::copy_n(stateIn, NumberOfVariables, stateOut);
+    else
+      PDE::wall(stateIn, normal, stateOut);
     for (int m = NumberOfVariables; m < NumberOfVariables + NPAR; m++) stateOut[m] = stateIn[m];
     double buf[3][NumberOfVariables];
     double* F[3] = {buf[0], buf[1], buf[2]};
@@ -198,22 +308,23 @@ inline tarch::la::Vector<DIMENSIONS, double> vec(const double* x) {
 
 // One whole cell predictor exactly as the generated glue does it
 // (AbstractGenericADERDGSolverImplementation.template:168-211).
-template <class S, bool useNCP>
+template <class S, bool useNCP, bool useSource>
 int predictor(S& s, const double* luh, const double* centre, const double* dx, double t, double dt,
               double* lQi, double* rhs, double* lFi, double* gradQ, double* lQhi, double* lFhi,
               double* lQhbnd, double* lFhbnd) {
   auto invDx = tarch::la::invertEntries(vec(dx));
-  return kernels::aderdg::generic::c::spaceTimePredictorNonlinear<false, true, false, useNCP, false, S>(
+  tl_src_on = useSource && source_near(centre, dx);
+  return kernels::aderdg::generic::c::spaceTimePredictorNonlinear<useSource, true, false, useNCP, false, S>(
       s, lQhbnd, nullptr, lFhbnd, lQi, rhs, lFi, gradQ, lQhi, lFhi, luh, vec(centre), invDx, t, dt);
 }
 
 // Uniform patch driver in the global non-fused order: dt = min_cells stableTimeStepSize(luh)
 // -> predictor + volume integral (all cells) -> Rusanov on all faces -> surface integral +
-// solution update. Periodic in every direction unless `walls` is set (then every domain face is
-// a reflective wall through boundaryConditions, 3d/boundaryConditions.cpph:29-122 and glue
+// solution update. Periodic in every direction unless `walls` is set (then every domain face goes
+// through boundaryConditions: 1 reflective walls, 3 outflow, 3d/boundaryConditions.cpph:29-122 and glue
 // :307-350). Cell c = (iz*ny + iy)*nx + ix. The reference's TBB/Peano scheduler is absent from
 // the checkout; an OpenMP loop over cells and faces stands in for it.
-template <class S, bool useNCP>
+template <class S, bool useNCP, bool useSource>
 int run_patch(const int* ncell, const double* offset, const double* size, int walls, double* luh_all,
               int nsteps, double t0, double fixed_dt, double* t_out, double* dts, int* picard,
               int nthreads) {
@@ -225,6 +336,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #endif
+  g_bc_mode = walls;
   double t = t0;
   auto cellIndex = [&](int ix, int iy, int iz) -> long { return ((long)iz * ny + iy) * nx + ix; };
   for (int step = 0; step < nsteps; step++) {
@@ -250,12 +362,12 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
         const int ix = c % nx, iy = (c / nx) % ny, iz = (int)(c / ((long)nx * ny));
         double centre[3] = {offset[0] + (ix + 0.5) * dx[0], offset[1] + (iy + 0.5) * dx[1],
                             DIMENSIONS == 3 ? offset[2] + (iz + 0.5) * dx[2] : 0.0};
-        int it = predictor<S, useNCP>(s, luh_all + c * Z::luh, centre, dx, t, dt, lQi.data(),
+        int it = predictor<S, useNCP, useSource>(s, luh_all + c * Z::luh, centre, dx, t, dt, lQi.data(),
                                       rhs.data(), lFi.data(), gradQ.data(), lQhi.data(), lFhi.data(),
                                       lQhbnd.data() + c * Z::lQhbnd, lFhbnd.data() + c * Z::lFhbnd);
         iters += it;
         if (picard) picard[(long)step * nc + c] = it;
-        kernels::aderdg::generic::c::volumeIntegralNonlinear<S, useNCP, true, false, Z::v, Z::n>(
+        kernels::aderdg::generic::c::volumeIntegralNonlinear<S, useNCP || useSource, true, false, Z::v, Z::n>(
             lduh.data() + c * Z::lduh, lFhi.data(), vec(dx));
       }
     }
@@ -326,16 +438,17 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
 }  // namespace exaref
 
 #define EXAREF_S(PDE, O, P) exaref::RefSolver<exaref::PDE, O, P>
-#define EXAREF_DEFINE(NAME, PDE, O, P, NCP)                                                             \
+#define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false)
+#define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC)                                                      \
   extern "C" int NAME##_predictor(const double* luh, const double* centre, const double* dx, double t,     \
                                   double dt, double* lQi, double* rhs, double* lFi, double* gradQ,          \
                                   double* lQhi, double* lFhi, double* lQhbnd, double* lFhbnd) {             \
     EXAREF_S(PDE, O, P) s;                                                                                  \
-    return exaref::predictor<EXAREF_S(PDE, O, P), NCP>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ,     \
+    return exaref::predictor<EXAREF_S(PDE, O, P), NCP, SRC>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ,     \
                                                        lQhi, lFhi, lQhbnd, lFhbnd);                         \
   }                                                                                                         \
   extern "C" void NAME##_volume(double* lduh, const double* lFhi, const double* dx) {                        \
-    kernels::aderdg::generic::c::volumeIntegralNonlinear<EXAREF_S(PDE, O, P), NCP, true, false,             \
+    kernels::aderdg::generic::c::volumeIntegralNonlinear<EXAREF_S(PDE, O, P), NCP || SRC, true, false,      \
                                                          exaref::PDE::NumberOfVariables, O + 1>(            \
         lduh, lFhi, exaref::vec(dx));                                                                       \
   }                                                                                                         \
@@ -375,11 +488,19 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
   extern "C" int NAME##_run(const int* ncell, const double* offset, const double* size, int walls,         \
                             double* luh, int nsteps, double t0, double fixed_dt, double* t_out,             \
                             double* dts, int* picard, int nthreads) {                                       \
-    return exaref::run_patch<EXAREF_S(PDE, O, P), NCP>(ncell, offset, size, walls, luh, nsteps, t0,         \
+    return exaref::run_patch<EXAREF_S(PDE, O, P), NCP, SRC>(ncell, offset, size, walls, luh, nsteps, t0,         \
                                                        fixed_dt, t_out, dts, picard, nthreads);             \
   }
 
+extern "C" void exaref_set_source(const double* src, int active) {
+  for (int k = 0; k < 8; k++) exaref::g_src[k] = src[k];
+  exaref::g_src_active = active;
+}
+extern "C" void exaref_set_boundary(int mode) { exaref::g_bc_mode = mode; }
+
 #if DIMENSIONS == 3
+EXAREF_DEFINE_S(exaref3d_acoustic_o4_p2, AcousticPDE, 4, 2, false, true)
+EXAREF_DEFINE_S(exaref3d_elastic_o3_p3, ElasticPDE, 3, 3, false, true)
 EXAREF_DEFINE(exaref3d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref3d_euler_o5_p0, EulerPDE, 5, 0, false)

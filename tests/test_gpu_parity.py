@@ -397,3 +397,58 @@ def test_two_slabs_with_halo_match_whole_grid(exa, torch, nz, split):
     got = np.concatenate([p.get_solution() for p, _ in slabs])
     assert rel(got, ref) < TOL
     assert slabs[0][0].time()[0][0] == whole.time()[0][0]
+
+
+# ------------------------------------------------------------------------------------------
+# Linear waves with per-node material parameters, a point source and outflow / wall boundaries
+# ------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("name,order,var,bc,steps", [
+    ("acoustic", 4, 0, 3, 4),   # outflow
+    ("acoustic", 4, 0, 0, 3),   # periodic
+    ("elastic", 3, 3, 3, 4),    # outflow
+    ("elastic", 3, 3, 1, 3),    # rigid walls
+    ("elastic", 4, 3, 3, 2),
+])
+def test_patch_linear_waves_source_vs_oracle(exa, name, order, var, bc, steps):
+    import exa_scenarios as sc
+    from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC
+    pde = {"acoustic": PDE_ACOUSTIC, "elastic": PDE_ELASTIC}[name]
+    ncell, size = (5, 4, 6), [1.0, 0.8, 1.2]
+    src = sc.ricker_source(3, size, f0=4.0, variable=var, width=0.1)
+    src = src[:4] + (0.05,) + src[5:]
+    luh0 = sc.layered_medium(name, ncell, size, order, seed=2)
+    o = Oracle(3, order, pde, source=src)
+    ref = luh0.copy()
+    t_ref, dts, _ = o.run(ref, ncell, size, steps, walls=bc)
+    s = exa.Solver(pde, 3, order, npar=exa.NPAR[pde])
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    p.set_point_source(src[:3], src[3], src[4], src[5], src[6], int(src[7]))
+    p.set_solution(luh0)
+    p.step(steps)
+    got = p.get_solution()
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert rel(got, ref) < TOL
+    assert np.abs(ref - luh0).max() > 1e-3
+    assert p.status() == 0
+    p.close()
+
+
+def test_point_source_off_matches_sourceless_oracle(exa):
+    """Removing the source (exa_patch_set_point_source(NULL)) gives the source-free update."""
+    import exa_scenarios as sc
+    from pyoracle import PDE_ACOUSTIC
+    ncell, size, order = (4, 4, 4), [1.0, 1.0, 1.0], 4
+    src = sc.ricker_source(3, size, variable=0, width=0.1)
+    luh0 = sc.layered_medium("acoustic", ncell, size, order, seed=5)
+    o = Oracle(3, order, PDE_ACOUSTIC)
+    ref = luh0.copy()
+    o.run(ref, ncell, size, 2, walls=3)
+    s = exa.Solver(exa.PDE_ACOUSTIC, 3, order, npar=2)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=exa.BC_OUTFLOW)])
+    p.set_point_source(src[:3], src[3], src[4], src[5], src[6], 0)
+    p.set_point_source(None)
+    p.set_solution(luh0)
+    p.step(2)
+    assert rel(p.get_solution(), ref) < TOL
+    p.close()
