@@ -17,6 +17,8 @@
 
 #include "../../include/exa_aderdg.h"
 #include "exa_kernels.cuh"
+#include "exa_adjoint.cuh"
+#include "exa_checkpoint.h"
 
 namespace {
 
@@ -60,6 +62,9 @@ struct Ops {
   virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
   virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
   virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
+  // discrete adjoint of one step (linear systems only)
+  bool adjoint_ok = false;
+  virtual cudaError_t adjoint(const AdjArgs& a, cudaStream_t st) = 0;
 };
 
 template <class PDE, int DIM, int N, int P>
@@ -83,7 +88,33 @@ struct OpsImpl final : Ops {
     predictor_kernel<PDE, DIM, N, P, MM><<<blocks, S::TPB, smem, st>>>(a);
     return cudaGetLastError();
   }
+  bool adj_smem_set = false;
+  cudaError_t adjoint(const AdjArgs& a, cudaStream_t st) override {
+    if constexpr (PDE::kAdjoint && !PDE::kNCP) {
+      using A = AdjShape<PDE, DIM, N, P>;
+      static_assert(A::smem <= 227 * 1024, "adjoint shared memory exceeds one CTA");
+      if (a.f.nfaces > 0) {
+        adjoint_face_kernel<PDE, DIM, N, P><<<(unsigned)((a.f.nfaces + 7) / 8), 256, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+      }
+      if (a.c.ncells <= 0) return cudaSuccess;
+      if (!adj_smem_set) {
+        cudaError_t e = cudaFuncSetAttribute(adjoint_predictor_kernel<PDE, DIM, N, P>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A::smem);
+        if (e != cudaSuccess) return e;
+        adj_smem_set = true;
+      }
+      adjoint_predictor_kernel<PDE, DIM, N, P><<<(unsigned)a.c.ncells, A::TPB, A::smem, st>>>(a);
+      return cudaGetLastError();
+    } else {
+      (void)a;
+      (void)st;
+      return cudaErrorNotSupported;
+    }
+  }
   OpsImpl() {
+    adjoint_ok = PDE::kAdjoint && !PDE::kNCP;
     mixed_ok = kMixed;
     dim = DIM;
     order = N;
@@ -552,6 +583,8 @@ struct exa_patch {
   int halo_axis = -1;        // axis with EXA_BC_HALO
   long long layer = 0;       // cells per layer normal to the halo axis
   long long halo_lo_first = 0, halo_hi_first = 0;  // first real cell of the low / high boundary layer
+  // discrete adjoint workspace (allocated on the first exa_patch_adjoint_step)
+  double *adjQ = nullptr, *adjF = nullptr, *adj_iter = nullptr;
 };
 
 static void patch_free(exa_patch* p) {
@@ -559,7 +592,7 @@ static void patch_free(exa_patch* p) {
   if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
   void* ptrs[] = {p->luh, p->lduh, p->lQhbnd, p->lFhbnd, p->picard, p->cell_grid, p->grid_dx, p->grid_t,
                   p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status,
-                  p->grid_geo, p->grid_first_d, p->src, p->btype};
+                  p->grid_geo, p->grid_first_d, p->src, p->btype, p->adjQ, p->adjF, p->adj_iter};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (p->stream) cudaStreamDestroy(p->stream);
@@ -883,6 +916,8 @@ int exa_patch_set_solution(exa_patch* p, const double* luh, int on_device) {
                            p->stream));
   int r = patch_initial_dt(p);
   if (r) return r;
+  // grid_dt now holds the CFL step of the new state: a following fixed-dt step must refill it
+  p->fixed_dt = -1.0;
   EXA_CUDA(cudaStreamSynchronize(p->stream));
   return EXA_OK;
 }
@@ -1181,3 +1216,79 @@ extern "C" int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, i
   }
   return EXA_OK;
 }
+
+// ------------------------------------------------------------------------------------------
+// discrete adjoint of one step (linear acoustic / elastic systems)
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int exa_patch_set_time(exa_patch* p, double t) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  const int ng = (int)p->grids.size();
+  exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, t);
+  EXA_CUDA(cudaGetLastError());
+  return EXA_OK;
+}
+
+int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
+  if (!p || !lambda) return fail(EXA_ERR_INVALID, "null argument");
+  exa::Ops& o = *p->s->ops;
+  if (!o.adjoint_ok) return fail(EXA_ERR_UNSUPPORTED, "the adjoint is built for the acoustic and elastic systems");
+  const int S = p->s->cfg.max_picard;
+  if (S <= 0) return fail(EXA_ERR_UNSUPPORTED, "the adjoint needs a fixed Picard sweep count (max_picard > 0)");
+  if (p->s->cfg.precision != EXA_PREC_FP64) return fail(EXA_ERR_UNSUPPORTED, "the adjoint runs in FP64");
+  if (p->nbfaces > 0 || p->halo_axis >= 0)
+    return fail(EXA_ERR_UNSUPPORTED, "the adjoint supports periodic grids (no boundary or halo faces)");
+  if (!(dt > 0)) return fail(EXA_ERR_INVALID, "the adjoint needs the fixed time step of the forward step");
+  const size_t nc = (size_t)p->ncells;
+  if (!p->adjQ) EXA_CUDA(cudaMalloc(&p->adjQ, nc * o.sz_qhb * sizeof(double)));
+  if (!p->adjF) EXA_CUDA(cudaMalloc(&p->adjF, nc * o.sz_fhb * sizeof(double)));
+  if (!p->adj_iter) EXA_CUDA(cudaMalloc(&p->adj_iter, nc * (size_t)S * o.sz_lQi / (o.nvar + o.npar) * o.nvar * sizeof(double)));
+  const int ng = (int)p->grids.size();
+  if (dt != p->fixed_dt) {
+    exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, dt);
+    EXA_CUDA(cudaGetLastError());
+    p->fixed_dt = dt;
+  }
+  // forward predictor at u_k: the face traces the Rusanov adjoint linearises around
+  exa::CellArgs c = patch_args(p);
+  EXA_CUDA(o.predictor(c, p->stream, false));
+  exa::AdjArgs a;
+  a.c = c;
+  a.f = patch_faces(p);
+  a.lam = lambda;
+  a.adjQ = p->adjQ;
+  a.adjF = p->adjF;
+  a.iter = p->adj_iter;
+  a.sweeps = S;
+  EXA_CUDA(p->s->ops->adjoint(a, p->stream));
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int exa_checkpoint_schedule(int steps, int snaps, exa_ck_action* out, int capacity, int* count,
+                            long long* forward_steps) {
+  if (steps < 1 || snaps < 1 || !count) return fail(EXA_ERR_INVALID, "steps and snaps must be >= 1");
+  if (steps > 8192) return fail(EXA_ERR_INVALID, "at most 8192 steps per schedule (chain schedules for more)");
+  const int free_slots = std::min(snaps - 1, steps);
+  exa_ck::Planner plan(steps, free_slots);
+  const std::vector<exa_ck::Action> acts = plan.schedule();
+  *count = (int)acts.size();
+  long long fw = 0;
+  for (const auto& x : acts)
+    if (x.action == exa_ck::ADVANCE) fw += x.b - x.a;
+  if (forward_steps) *forward_steps = fw;
+  if (!out) return EXA_OK;
+  if (capacity < (int)acts.size()) return fail(EXA_ERR_INVALID, "capacity below the schedule length");
+  for (size_t i = 0; i < acts.size(); i++) {
+    out[i].action = acts[i].action;
+    out[i].a = acts[i].a;
+    out[i].b = acts[i].b;
+  }
+  return EXA_OK;
+}
+
+}  // extern "C"

@@ -9,6 +9,9 @@
 //   ncp<DIM>(Q, gradQ, BgradQ)       gradQ[d*V + m]  (only when kNCP)
 //   wall<DIM>(QIn, normal, QOut)     ghost state of a reflective wall (boundaryValues)
 //   static constexpr bool kSource;   the patch's point source (algebraicSource) may act on it
+//   static constexpr bool kAdjoint;  the discrete adjoint is built for it (linear systems), with
+//   flux_vjp<DIM>(Q, lF, lQ)         lQ[k] += sum_{d,m} lF[d*V + m] dF_d[m]/dQ[k], k < V + P
+//   max_speed_grad<DIM>(Q, d, g)     returns max_m |lambda_m(Q)| and sets g[k] = its dQ[k] gradient
 //
 // The bodies restate the reference applications' formulas in the same operation order so that
 // the FP64 path agrees with the reference to rounding.
@@ -22,6 +25,7 @@ struct EulerPDE {
   static constexpr int V = 5;
   static constexpr bool kNCP = false;
   static constexpr bool kSource = false;  // no algebraicSource
+  static constexpr bool kAdjoint = false;
   static constexpr int id = 0;
 
   template <int DIM, class T>
@@ -77,6 +81,7 @@ struct SWEPDE {
   static constexpr int V = 4;
   static constexpr bool kNCP = true;
   static constexpr bool kSource = false;
+  static constexpr bool kAdjoint = false;
   static constexpr int id = 1;
   static constexpr double grav = 9.81;
 
@@ -139,6 +144,7 @@ struct AcousticPDE {
   static constexpr int P = 2;
   static constexpr bool kNCP = false;
   static constexpr bool kSource = true;  // regularised point source (Ricker)
+  static constexpr bool kAdjoint = true;
   static constexpr int id = 2;
 
   template <int DIM, class T>
@@ -176,6 +182,32 @@ struct AcousticPDE {
     for (int k = 0; k < 3; k++)
       if (k == normal) Qout[1 + k] = -Qout[1 + k];
   }
+  // transposed flux Jacobian with respect to (p, u, v, w, rho, c)
+  template <int DIM>
+  static __device__ __forceinline__ void flux_vjp(const double* Q, const double* lF, double* lQ) {
+    const double rho = Q[4], c = Q[5];
+    const double K = rho * c * c;
+    const double ir = 1.0 / rho;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double a = lF[4 * d];          // against F_d[0] = K u_d
+      const double b = lF[4 * d + 1 + d];  // against F_d[1 + d] = p / rho
+      const double ud = d == 0 ? Q[1] : (d == 1 ? Q[2] : Q[3]);
+      if (d == 0) lQ[1] += K * a;
+      if (d == 1) lQ[2] += K * a;
+      if (d == 2) lQ[3] += K * a;
+      lQ[0] += b * ir;
+      lQ[4] += a * c * c * ud - b * Q[0] * ir * ir;
+      lQ[5] += a * 2.0 * rho * c * ud;
+    }
+  }
+  template <int DIM>
+  static __device__ __forceinline__ double max_speed_grad(const double* Q, int, double* g) {
+#pragma unroll
+    for (int k = 0; k < 6; k++) g[k] = 0.0;
+    g[5] = Q[5] >= 0.0 ? 1.0 : -1.0;
+    return fabs(Q[5]);
+  }
 };
 
 // Linear elasticity, velocity-stress form with per-node parameters (V = 9: v1 v2 v3 s11 s22 s33
@@ -188,6 +220,7 @@ struct ElasticPDE {
   static constexpr int P = 3;
   static constexpr bool kNCP = false;
   static constexpr bool kSource = true;  // regularised point source (Ricker)
+  static constexpr bool kAdjoint = true;
   static constexpr int id = 3;
 
   template <int DIM, class T>
@@ -241,6 +274,63 @@ struct ElasticPDE {
 #pragma unroll
     for (int k = 0; k < 3; k++) Qout[k] = -Qout[k];
     (void)normal;
+  }
+  // transposed flux Jacobian with respect to (v1 v2 v3 s11 s22 s33 s12 s13 s23, rho, cp, cs)
+  template <int DIM>
+  static __device__ __forceinline__ void flux_vjp(const double* Q, const double* lF, double* lQ) {
+    const double rho = Q[9], cp = Q[10], cs = Q[11];
+    const double mu = rho * cs * cs;
+    const double lam = rho * cp * cp - 2.0 * mu;
+    const double ir = 1.0 / rho;
+    const double sg[3][3] = {{Q[3], Q[6], Q[7]}, {Q[6], Q[4], Q[8]}, {Q[7], Q[8], Q[5]}};
+    // slot of stress s_ij in Q
+    constexpr int sidx[3][3] = {{3, 6, 7}, {6, 4, 8}, {7, 8, 5}};
+    double g_lam = 0.0, g_mu = 0.0, g_ir = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const double* f = lF + 9 * d;
+      // f_i = -s_id / rho
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        lQ[sidx[i][d]] -= f[i] * ir;
+        g_ir -= f[i] * sg[i][d];
+      }
+      const double vd = Q[d];
+      // f_{3+k} = -(lambda v_d + 2 mu v_d delta_kd)
+      const double fsum = f[3] + f[4] + f[5];
+      lQ[d] -= lam * fsum + 2.0 * mu * f[3 + d];
+      g_lam -= vd * fsum;
+      g_mu -= 2.0 * vd * f[3 + d];
+      // shear: f6 = -mu (d0 v1 + d1 v0), f7 = -mu (d0 v2 + d2 v0), f8 = -mu (d1 v2 + d2 v1)
+      if (d == 0) {
+        lQ[1] -= mu * f[6];
+        lQ[2] -= mu * f[7];
+        g_mu -= Q[1] * f[6] + Q[2] * f[7];
+      } else if (d == 1) {
+        lQ[0] -= mu * f[6];
+        lQ[2] -= mu * f[8];
+        g_mu -= Q[0] * f[6] + Q[2] * f[8];
+      } else {
+        lQ[0] -= mu * f[7];
+        lQ[1] -= mu * f[8];
+        g_mu -= Q[0] * f[7] + Q[1] * f[8];
+      }
+    }
+    // lambda = rho cp^2 - 2 rho cs^2, mu = rho cs^2, 1/rho
+    lQ[9] += g_lam * (cp * cp - 2.0 * cs * cs) + g_mu * cs * cs - g_ir * ir * ir;
+    lQ[10] += g_lam * 2.0 * rho * cp;
+    lQ[11] += -g_lam * 4.0 * rho * cs + g_mu * 2.0 * rho * cs;
+  }
+  template <int DIM>
+  static __device__ __forceinline__ double max_speed_grad(const double* Q, int, double* g) {
+#pragma unroll
+    for (int k = 0; k < 12; k++) g[k] = 0.0;
+    if (fabs(Q[10]) >= fabs(Q[11])) {
+      g[10] = Q[10] >= 0.0 ? 1.0 : -1.0;
+      return fabs(Q[10]);
+    }
+    g[11] = Q[11] >= 0.0 ? 1.0 : -1.0;
+    return fabs(Q[11]);
   }
 };
 

@@ -65,6 +65,13 @@ class PointSource(ctypes.Structure):
                 ("amplitude", ctypes.c_double), ("width", ctypes.c_double), ("variable", ctypes.c_int)]
 
 
+class CkAction(ctypes.Structure):
+    _fields_ = [("action", ctypes.c_int), ("a", ctypes.c_int), ("b", ctypes.c_int)]
+
+
+CK_STORE, CK_RESTORE, CK_ADVANCE, CK_ADJOINT = 0, 1, 2, 3
+
+
 class _PatchStats(ctypes.Structure):
     _fields_ = [("steps", ctypes.c_longlong), ("picard_mean", ctypes.c_double), ("picard_hist", ctypes.c_int * 32)]
 
@@ -115,6 +122,10 @@ def load_library(path=None):
         "exa_patch_dt_copy": [vp, vp, i],
         "exa_build_face_lists": [i, i, ctypes.POINTER(GridDesc), ctypes.POINTER(FaceLists)],
         "exa_patch_set_point_source": [vp, ctypes.POINTER(PointSource)],
+        "exa_patch_set_time": [vp, d],
+        "exa_patch_adjoint_step": [vp, vp, d],
+        "exa_checkpoint_schedule": [i, i, ctypes.POINTER(CkAction), i, ctypes.POINTER(ctypes.c_int),
+                                    ctypes.POINTER(ctypes.c_longlong)],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -306,6 +317,19 @@ def build_face_lists(dim, grids):
             "bcell": bcell[:fl.nbfaces], "bface": bface[:fl.nbfaces]}
 
 
+def checkpoint_schedule(steps, snaps):
+    """Host-only: the binomial checkpointing schedule (list of (action, a, b)) and its forward steps."""
+    lib = load_library()
+    cnt = ctypes.c_int(0)
+    fw = ctypes.c_longlong(0)
+    _check(lib.exa_checkpoint_schedule(int(steps), int(snaps), None, 0, ctypes.byref(cnt), ctypes.byref(fw)),
+           "exa_checkpoint_schedule")
+    arr = (CkAction * cnt.value)()
+    _check(lib.exa_checkpoint_schedule(int(steps), int(snaps), arr, cnt.value, ctypes.byref(cnt), ctypes.byref(fw)),
+           "exa_checkpoint_schedule")
+    return [(x.action, x.a, x.b) for x in arr], int(fw.value)
+
+
 class Patch:
     """Device-resident uniform grid(s); the step is one CUDA graph launch."""
 
@@ -346,6 +370,13 @@ class Patch:
 
     def dt_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_copy")
+
+    def set_time(self, t):
+        _check(self.lib.exa_patch_set_time(self.h, float(t)), "exa_patch_set_time")
+
+    def adjoint_step(self, lam, dt):
+        """lam (CUDA float64 tensor, luh layout): dJ/du_{k+1} in, dJ/du_k out (parameters accumulate)."""
+        _check(self.lib.exa_patch_adjoint_step(self.h, _ptr(lam), float(dt)), "exa_patch_adjoint_step")
 
     def close(self):
         if getattr(self, "h", None):

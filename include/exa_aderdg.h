@@ -282,6 +282,38 @@ typedef struct {
 } exa_face_lists;
 int exa_build_face_lists(int dim, int ngrids, const exa_grid_desc* grids, exa_face_lists* out);
 
+/* ---- discrete adjoint (acoustic and elastic systems) -----------------------------------------
+ * No reference counterpart: the reference has no adjoint. The forward step differentiated is
+ * exa_patch_step(p, 1, dt) with a fixed dt and a solver created with max_picard > 0 (the
+ * reference's UseMaxPicardIterations mode: a fixed Picard sweep count, no residual test), on
+ * periodic grids, FP64.
+ *
+ * exa_patch_adjoint_step: the patch's current solution is u_k at time t_k (exa_patch_set_time).
+ * lambda (device, luh layout: D doubles per node) holds dJ/du_{k+1} on entry and
+ * (d u_{k+1} / d u_k)^T lambda on exit. The material-parameter entries V..D-1 accumulate: their
+ * entry value plus the step's parameter adjoint, so after the adjoint of step 0 they hold
+ * dJ/d(parameters) per node. The patch's solution is left unchanged; the call enqueues on the
+ * patch stream. */
+int exa_patch_set_time(exa_patch* p, double t);
+int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt);
+
+/* ---- binomial checkpointing (host only) -------------------------------------------------------
+ * A schedule that reverses `steps` time steps while holding at most `snaps` stored states (the
+ * initial state included), with the fewest forward recomputations (Griewank's binomial
+ * checkpointing, computed by dynamic programming over the split points). Actions, in order:
+ *   EXA_CK_STORE   a=slot, b=step   store the current state (which is u_step) in slot a
+ *   EXA_CK_RESTORE a=slot, b=step   make slot a's state (u_step) current
+ *   EXA_CK_ADVANCE a=from, b=to     advance the current state from u_from to u_to
+ *   EXA_CK_ADJOINT a=step           adjoint of step a (current state u_a)
+ * The first action stores u_0 in slot 0. With out == NULL only *count and *forward_steps are
+ * set; otherwise at most `capacity` actions are written (EXA_ERR_INVALID if too few). */
+enum { EXA_CK_STORE = 0, EXA_CK_RESTORE = 1, EXA_CK_ADVANCE = 2, EXA_CK_ADJOINT = 3 };
+typedef struct {
+  int action, a, b;
+} exa_ck_action;
+int exa_checkpoint_schedule(int steps, int snaps, exa_ck_action* out, int capacity, int* count,
+                            long long* forward_steps);
+
 #ifdef __cplusplus
 }
 #endif

@@ -146,7 +146,8 @@ class RefKernels:
 
     def __init__(self, dim, order, pde="euler", npar=0, source=None):
         """source: point source (x, y, z, f0, t0, amplitude, width, variable) for the acoustic and
-        elastic instantiations (process-wide setting of the library), or None."""
+        elastic instantiations (process-wide setting of the library), or None. pde "acousticfixed"
+        / "elasticfixed": the same systems with a fixed Picard count (UseMaxPicardIterations)."""
         path = os.path.join(HERE, "_ref", "libexaref%dd.so" % dim)
         if not os.path.exists(path):
             raise FileNotFoundError(path)
@@ -155,7 +156,7 @@ class RefKernels:
         if not hasattr(self.lib, self.prefix + "_predictor"):
             raise AttributeError("instantiation %s not built" % self.prefix)
         self.dim, self.n = dim, order + 1
-        self.v = {"euler": 5, "swe": 4, "acoustic": 4, "elastic": 9}[pde]
+        self.v = {"euler": 5, "swe": 4, "acoustic": 4, "elastic": 9, "acousticfixed": 4, "elasticfixed": 9}[pde]
         src = (ctypes.c_double * 8)(*(list(source) if source is not None else [0, 0, 0, 0, 0, 0, 1, 0]))
         self.lib.exaref_set_source(src, 1 if source is not None else 0)
         self.D = self.v + npar

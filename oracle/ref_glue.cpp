@@ -224,13 +224,14 @@ inline double point_source(const double* x, double t) {
   return g_src[5] * ricker * std::exp(-0.5 * r2 / (w * w)) * norm;
 }
 
-template <class PDE, int ORDER, int NPAR>
+// FIXED selects the reference's UseMaxPicardIterations mode: Order+1 sweeps, no residual test.
+template <class PDE, int ORDER, int NPAR, bool FIXED = false>
 struct RefSolver {
   static constexpr int Order = ORDER;
   static constexpr int NumberOfVariables = PDE::NumberOfVariables;
   static constexpr int NumberOfParameters = NPAR;
   static constexpr int MaxPicardIterations = ORDER + 1;
-  static constexpr bool UseMaxPicardIterations = false;
+  static constexpr bool UseMaxPicardIterations = FIXED;
   static constexpr double CFL = 0.9;
   static constexpr double PNPM = kPNPM[ORDER];
   static constexpr bool UseLobattoBasis = false;
@@ -275,12 +276,12 @@ struct RefSolver {
     std::copy_n(F[normal], NumberOfVariables, fluxOut);
   }
 };
-template <class P, int O, int N> double** RefSolver<P, O, N>::weights = kernels::legendre::weights;
-template <class P, int O, int N> double** RefSolver<P, O, N>::nodes = kernels::legendre::nodes;
-template <class P, int O, int N> double*** RefSolver<P, O, N>::Kxi = kernels::legendre::Kxi;
-template <class P, int O, int N> double*** RefSolver<P, O, N>::dudx = kernels::legendre::dudx;
-template <class P, int O, int N> double*** RefSolver<P, O, N>::iK1 = kernels::legendre::iK1;
-template <class P, int O, int N> double*** RefSolver<P, O, N>::FCoeff = kernels::legendre::FCoeff;
+template <class P, int O, int N, bool X> double** RefSolver<P, O, N, X>::weights = kernels::legendre::weights;
+template <class P, int O, int N, bool X> double** RefSolver<P, O, N, X>::nodes = kernels::legendre::nodes;
+template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::Kxi = kernels::legendre::Kxi;
+template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::dudx = kernels::legendre::dudx;
+template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::iK1 = kernels::legendre::iK1;
+template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::FCoeff = kernels::legendre::FCoeff;
 
 template <class S>
 struct Sizes {
@@ -437,58 +438,58 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
 
 }  // namespace exaref
 
-#define EXAREF_S(PDE, O, P) exaref::RefSolver<exaref::PDE, O, P>
-#define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false)
-#define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC)                                                      \
+#define EXAREF_S(PDE, O, P, X) exaref::RefSolver<exaref::PDE, O, P, X>
+#define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false, false)
+#define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC, FIXED)                                               \
   extern "C" int NAME##_predictor(const double* luh, const double* centre, const double* dx, double t,     \
                                   double dt, double* lQi, double* rhs, double* lFi, double* gradQ,          \
                                   double* lQhi, double* lFhi, double* lQhbnd, double* lFhbnd) {             \
-    EXAREF_S(PDE, O, P) s;                                                                                  \
-    return exaref::predictor<EXAREF_S(PDE, O, P), NCP, SRC>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ,     \
+    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
+    return exaref::predictor<EXAREF_S(PDE, O, P, FIXED), NCP, SRC>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ,     \
                                                        lQhi, lFhi, lQhbnd, lFhbnd);                         \
   }                                                                                                         \
   extern "C" void NAME##_volume(double* lduh, const double* lFhi, const double* dx) {                        \
-    kernels::aderdg::generic::c::volumeIntegralNonlinear<EXAREF_S(PDE, O, P), NCP || SRC, true, false,      \
+    kernels::aderdg::generic::c::volumeIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED), NCP || SRC, true, false,      \
                                                          exaref::PDE::NumberOfVariables, O + 1>(            \
         lduh, lFhi, exaref::vec(dx));                                                                       \
   }                                                                                                         \
   extern "C" void NAME##_riemann(double* FL, double* FR, const double* QL, const double* QR, double t,      \
                                  double dt, const double* dx, int direction) {                              \
-    EXAREF_S(PDE, O, P) s;                                                                                  \
-    kernels::aderdg::generic::c::riemannSolverNonlinear<NCP, false, EXAREF_S(PDE, O, P)>(                   \
+    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
+    kernels::aderdg::generic::c::riemannSolverNonlinear<NCP, false, EXAREF_S(PDE, O, P, FIXED)>(                   \
         s, FL, FR, QL, QR, t, dt, exaref::vec(dx), direction);                                              \
   }                                                                                                         \
   extern "C" void NAME##_surface(double* lduh, const double* lFhbnd, const double* dx) {                    \
-    kernels::aderdg::generic::c::surfaceIntegralNonlinear<EXAREF_S(PDE, O, P),                              \
+    kernels::aderdg::generic::c::surfaceIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED),                              \
                                                           exaref::PDE::NumberOfVariables, O + 1>(           \
         lduh, lFhbnd, exaref::vec(dx));                                                                     \
   }                                                                                                         \
   extern "C" void NAME##_face(double* lduh, const double* lFhbnd, int direction, int orientation,           \
                               const double* dx) {                                                           \
-    kernels::aderdg::generic::c::faceIntegralNonlinear<EXAREF_S(PDE, O, P), exaref::PDE::NumberOfVariables, \
+    kernels::aderdg::generic::c::faceIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED), exaref::PDE::NumberOfVariables, \
                                                        O + 1>(lduh, lFhbnd, direction, orientation,         \
                                                               exaref::vec(dx));                             \
   }                                                                                                         \
   extern "C" void NAME##_update(double* luh, const double* luhOld, const double* lduh, double dt) {        \
-    EXAREF_S(PDE, O, P) s;                                                                                  \
-    kernels::aderdg::generic::c::solutionUpdate<EXAREF_S(PDE, O, P)>(s, luh, luhOld, lduh, dt);             \
+    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
+    kernels::aderdg::generic::c::solutionUpdate<EXAREF_S(PDE, O, P, FIXED)>(s, luh, luhOld, lduh, dt);             \
   }                                                                                                         \
   extern "C" double NAME##_dt(const double* luh, const double* dx) {                                        \
-    EXAREF_S(PDE, O, P) s;                                                                                  \
-    return kernels::aderdg::generic::c::stableTimeStepSize<EXAREF_S(PDE, O, P), false>(s, luh,              \
+    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
+    return kernels::aderdg::generic::c::stableTimeStepSize<EXAREF_S(PDE, O, P, FIXED), false>(s, luh,              \
                                                                                        exaref::vec(dx));    \
   }                                                                                                         \
   extern "C" void NAME##_boundary(double* FOut, double* QOut, const double* FIn, const double* QIn,        \
                                   const double* centre, const double* dx, double t, double dt,              \
                                   int faceIndex, int normal) {                                              \
-    EXAREF_S(PDE, O, P) s;                                                                                  \
-    kernels::aderdg::generic::c::boundaryConditions<false, EXAREF_S(PDE, O, P)>(                            \
+    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
+    kernels::aderdg::generic::c::boundaryConditions<false, EXAREF_S(PDE, O, P, FIXED)>(                            \
         s, FOut, QOut, FIn, QIn, nullptr, exaref::vec(centre), exaref::vec(dx), t, dt, faceIndex, normal);  \
   }                                                                                                         \
   extern "C" int NAME##_run(const int* ncell, const double* offset, const double* size, int walls,         \
                             double* luh, int nsteps, double t0, double fixed_dt, double* t_out,             \
                             double* dts, int* picard, int nthreads) {                                       \
-    return exaref::run_patch<EXAREF_S(PDE, O, P), NCP, SRC>(ncell, offset, size, walls, luh, nsteps, t0,         \
+    return exaref::run_patch<EXAREF_S(PDE, O, P, FIXED), NCP, SRC>(ncell, offset, size, walls, luh, nsteps, t0,         \
                                                        fixed_dt, t_out, dts, picard, nthreads);             \
   }
 
@@ -499,8 +500,10 @@ extern "C" void exaref_set_source(const double* src, int active) {
 extern "C" void exaref_set_boundary(int mode) { exaref::g_bc_mode = mode; }
 
 #if DIMENSIONS == 3
-EXAREF_DEFINE_S(exaref3d_acoustic_o4_p2, AcousticPDE, 4, 2, false, true)
-EXAREF_DEFINE_S(exaref3d_elastic_o3_p3, ElasticPDE, 3, 3, false, true)
+EXAREF_DEFINE_S(exaref3d_acoustic_o4_p2, AcousticPDE, 4, 2, false, true, false)
+EXAREF_DEFINE_S(exaref3d_elastic_o3_p3, ElasticPDE, 3, 3, false, true, false)
+EXAREF_DEFINE_S(exaref3d_acousticfixed_o4_p2, AcousticPDE, 4, 2, false, true, true)
+EXAREF_DEFINE_S(exaref3d_elasticfixed_o3_p3, ElasticPDE, 3, 3, false, true, true)
 EXAREF_DEFINE(exaref3d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref3d_euler_o5_p0, EulerPDE, 5, 0, false)
