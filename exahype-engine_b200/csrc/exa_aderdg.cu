@@ -651,7 +651,7 @@ static int patch_enqueue_step(exa_patch* p, bool cfl) {
     exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, p->grid_dt_next, p->steps);
   } else {
     // fixed dt: t += dt, dt unchanged
-    exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, p->grid_dt, p->steps);
+    exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, nullptr, p->steps);
   }
   EXA_CUDA(cudaGetLastError());
   return EXA_OK;
@@ -1038,7 +1038,7 @@ int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt) {
     }
     case EXA_PHASE_ADVANCE: {
       exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt,
-                                                                   cfl ? p->grid_dt_next : p->grid_dt, p->steps);
+                                                                   cfl ? p->grid_dt_next : nullptr, p->steps);
       EXA_CUDA(cudaGetLastError());
       return EXA_OK;
     }

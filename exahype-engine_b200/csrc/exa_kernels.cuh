@@ -466,12 +466,15 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
 }
 
 // t += dt, dt = dt_next, dt_next = +inf for every grid (one thread per grid).
+// dt_next == nullptr: a fixed time step, dt stays as it is
 __global__ void advance_kernel(int ngrids, double* t, double* dt, double* dt_next, long long* steps) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ngrids) return;
   t[g] += dt[g];
-  dt[g] = dt_next[g];
-  dt_next[g] = __longlong_as_double(0x7ff0000000000000ll);
+  if (dt_next) {
+    dt[g] = dt_next[g];
+    dt_next[g] = __longlong_as_double(0x7ff0000000000000ll);
+  }
   if (g == 0 && steps) steps[0] += 1;
 }
 

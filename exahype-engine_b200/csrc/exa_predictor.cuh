@@ -431,8 +431,9 @@ predictor_kernel(CellArgs a) {
       if (!finite(rr) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
       // exit test (:407-412): |res|^2 < 1e-7^2, unless a fixed sweep count is requested
       if (a.max_picard <= 0 && rr < 1e-7 * 1e-7) done = true;
-      if (!done) {
-        // the new iterate becomes the old one
+      // the new iterate becomes the old one, except after the last sweep: lFhi is the flux of
+      // the iterate that sweep started from (a fixed sweep count, or the cap without convergence)
+      if (!done && s + 1 < maxIter) {
 #pragma unroll
         for (int t = 0; t < n; t++)
 #pragma unroll

@@ -136,7 +136,7 @@ def test_misfit_gradient_vs_gpu_fd_and_checkpoint_budget(exa, torch):
     J = Misfit.apply(params, field, inv, data)
     J.backward()
     gp, gf = params.grad.clone(), field.grad.clone()
-    assert float(J) > 0 and torch.isfinite(gp).all() and torch.isfinite(gf).all()
+    assert float(J.detach()) > 0 and torch.isfinite(gp).all() and torch.isfinite(gf).all()
     rng = np.random.default_rng(5)
     for k in range(4):
         vp = torch.tensor(rng.normal(size=tuple(params.shape)), device=dev) * params.detach()

@@ -452,3 +452,59 @@ def test_point_source_off_matches_sourceless_oracle(exa):
     p.step(2)
     assert rel(p.get_solution(), ref) < TOL
     p.close()
+
+
+@pytest.mark.parametrize("pde_name,order,bc", [("euler", 3, 0), ("acoustic", 4, 3), ("elastic", 3, 1)])
+def test_patch_fixed_picard_count_vs_oracle(exa, pde_name, order, bc):
+    """max_picard = Order+1: the reference's fixed-count mode (no residual test); lFhi is the flux
+    of the last sweep's starting iterate."""
+    import exa_scenarios as sc
+    from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC, PDE_EULER
+    ncell, size, steps = (4, 3, 5), [1.0, 0.75, 1.25], 3
+    if pde_name == "euler":
+        rng = np.random.default_rng(2)
+        luh0 = euler_cells(rng, int(np.prod(ncell)), (order + 1) ** 3, amp=0.05).reshape(-1)
+        pde, src = PDE_EULER, None
+    else:
+        pde = PDE_ACOUSTIC if pde_name == "acoustic" else PDE_ELASTIC
+        luh0 = sc.layered_medium(pde_name, ncell, size, order, seed=6)
+        src = sc.ricker_source(3, size, f0=4.0, variable=0 if pde_name == "acoustic" else 3, width=0.1)
+        src = src[:4] + (0.05,) + src[5:]
+    o = Oracle(3, order, pde, source=src, max_picard=order + 1)
+    ref = luh0.copy()
+    t_ref, _, pic = o.run(ref, ncell, size, steps, walls=bc, want_picard=True)
+    assert (pic == order + 1).all()
+    s = exa.Solver(pde, 3, order, npar=exa.NPAR[pde], max_picard=order + 1)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    if src is not None:
+        p.set_point_source(src[:3], src[3], src[4], src[5], src[6], int(src[7]))
+    p.set_solution(luh0)
+    p.step(steps)
+    assert rel(p.get_solution(), ref) < TOL
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    p.close()
+
+
+def test_patch_fixed_dt_many_steps_vs_oracle(exa):
+    """Several steps with a fixed time step, through exa_patch_step and through the phases."""
+    rng = np.random.default_rng(8)
+    order, ncell, size, steps = 3, (3, 4, 3), [0.9, 1.0, 0.8], 5
+    luh0 = euler_cells(rng, int(np.prod(ncell)), (order + 1) ** 3, amp=0.04).reshape(-1)
+    o = Oracle(3, order)
+    ref = luh0.copy()
+    dt = 0.5 * min(o.dt(luh0[c * 64 * 5:(c + 1) * 64 * 5], np.array(size) / np.array(ncell)) for c in range(36))
+    t_ref, dts, _ = o.run(ref, ncell, size, steps, fixed_dt=dt)
+    assert np.all(dts == dt)
+    s = exa.Solver(exa.PDE_EULER, 3, order)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size)])
+    p.set_solution(luh0)
+    p.step(steps, dt)
+    assert rel(p.get_solution(), ref) < TOL
+    t, dtp = p.time()
+    assert abs(t[0] - steps * dt) <= 1e-14 and dtp[0] == dt
+    p.set_solution(luh0)
+    for _ in range(steps):
+        for ph in (exa.PHASE_PREDICTOR, exa.PHASE_FACES, exa.PHASE_UPDATE, exa.PHASE_ADVANCE):
+            p.step_phase(ph, dt)
+    assert rel(p.get_solution(), ref) < TOL
+    p.close()

@@ -327,3 +327,33 @@ def test_linear_source_patch_run_vs_ref(name, order, npar, var, walls):
     assert np.array_equal(pa + 1, pb)  # break index vs sweep count
     assert relerr(lb, la) < 1e-12
     assert np.abs(lb - luh0).max() > 1e-3  # the waves and the source did act
+
+
+@pytest.mark.parametrize("name,order,npar,var", LINEAR)
+def test_linear_fixed_picard_count_vs_ref(name, order, npar, var):
+    """The reference's UseMaxPicardIterations mode (Order+1 sweeps, no residual test)."""
+    from exa_scenarios import layered_medium, ricker_source
+    from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC
+    size = [1.0, 0.8, 1.2]
+    src = ricker_source(3, size, f0=4.0, variable=var, width=0.1)
+    src = src[:4] + (0.05,) + src[5:]
+    try:
+        ref = RefKernels(3, order, name + "fixed", npar, source=src)
+    except (FileNotFoundError, AttributeError, OSError) as e:
+        pytest.skip("reference kernels not built: %s" % e)
+    o = Oracle(3, order, {"acoustic": PDE_ACOUSTIC, "elastic": PDE_ELASTIC}[name], source=src,
+               max_picard=order + 1)
+    ncell = (4, 3, 5)
+    luh0 = layered_medium(name, ncell, size, order, seed=4)
+    la, lb = luh0.copy(), luh0.copy()
+    dt = 0.5 * ref.dt(luh0[:(order + 1) ** 3 * o.D], np.array(size) / np.array(ncell))
+    ref.run(la, ncell, size, 3, walls=3, fixed_dt=dt)
+    o.run(lb, ncell, size, 3, walls=3, fixed_dt=dt)
+    assert relerr(lb, la) < 1e-12
+    # single cell: every output of the predictor
+    dx = np.array([0.2, 0.2, 0.2])
+    luh = luh0[:(order + 1) ** 3 * o.D].copy()
+    a = ref.predictor(luh, dx, dt, centre=[src[0], src[1], src[2]], t=0.01)
+    b = o.predictor(luh, dx, dt, centre=[src[0], src[1], src[2]], t=0.01)
+    for key in ("lQhi", "lFhi", "lQhbnd", "lFhbnd"):
+        assert relerr(b[key], a[key]) < 1e-13, key
