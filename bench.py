@@ -41,8 +41,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "swe_batched"],
-                    help="euler3d: the headline workload; swe_batched: 512 wall-bounded 2D SWE grids, N=4")
+    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "swe_batched", "acoustic_adjoint"],
+                    help="euler3d: the headline workload; swe_batched: 512 wall-bounded 2D SWE grids, N=4; "
+                         "acoustic_adjoint: misfit gradient of a 32^3 N=4 acoustic run, 300 steps")
+    ap.add_argument("--fd-directions", type=int, default=16, help="acoustic_adjoint: finite-difference checks")
     return ap.parse_args()
 
 
@@ -101,6 +103,9 @@ def flops_per_cell_step(sweeps):
 
 
 PRED_BYTES_PER_CELL = 8.0 * (1080 + 1080 + 1080 + 1080)  # luh in; lduh, lQhbnd, lFhbnd out
+# DRAM bytes per cell of one predictor launch measured by ncu on a 27^3 block (19,683 cells):
+# 170.87 MB read + 456.64 MB written
+PRED_DRAM_BYTES_PER_CELL = (170.872832e6 + 456.639744e6) / 19683
 
 
 def cpu_baseline(steps=2, kind="reference"):
@@ -217,6 +222,111 @@ def run_swe_batched(args):
     print(json.dumps(line), flush=True)
 
 
+def run_acoustic_adjoint(args):
+    """Gradient of a receiver misfit with respect to per-cell (rho, c) and the initial pressure:
+    3D acoustics, N=4, 32^3 periodic cells, 300 fixed steps, 64 receivers, binomial checkpointing
+    with 20 stored states. One timed "step" is one whole gradient (forward run with the receivers,
+    reverse sweep with recomputation). Checked against central finite differences (h = 1e-6)
+    of the GPU forward model along seeded random directions."""
+    import torch
+    import exa_aderdg as exa
+    from exa_adjoint import Misfit, WaveInversion, acoustic_model, cfl_dt, fd_directional
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    ncell, size, order, nsteps, snaps = (32, 32, 32), [1.0, 1.0, 1.0], 4, 300, 20
+    m = acoustic_model(ncell, size, order, seed=0, width=0.05)
+    dt = cfl_dt(ncell, size, order, float(m["c_true"].max()))
+    inv = WaveInversion(exa.PDE_ACOUSTIC, ncell, size, order, dt, nsteps, m["receivers"], snaps=snaps)
+    dev = torch.device("cuda")
+    p0 = torch.tensor(m["p0"], device=dev)
+    data = inv.forward_traces(inv.assemble(torch.tensor(np.stack([m["rho"], m["c_true"]], -1), device=dev), p0))
+    params0 = torch.tensor(np.stack([m["rho"], m["c"]], -1), device=dev)
+    stream = inv.stream
+
+    def gradient():
+        params = params0.clone().requires_grad_(True)
+        field = p0.clone().requires_grad_(True)
+        J = Misfit.apply(params, field, inv, data)
+        J.backward()
+        return J.detach(), params.grad, field.grad
+
+    W, K = max(args.warmup, 1), max(args.steps, 1)
+    for _ in range(W):
+        gradient()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        ev0.record(stream)
+        for _ in range(K):
+            J, gp, gf = gradient()
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / K
+    # forward step and adjoint step alone
+    luh0 = inv.assemble(params0, p0)
+    inv._set(luh0, 0)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    inv.patch.step(20, dt)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms_fwd = ev0.elapsed_time(ev1) / 20
+    lam = torch.randn((inv.ncells, inv.nd, inv.D), dtype=torch.float64, device=dev)
+    inv._set(luh0, 0)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(20):
+        inv.patch.adjoint_step(lam, dt)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms_adj = ev0.elapsed_time(ev1) / 20
+    # finite differences along seeded directions
+    rng = np.random.default_rng(1)
+    errs = []
+    for _ in range(args.fd_directions):
+        vp = torch.tensor(rng.normal(size=tuple(params0.shape)), device=dev) * params0
+        vf = torch.tensor(rng.normal(size=tuple(p0.shape)), device=dev)
+        fd = fd_directional(inv, params0, p0, vp, vf, data, h=1e-6)
+        ad = float((gp * vp).sum() + (gf * vf).sum())
+        errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+    errs_all = list(errs)
+    cells = inv.ncells
+    dof_step = cells * inv.V * inv.nd
+    line = {"metric": "ADER-DG adjoint gradient, simulated DoF-updates/s (3D acoustic N=4, 32^3, 300 steps)",
+            "value": nsteps * dof_step / (ms * 1e-3), "unit": "DoF-updates/s", "n_gpus": 1, "steps": K,
+            "warmup": W, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "misfit gradient w.r.t. per-cell (rho, c) and initial pressure: 3D acoustics "
+                                   "N=4, 32^3 periodic cells, fixed dt, %d Picard sweeps, %d steps, 64 receivers, "
+                                   "binomial checkpointing with %d stored states" % (order + 1, nsteps, snaps),
+                       "cells": cells, "dof_per_step": dof_step, "recomputed_steps": inv.recompute_steps,
+                       "dt": dt},
+            "forward_ms_per_step": ms_fwd, "adjoint_ms_per_step": ms_adj,
+            "gradient_s": ms * 1e-3, "misfit": float(J),
+            "fd_check": {"directions": len(errs), "h": 1e-6, "max_rel_err": max(errs) if errs else None,
+                         "median_rel_err": float(np.median(errs)) if errs else None,
+                         "rel_err_per_direction": errs_all},
+            "gpu_launches": None, "clocks": clocks.summary()}
+    if not args.no_cpu:
+        # the reference has no adjoint: its generic kernels (fixed Picard count) time forward steps
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from pyoracle import RefKernels
+        try:
+            ref, kind = RefKernels(3, order, "acousticfixed", 2), "reference"
+            luh = luh0.cpu().numpy().reshape(-1).copy()
+            cores = os.cpu_count()
+            ref.run(luh, ncell, size, 1, fixed_dt=dt, nthreads=cores)
+            t0 = time.perf_counter()
+            ref.run(luh, ncell, size, 2, t0=dt, fixed_dt=dt, nthreads=cores)
+            el = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": 2 * dof_step / el, "unit": "DoF-updates/s", "cores": cores, "kind": kind,
+                                    "sample": "2 forward steps of the 32^3 N=4 acoustic model (fixed Picard count); "
+                                              "the reference has no adjoint, %.1f s" % el}
+        except Exception as e:  # reference kernels not built on this machine
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line), flush=True)
+    inv.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -224,6 +334,9 @@ def main():
         return
     if args.workload == "swe_batched":
         run_swe_batched(args)
+        return
+    if args.workload == "acoustic_adjoint":
+        run_acoustic_adjoint(args)
         return
     import torch
     import torch.distributed as dist
@@ -400,7 +513,11 @@ def main():
         "roofline": {"bound": "tensor", "kernel": "predictor_kernel (fused Picard + volume integral)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
-                     "traffic": None, "algorithmic_flops_per_launch": flops_launch, "launch_ms": pred_ms,
+                     "traffic": PRED_DRAM_BYTES_PER_CELL * cells,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch "
+                                       "on a 27^3 block (profiles/predictor_euler3d_n5_27cubed_ncu.md), scaled "
+                                       "by cells",
+                     "algorithmic_flops_per_launch": flops_launch, "launch_ms": pred_ms,
                      "hbm_gbs_of_launch": cells * PRED_BYTES_PER_CELL / (pred_ms * 1e-3) / 1e9,
                      "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},
         "gpu_launches": K * 4,

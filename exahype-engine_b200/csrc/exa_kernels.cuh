@@ -33,6 +33,58 @@ enum : unsigned {
   ST_BAD_DT = 8u,
 };
 
+// Shared-memory layout of the predictor's flux blocks (one block per cell, direction, variable).
+// Node p of direction d's block sits at p + (p / G1) S1 + (p / G2) S2: whole lines stay
+// contiguous (the groups are multiples of the line's footprint: n nodes for x lines, an n^2
+// plane for y lines), and the padding spreads the accesses of phase 1/3 (one thread per node)
+// and of phase 2 (one thread per line) over the 32 banks. BS is the block stride. The values
+// were chosen per (DIM, n) by counting shared-memory wavefronts of every access of a time node
+// (64-bit accesses, 16 lanes per wavefront) over candidate paddings.
+// per direction d: the group sizes G1, G2 (0 = none) and the padding S1, S2 per group
+#define EXA_FLUX_LAYOUT(g1x, g1y, s1x, s1y, g2x, s2x, ext)                                   \
+  static __host__ __device__ constexpr int G1(int d) { return d == 0 ? g1x : (d == 1 ? g1y : 0); } \
+  static __host__ __device__ constexpr int S1(int d) { return d == 0 ? s1x : (d == 1 ? s1y : 0); } \
+  static __host__ __device__ constexpr int G2(int d) { return d == 0 ? g2x : 0; }                  \
+  static __host__ __device__ constexpr int S2(int d) { return d == 0 ? s2x : 0; }                  \
+  static constexpr int extra = ext;
+template <int DIM, int n>
+struct FluxLayout {  // default: unpadded, odd block stride
+  EXA_FLUX_LAYOUT(0, 0, 0, 0, 0, 0, 1)
+};
+template <>
+struct FluxLayout<3, 6> {  // N=5: 1700 -> 1386 wavefronts per time node (ideal 1248)
+  EXA_FLUX_LAYOUT(48, 36, 3, 2, 96, 10, 0)
+};
+template <>
+struct FluxLayout<3, 4> {  // N=3: conflict-free
+  EXA_FLUX_LAYOUT(16, 16, 1, 4, 0, 0, 0)
+};
+template <>
+struct FluxLayout<3, 5> {  // N=4: unpadded lines, block stride 137
+  EXA_FLUX_LAYOUT(0, 0, 0, 0, 0, 0, 12)
+};
+template <>
+struct FluxLayout<2, 4> {
+  EXA_FLUX_LAYOUT(0, 0, 0, 0, 0, 0, 5)
+};
+template <>
+struct FluxLayout<2, 5> {
+  EXA_FLUX_LAYOUT(0, 0, 0, 0, 0, 0, 0)
+};
+#undef EXA_FLUX_LAYOUT
+template <int DIM, int n>
+__host__ __device__ constexpr int flux_off(int d, int p) {
+  using F = FluxLayout<DIM, n>;
+  return p + (F::G1(d) ? (p / F::G1(d)) * F::S1(d) : 0) + (F::G2(d) ? (p / F::G2(d)) * F::S2(d) : 0);
+}
+template <int DIM, int n>
+constexpr int flux_block() {
+  constexpr int nd = DIM == 3 ? n * n * n : n * n;
+  int mx = 0;
+  for (int d = 0; d < DIM; d++) mx = flux_off<DIM, n>(d, nd - 1) + 1 > mx ? flux_off<DIM, n>(d, nd - 1) + 1 : mx;
+  return mx + FluxLayout<DIM, n>::extra;
+}
+
 template <class PDE, int DIM, int N, int P>
 struct Shape {
   static constexpr int n = N + 1;
@@ -46,9 +98,8 @@ struct Shape {
   static constexpr int sizeQhb = 2 * DIM * nf * D;
   static constexpr int sizeFhb = 2 * DIM * nf * V;
   static constexpr int maxSweeps = 2 * n;
-  // flux/partials block of one (cell, dir, var): lines of n nodes, the x lines padded to n+1
-  // doubles so that neighbouring lines start in different shared-memory banks
-  static constexpr int BS = NL * (n + 1);
+  // flux/partials block of one (cell, dir, var), laid out by FluxLayout
+  static constexpr int BS = flux_block<DIM, n>();
   // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][D] + flux/partials
   static constexpr int smemQ = CPB * n * nd * D;
   static constexpr int smemF = CPB * DIM * V * BS;

@@ -28,15 +28,14 @@ namespace exa {
 
 template <int DIM, int n>
 __device__ __forceinline__ int pline_base(int d, int L) {
-  // start of line L of direction d inside a padded (dir, var) block
-  if (d == 0) return L * (n + 1);
-  if (DIM == 3 && d == 1) return (L / n) * n * n + (L % n);
-  return L;
+  // start of line L of direction d inside a padded (dir, var) block; its nodes follow with the
+  // unpadded stride (1, n, n^2), because the padding groups hold whole lines
+  return flux_off<DIM, n>(d, line_base<DIM, n>(d, L));
 }
 template <int DIM, int n>
 __device__ __forceinline__ int pnode_off(int d, int p) {
   // offset of node p inside a padded (dir, var) block
-  return d == 0 ? p + p / n : p;
+  return flux_off<DIM, n>(d, p);
 }
 
 template <class PDE, int DIM, int N, int P, bool MIXED>

@@ -203,6 +203,17 @@ class WaveInversion:
         self.patch.close()
 
 
+def fd_directional(inv, params, field0, vp, vf, data, h=1e-6):
+    """Central finite difference (J(x + h v) - J(x - h v)) / (2 h) of the misfit along (vp, vf),
+    evaluated as sum_k (tr+ - tr-) . ((tr+ + tr-)/2 - d) / (2 h): the same two model runs and the
+    same difference, without forming J+ and J- first (their leading digits cancel)."""
+    trp = inv.forward_traces(inv.assemble(params + h * vp, field0 + h * vf))
+    trm = inv.forward_traces(inv.assemble(params - h * vp, field0 - h * vf))
+    diff = (trp - trm)[1:]
+    mean = 0.5 * (trp + trm)[1:] - data[1:]
+    return float((diff * mean).sum()) / (2.0 * h)
+
+
 class Misfit(torch.autograd.Function):
     """J(params [cells, P], field0 [cells, nd] or [cells, nd, V]) for a WaveInversion and data."""
 
