@@ -41,9 +41,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="euler3d", choices=["euler3d", "swe_batched", "acoustic_adjoint"],
+    ap.add_argument("--workload", default="euler3d",
+                    choices=["euler3d", "swe_batched", "acoustic_adjoint", "elastic3d"],
                     help="euler3d: the headline workload; swe_batched: 512 wall-bounded 2D SWE grids, N=4; "
-                         "acoustic_adjoint: misfit gradient of a 32^3 N=4 acoustic run, 300 steps")
+                         "acoustic_adjoint: misfit gradient of a 32^3 N=4 acoustic run, 300 steps; "
+                         "elastic3d: layered elastic medium, N=7, 48^3 cells, absorbing faces, 10 Hz source")
+    ap.add_argument("--ncell-elastic", type=int, default=48)
+    ap.add_argument("--elastic-active", action="store_true",
+                    help="elastic3d: start from a smooth random velocity field so that every cell iterates")
     ap.add_argument("--fd-directions", type=int, default=16, help="acoustic_adjoint: finite-difference checks")
     return ap.parse_args()
 
@@ -281,13 +286,27 @@ def run_acoustic_adjoint(args):
     ms_adj = ev0.elapsed_time(ev1) / 20
     # finite differences along seeded directions
     rng = np.random.default_rng(1)
-    errs = []
+    errs, kinks = [], []
+    cgrid = params0[:, 1].reshape(ncell[2], ncell[1], ncell[0])
+
+    def kink_faces(vc, h):
+        """Faces whose Rusanov wave speed max(c_L, c_R) switches sides between c + h v and c - h v."""
+        cp_ = (params0[:, 1] + h * vc).reshape(cgrid.shape)
+        cm_ = (params0[:, 1] - h * vc).reshape(cgrid.shape)
+        cnt = 0
+        for ax in range(3):
+            dp = cp_ - torch.roll(cp_, -1, dims=ax)
+            dm = cm_ - torch.roll(cm_, -1, dims=ax)
+            cnt += int(((dp >= 0) != (dm >= 0)).sum())
+        return cnt
+
     for _ in range(args.fd_directions):
         vp = torch.tensor(rng.normal(size=tuple(params0.shape)), device=dev) * params0
         vf = torch.tensor(rng.normal(size=tuple(p0.shape)), device=dev)
         fd = fd_directional(inv, params0, p0, vp, vf, data, h=1e-6)
         ad = float((gp * vp).sum() + (gf * vf).sum())
         errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+        kinks.append(kink_faces(vp[:, 1], 1e-6))
     errs_all = list(errs)
     cells = inv.ncells
     dof_step = cells * inv.V * inv.nd
@@ -304,7 +323,8 @@ def run_acoustic_adjoint(args):
             "gradient_s": ms * 1e-3, "misfit": float(J),
             "fd_check": {"directions": len(errs), "h": 1e-6, "max_rel_err": max(errs) if errs else None,
                          "median_rel_err": float(np.median(errs)) if errs else None,
-                         "rel_err_per_direction": errs_all},
+                         "rel_err_per_direction": errs_all,
+                         "kink_faces_per_direction": kinks},
             "gpu_launches": None, "clocks": clocks.summary()}
     if not args.no_cpu:
         # the reference has no adjoint: its generic kernels (fixed Picard count) time forward steps
@@ -327,6 +347,122 @@ def run_acoustic_adjoint(args):
     inv.close()
 
 
+def fp64_peak_tflops():
+    """FP64 peak measured here with cuBLAS DGEMM 8192^3 (MEASURED_PEAKS.json carries no FP64 figure)."""
+    import torch
+    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record()
+    for _ in range(3):
+        torch.matmul(a, b)
+    g1.record()
+    g1.synchronize()
+    peak = 3 * 2 * 8192.0 ** 3 / (g0.elapsed_time(g1) * 1e-3) / 1e12
+    del a, b
+    return peak
+
+
+def elastic_flops_per_cell_step(sweeps):
+    """Algorithmic FLOPs of one cell-step, 3D elastic flux form, N=7 (n=8, v=9, D=12):
+    per Picard sweep 2(d+1) n^(d+2) v = 2,359,296 (contractions and the time solve) plus
+    n^(d+1) (flux 75 + 5v) = 491,520; tail 2 n^(d+1)(d v + D) + 4 d n^d (v + D) + 2 d n^(d+1) v
+    = 669,696 (time averaging, extrapolation, volume integral)."""
+    return 2850816.0 * sweeps + 669696.0
+
+
+def cells_of(ncell):
+    return int(np.prod(ncell))
+
+
+def run_elastic3d(args):
+    """Layered elastic medium (6 seeded horizontal layers), order 7, 48^3 cells on a 10 km cube,
+    absorbing (outflow) faces, 10 Hz Ricker source on the vertical velocity at a seeded interior
+    point, CFL time step. The streamed predictor (Picard iterates in global scratch) runs it."""
+    import torch
+    import exa_aderdg as exa
+    import exa_scenarios as sc
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = args.ncell_elastic
+    ncell, size, order = (n, n, n), [10.0, 10.0, 10.0], 7
+    luh0, table = sc.elastic_layers(ncell, size, order, seed=0)
+    if args.elastic_active:
+        x = sc.nodal_positions(ncell, size, order)
+        q = luh0.reshape(cells_of(ncell), -1, 12)
+        for k in range(3):
+            q[..., k] = 0.1 * np.sin(2 * np.pi * (k + 1) * x[..., (k + 1) % 3] / size[0])
+    src = sc.elastic_source(size, seed=0, f0=10.0, width=10.0 / n)
+    solver = exa.Solver(exa.PDE_ELASTIC, 3, order, npar=3)
+    patch = exa.Patch(solver, [dict(ncell=ncell, size=size, bc=exa.BC_OUTFLOW)])
+    patch.set_point_source(src[:3], src[3], src[4], src[5], src[6], int(src[7]))
+    patch.set_solution(luh0)
+    stream = torch.cuda.ExternalStream(patch.stream)
+    cells = int(np.prod(ncell))
+    dof_step = cells * 9 * (order + 1) ** 3
+    W, K = args.warmup, args.steps
+    patch.step(W)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        ev0.record(stream)
+        patch.step(K)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / K
+    st = patch.stats()
+    sweeps = st["picard_mean"]
+    # the predictor alone (same state, same dt)
+    reps = 3
+    ev0.record(stream)
+    for _ in range(reps):
+        patch.step_phase(exa.PHASE_PREDICTOR, 0.0)
+    ev1.record(stream)
+    ev1.synchronize()
+    pred_ms = ev0.elapsed_time(ev1) / reps
+    flops_launch = elastic_flops_per_cell_step(sweeps) * cells
+    fp64_peak = fp64_peak_tflops()
+    achieved = flops_launch / (pred_ms * 1e-3) / 1e12
+    line = {"metric": "ADER-DG DoF-updates/s (3D elastic N=7, 48^3 cells)", "value": dof_step / (ms * 1e-3),
+            "unit": "DoF-updates/s", "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "3D elastic (velocity-stress, flux form, per-cell rho/cp/cs), N=7, %d^3 cells on "
+                                   "[0,10 km]^3, 6 seeded horizontal layers, outflow faces, 10 Hz Ricker source, "
+                                   "CFL 0.9; streamed predictor" % n,
+                       "cells": cells, "dof_per_step": dof_step, "l2": "inputs 5.4 GB > L2, no flush needed"},
+            "picard_sweeps_mean": sweeps, "status_bits": patch.status(),
+            "initial_state": "smooth random velocity field" if args.elastic_active else "at rest (source-driven)",
+            "roofline": {"bound": "tensor", "kernel": "predictor_streamed_kernel", "achieved": achieved,
+                         "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                         "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run", "traffic": None,
+                         "launch_ms": pred_ms, "algorithmic_flops_per_launch": flops_launch},
+            "gpu_launches": K * 5, "clocks": clocks.summary()}
+    if not args.no_cpu:
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        from pyoracle import RefKernels
+        try:
+            ref = RefKernels(3, order, "elastic", 3, source=src)
+            sample = (12, 12, 12)
+            lsm, _ = sc.elastic_layers(sample, [10.0 * k / n for k in sample], order, seed=0)
+            cores = os.cpu_count()
+            if args.elastic_active:
+                xs = sc.nodal_positions(sample, [10.0 * k / n for k in sample], order)
+                qs = lsm.reshape(cells_of(sample), -1, 12)
+                for k in range(3):
+                    qs[..., k] = 0.1 * np.sin(2 * np.pi * (k + 1) * xs[..., (k + 1) % 3] / size[0])
+            t0 = time.perf_counter()
+            ref.run(lsm, sample, [10.0 * k / n for k in sample], 2, walls=3, nthreads=cores)
+            el = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": int(np.prod(sample)) * 9 * 512 * 2 / el, "unit": "DoF-updates/s",
+                                    "cores": cores, "kind": "reference",
+                                    "sample": "12^3 block of the same medium at the same dx, 2 steps, %.1f s" % el}
+        except Exception as e:
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    print(json.dumps(line), flush=True)
+    patch.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -337,6 +473,9 @@ def main():
         return
     if args.workload == "acoustic_adjoint":
         run_acoustic_adjoint(args)
+        return
+    if args.workload == "elastic3d":
+        run_elastic3d(args)
         return
     import torch
     import torch.distributed as dist
@@ -453,19 +592,7 @@ def main():
     e1.synchronize()
     pred_ms = e0.elapsed_time(e1) / reps
     mean_sweeps = float(pic.double().mean().item())
-    # FP64 tensor-pipe peak measured here with cuBLAS DGEMM (MEASURED_PEAKS.json carries no FP64 figure)
-    a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    b = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
-    torch.matmul(a, b)
-    torch.cuda.synchronize()
-    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    g0.record()
-    for _ in range(3):
-        torch.matmul(a, b)
-    g1.record()
-    g1.synchronize()
-    fp64_peak = 3 * 2 * 8192.0 ** 3 / (g0.elapsed_time(g1) * 1e-3) / 1e12
-    del a, b
+    fp64_peak = fp64_peak_tflops()
     flops_launch = cells * (395280.0 * mean_sweeps + 116640.0)
     achieved = flops_launch / (pred_ms * 1e-3) / 1e12
 

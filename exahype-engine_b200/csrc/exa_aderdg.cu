@@ -59,6 +59,8 @@ struct Ops {
   virtual ~Ops() {}
   bool mixed_ok = false;  // mixed-precision predictor instantiated
   virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed = false) = 0;
+  // device scratch the predictor needs for a launch over ncells (outside stream capture)
+  virtual cudaError_t reserve(long long ncells) = 0;
   virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
   virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
   virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
@@ -71,11 +73,55 @@ template <class PDE, int DIM, int N, int P>
 struct OpsImpl final : Ops {
   using S = Shape<PDE, DIM, N, P>;
   bool smem_set = false, smem_set_mixed = false;
+  // cells whose space-time state does not fit a CTA run the streamed predictor
+  static constexpr bool kStreamed = S::predictor_smem + 4096 > 227 * 1024;
   // the mixed form needs PDEs without NCP and its larger shared-memory footprint must fit a CTA
-  static constexpr bool kMixed = !PDE::kNCP && S::predictor_smem_mixed + 4096 <= 227 * 1024;
-  static_assert(S::predictor_smem + 4096 <= 227 * 1024, "predictor shared memory exceeds one CTA");
+  static constexpr bool kMixed = !kStreamed && !PDE::kNCP && S::predictor_smem_mixed + 4096 <= 227 * 1024;
+  static constexpr bool kAdj = PDE::kAdjoint && !PDE::kNCP && AdjShape<PDE, DIM, N, P>::smem <= 227 * 1024;
+  // streamed predictor: scratch per device, grown on demand
+  std::mutex scratch_mu;
+  double* scratch[64] = {};
+  size_t scratch_slots[64] = {};
+  int stream_grid[64] = {};
+  cudaError_t reserve(long long ncells) override {
+    if constexpr (kStreamed) {
+      using T = StreamShape<PDE, DIM, N, P>;
+      static_assert(T::smem + 4096 <= 227 * 1024, "streamed predictor shared memory exceeds one CTA");
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess) return e;
+      if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+      std::lock_guard<std::mutex> lk(scratch_mu);
+      if (!smem_set) {
+        e = cudaFuncSetAttribute(predictor_streamed_kernel<PDE, DIM, N, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)T::smem);
+        if (e != cudaSuccess) return e;
+        smem_set = true;
+      }
+      int sms = 0, occ = 0;
+      if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, predictor_streamed_kernel<PDE, DIM, N, P>, T::TPB,
+                                                             T::smem)) != cudaSuccess)
+        return e;
+      const long long want = std::max(1LL, std::min<long long>(ncells, (long long)sms * std::max(occ, 1)));
+      if ((size_t)want > scratch_slots[dev]) {
+        if (scratch[dev]) cudaFree(scratch[dev]);
+        scratch[dev] = nullptr;
+        scratch_slots[dev] = 0;
+        e = cudaMalloc(&scratch[dev], (size_t)want * T::slot_doubles * sizeof(double));
+        if (e != cudaSuccess) return e;
+        scratch_slots[dev] = (size_t)want;
+      }
+      stream_grid[dev] = (int)scratch_slots[dev];
+    } else {
+      (void)ncells;
+    }
+    return cudaSuccess;
+  }
   template <bool M>
   cudaError_t launch_predictor(const CellArgs& a, cudaStream_t st, bool& set) {
+    static_assert(!kStreamed, "cells of this size run the streamed predictor");
+    static_assert(S::predictor_smem + 4096 <= 227 * 1024, "predictor shared memory exceeds one CTA");
     constexpr bool MM = M && kMixed;
     const size_t smem = MM ? S::predictor_smem_mixed : S::predictor_smem;
     if (!set) {
@@ -90,7 +136,7 @@ struct OpsImpl final : Ops {
   }
   bool adj_smem_set = false;
   cudaError_t adjoint(const AdjArgs& a, cudaStream_t st) override {
-    if constexpr (PDE::kAdjoint && !PDE::kNCP) {
+    if constexpr (kAdj) {
       using A = AdjShape<PDE, DIM, N, P>;
       static_assert(A::smem <= 227 * 1024, "adjoint shared memory exceeds one CTA");
       if (a.f.nfaces > 0) {
@@ -114,7 +160,7 @@ struct OpsImpl final : Ops {
     }
   }
   OpsImpl() {
-    adjoint_ok = PDE::kAdjoint && !PDE::kNCP;
+    adjoint_ok = kAdj;
     mixed_ok = kMixed;
     dim = DIM;
     order = N;
@@ -135,11 +181,28 @@ struct OpsImpl final : Ops {
   }
   cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed) override {
     if (a.ncells <= 0) return cudaSuccess;
-    if (mixed) {
-      if (!kMixed) return cudaErrorNotSupported;
-      return launch_predictor<true>(a, st, smem_set_mixed);
+    if constexpr (kStreamed) {
+      using T = StreamShape<PDE, DIM, N, P>;
+      if (mixed) return cudaErrorNotSupported;
+      int dev = 0;
+      cudaError_t e = cudaGetDevice(&dev);
+      if (e != cudaSuccess) return e;
+      if (dev < 0 || dev >= 64 || !scratch[dev]) return cudaErrorNotReady;  // reserve() first
+      CellArgs b = a;
+      b.scratch = scratch[dev];
+      const unsigned blocks = (unsigned)std::min<long long>(a.ncells, stream_grid[dev]);
+      predictor_streamed_kernel<PDE, DIM, N, P><<<blocks, T::TPB, T::smem, st>>>(b);
+      return cudaGetLastError();
     }
-    return launch_predictor<false>(a, st, smem_set);
+    if (mixed) {
+      if constexpr (!kMixed) {
+        return cudaErrorNotSupported;
+      } else {
+        return launch_predictor<true>(a, st, smem_set_mixed);
+      }
+    }
+    if constexpr (!kStreamed) return launch_predictor<false>(a, st, smem_set);
+    return cudaErrorNotSupported;
   }
   cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
     if (a.ncells <= 0) return cudaSuccess;
@@ -183,6 +246,7 @@ Ops* find_ops(int pde, int dim, int order, int npar) {
   EXA_CASE(EXA_PDE_ACOUSTIC, AcousticPDE, 3, 4, 2)
   EXA_CASE(EXA_PDE_ELASTIC, ElasticPDE, 3, 3, 3)
   EXA_CASE(EXA_PDE_ELASTIC, ElasticPDE, 3, 4, 3)
+  EXA_CASE(EXA_PDE_ELASTIC, ElasticPDE, 3, 7, 3)
 #undef EXA_CASE
   return nullptr;
 }
@@ -299,6 +363,7 @@ int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double*
   a.lFhbnd = lFhbnd;
   a.picard = picard_sweeps;
   set_uniform(a, s, dx, dt);
+  EXA_CUDA(s->ops->reserve(ncells));
   EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream, s->cfg.precision == EXA_PREC_MIXED));
   return EXA_OK;
 }
@@ -432,7 +497,8 @@ int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbn
   double dx[3] = {1.0, 1.0, 1.0};
   for (int k = 0; k < s->cfg.dim; k++) dx[k] = 1.0 / invDx[k];
   set_uniform(a, s, dx, dt);
-  cudaError_t e = s->ops->predictor(a, 0, s->cfg.precision == EXA_PREC_MIXED);
+  cudaError_t e = s->ops->reserve(1);
+  if (e == cudaSuccess) e = s->ops->predictor(a, 0, s->cfg.precision == EXA_PREC_MIXED);
   if (e != cudaSuccess) {
     cuda_fail(e, "predictor");
     return -1;
@@ -814,7 +880,7 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   }
   p->nfaces = (int)fL.size();
   p->nbfaces = (int)bc.size();
-  const exa::Ops& o = *s->ops;
+  exa::Ops& o = *s->ops;
   const long long nc = p->ncells;
   auto alloc = [&](void** ptr, size_t bytes) -> int {
     cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 8);
@@ -881,6 +947,12 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   if (!ok) {
     patch_free(p.get());
     return cuda_fail(cudaGetLastError(), "patch upload");
+  }
+  // the streamed predictor's scratch must exist before a step is captured into a graph
+  e = o.reserve(p->ncells);
+  if (e != cudaSuccess) {
+    patch_free(p.get());
+    return cuda_fail(e, "predictor scratch");
   }
   *out = p.release();
   return EXA_OK;

@@ -144,6 +144,8 @@ struct CellArgs {
   const double* grid_t;          // [grid] time at the start of the step (nullable: u_t)
   double u_t;
   // optional export of the predictor's internals, reference layouts (per-cell shims, tests)
+  // scratch of the streamed predictor: one slot per resident CTA (set by the launcher)
+  double* scratch;
   double* ex_lQi;
   double* ex_lFi;
   double* ex_lQhi;
@@ -241,6 +243,7 @@ __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
 }  // namespace exa
 
 #include "exa_predictor.cuh"
+#include "exa_predictor_streamed.cuh"
 
 namespace exa {
 

@@ -1,0 +1,345 @@
+// Space-time predictor for cells whose space-time state does not fit a CTA's shared memory
+// (high orders with many variables, e.g. the elastic system at N=7: 8^4 x 9 doubles = 295 KB of
+// Picard iterate per cell). Same algorithm, same references and same results as
+// predictor_kernel (exa_predictor.cuh); only where the state lives differs:
+//
+//   shared memory  the flux blocks of one time node [dir][var][node] (contracted in place), and
+//                  in the tail the time-averaged state lQhi [node][D];
+//   registers      the node's luh;
+//   global scratch per resident CTA: the old and the new Picard iterate and the rhs slices,
+//                  [t][node][V] each. With one CTA per SM the scratch of all CTAs (148 x 3 x
+//                  8 x 512 x 9 doubles = 131 MB) stays mostly in L2.
+//
+// The kernel is persistent: gridDim.x CTAs walk the cells, CTA b using scratch slot b. One CTA
+// holds one cell, one thread per node (n^3 <= 1024). PDEs without NCP only.
+#pragma once
+
+namespace exa {
+
+template <class PDE, int DIM, int N, int P>
+struct StreamShape {
+  using S = Shape<PDE, DIM, N, P>;
+  static constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, NL = S::NL, BS = S::BS;
+  static constexpr int TPB = (nd + 31) / 32 * 32;
+  static constexpr int items = DIM * V * NL;
+  static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)nd * D);
+  static constexpr size_t slot_doubles = 3 * (size_t)n * nd * V;  // old, new, rhs
+};
+
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__((StreamShape<PDE, DIM, N, P>::TPB))
+predictor_streamed_kernel(CellArgs a) {
+  using T = StreamShape<PDE, DIM, N, P>;
+  using S = Shape<PDE, DIM, N, P>;
+  using G = GL<N>;
+  constexpr int n = T::n, V = T::V, D = T::D, nd = T::nd, NL = T::NL, BS = T::BS, nf = S::nf;
+  static_assert(!PDE::kNCP, "the streamed predictor is built for PDEs without NCP");
+  static_assert(T::TPB <= 1024, "one thread per node");
+  extern __shared__ double smem[];
+  double* sF = smem;                        // [DIM][V][BS]
+  double* sQh = smem + (size_t)DIM * V * BS;  // [nd][D]: lQhi in the tail
+  __shared__ double s_lw[DIM * NL];
+  __shared__ double s_red[T::TPB / 32];
+  __shared__ double s_res;
+
+  const int p = threadIdx.x;
+  const bool live_node = p < nd;
+  int co[3] = {0, 0, 0};
+  node_coords<DIM, n>(live_node ? p : 0, co);
+  const double w_sp = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
+                               : G::weights(co[1]) * G::weights(co[0]);
+  const double iweight = 1.0 / w_sp;
+  int off[DIM];
+#pragma unroll
+  for (int d = 0; d < DIM; d++) off[d] = flux_off<DIM, n>(d, live_node ? p : 0);
+  const size_t slab = (size_t)n * nd * V;
+  double* slot = a.scratch + (size_t)blockIdx.x * T::slot_doubles;
+
+  for (long cell = blockIdx.x; cell < a.ncells; cell += gridDim.x) {
+    const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+    const double dt = a.grid_dt ? a.grid_dt[g] : a.u_dt;
+    double invdx[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) invdx[d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
+    for (int j = p; j < DIM * NL; j += T::TPB) {
+      const int d = j / NL, L = j % NL;
+      const double wt = DIM == 3 ? G::weights(L / n) * G::weights(L % n) : G::weights(L);
+      s_lw[j] = wt * dt * invdx[d];
+    }
+    double u[D];
+    {
+      const double* luh = a.luh + (size_t)cell * nd * D + (size_t)(live_node ? p : 0) * D;
+#pragma unroll
+      for (int m = 0; m < D; m++) u[m] = live_node ? luh[m] : 1.0;
+    }
+    // point source (algebraicSource at x_p, t + node_i dt)
+    bool srcOn = false;
+    double tcell = 0.0;
+    const double dxv[3] = {1.0 / invdx[0], DIM > 1 ? 1.0 / invdx[1] : 1.0, DIM > 2 ? 1.0 / invdx[2] : 1.0};
+    if (PDE::kSource && a.src) {
+      double cc[3];
+      cell_centre(a, cell, g, dxv, cc);
+      srcOn = source_near<DIM>(a.src, cc, dxv);
+      tcell = a.grid_t ? a.grid_t[g] : a.u_t;
+    }
+    const int srcVar = (PDE::kSource && a.src) ? (int)a.src[7] : -1;
+    auto src_at = [&](int i) -> double {
+      double cc[3], x[3];
+      cell_centre(a, cell, g, dxv, cc);
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[d] = cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5);
+      return point_source<DIM>(a.src, x, tcell + G::nodes(i) * dt);
+    };
+    __syncthreads();
+
+    // contraction of every line with Kxi, in place, scaled by coef * s_lw
+    auto contract = [&](double coef) {
+      for (int it = p; it < T::items; it += T::TPB) {
+        const int L = it % NL, d = it / (V * NL), m = (it / NL) % V;
+        double* f = sF + (size_t)(d * V + m) * BS + flux_off<DIM, n>(d, line_base<DIM, n>(d, L));
+        const int st = line_stride<n>(d);
+        const double c = coef * s_lw[d * NL + L];
+        double x[n];
+#pragma unroll
+        for (int k = 0; k < n; k++) x[k] = f[k * st];
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+          double acc = 0.0;
+#pragma unroll
+          for (int k = 0; k < n; k++) acc = fma(x[k], G::Kxi(k, l), acc);
+          f[l * st] = c * acc;
+        }
+      }
+    };
+    auto store_flux = [&](const double* q) {
+      double F[DIM * V];
+      PDE::template flux<DIM>(q, F);
+      if (live_node) {
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int m = 0; m < V; m++) sF[(d * V + m) * BS + off[d]] = F[d * V + m];
+      }
+    };
+
+    double* qo = slot;             // old iterate [t][node][V]
+    double* qn = slot + slab;      // new iterate
+    double* R = slot + 2 * slab;   // rhs slices, scaled by 1/w_p
+    const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
+    int sweeps = 0;
+    bool last_old_is_luh = true;   // the last sweep started from lQi = luh
+    for (int s = 0; s < maxIter; s++) {
+      if (s == 0) {
+        // lQi[., t] = luh (:71-82): one flux and one set of contractions for every time node
+        store_flux(u);
+        __syncthreads();
+        contract(1.0);
+        __syncthreads();
+        if (live_node) {
+#pragma unroll
+          for (int i = 0; i < n; i++) {
+            const double wi = G::weights(i);
+            const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
+#pragma unroll
+            for (int m = 0; m < V; m++) {
+              double o = 0.0;
+#pragma unroll
+              for (int d = 0; d < DIM; d++) o += sF[(d * V + m) * BS + off[d]];
+              double rhs = w_sp * G::F0(i) * u[m] - wi * o;
+              if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
+              R[((size_t)i * nd + p) * V + m] = iweight * rhs;
+            }
+          }
+        }
+      } else {
+        for (int i = 0; i < n; i++) {
+          double q[D];
+#pragma unroll
+          for (int m = 0; m < D; m++) q[m] = (m < V && live_node) ? qo[((size_t)i * nd + p) * V + m] : u[m];
+          store_flux(q);
+          __syncthreads();
+          contract(G::weights(i));
+          __syncthreads();
+          if (live_node) {
+            const double wi = G::weights(i);
+            const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
+#pragma unroll
+            for (int m = 0; m < V; m++) {
+              double rhs = w_sp * G::F0(i) * u[m];
+#pragma unroll
+              for (int d = 0; d < DIM; d++) rhs -= sF[(d * V + m) * BS + off[d]];
+              if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
+              R[((size_t)i * nd + p) * V + m] = iweight * rhs;
+            }
+          }
+          __syncthreads();  // the next time node overwrites the flux blocks
+        }
+      }
+      // iK1 time solve (:370-405) per node, residual against the old iterate
+      double res = 0.0;
+      if (live_node) {
+#pragma unroll 1
+        for (int m = 0; m < V; m++) {
+          double r[n];
+#pragma unroll
+          for (int i = 0; i < n; i++) r[i] = R[((size_t)i * nd + p) * V + m];
+#pragma unroll
+          for (int t = 0; t < n; t++) {
+            double q = 0.0;
+#pragma unroll
+            for (int i = 0; i < n; i++) q = fma(r[i], G::iK1(t, i), q);
+            const double old = s == 0 ? u[m] : qo[((size_t)t * nd + p) * V + m];
+            const double dl = q - old;
+            res = fma(dl, dl, res);
+            qn[((size_t)t * nd + p) * V + m] = q;
+          }
+        }
+      }
+      // residual of the cell: warp tree, then the warp partials
+#pragma unroll
+      for (int o2 = 16; o2 > 0; o2 >>= 1) res += __shfl_xor_sync(0xffffffffu, res, o2);
+      if ((p & 31) == 0) s_red[p >> 5] = res;
+      __syncthreads();
+      if (p == 0) {
+        double t = 0.0;
+        for (int w = 0; w < T::TPB / 32; w++) t += s_red[w];
+        s_res = t;
+      }
+      __syncthreads();
+      const double rr = s_res;
+      sweeps = s + 1;
+      if (!finite(rr) && a.status && p == 0) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+      const bool done = a.max_picard <= 0 && rr < 1e-7 * 1e-7;
+      if (done || s + 1 == maxIter) {
+        if (!done && a.max_picard <= 0 && a.status && p == 0) atomicOr(a.status, ST_PICARD_CAP);
+        last_old_is_luh = s == 0;
+        break;
+      }
+      // the new iterate becomes the old one
+      double* t = qo;
+      qo = qn;
+      qn = t;
+      __syncthreads();
+    }
+    if (a.picard && p == 0) a.picard[cell] = sweeps;
+
+    // ---------------- time averaging (:441-515) ----------------
+    // lQhi from the new iterate; lFhi = sum_t w_t F(old iterate of the last sweep at t)
+    double qh[D];
+    if (live_node) {
+#pragma unroll
+      for (int m = 0; m < D; m++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int t = 0; t < n; t++) acc = fma(m < V ? qn[((size_t)t * nd + p) * V + m] : u[m], G::weights(t), acc);
+        qh[m] = acc;
+        sQh[(size_t)p * D + m] = acc;
+      }
+      if (a.ex_lQi) {
+        double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
+        for (int t = 0; t < n; t++)
+          for (int m = 0; m < D; m++) e[t * D + m] = m < V ? qn[((size_t)t * nd + p) * V + m] : u[m];
+      }
+      if (a.ex_lQhi)
+        for (int m = 0; m < D; m++) a.ex_lQhi[(size_t)cell * nd * D + p * D + m] = qh[m];
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) sF[(d * V + m) * BS + off[d]] = 0.0;
+#pragma unroll 1
+      for (int i = 0; i < n; i++) {
+        double q[D], F[DIM * V];
+#pragma unroll
+        for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? qo[((size_t)i * nd + p) * V + m] : u[m];
+        PDE::template flux<DIM>(q, F);
+        const double wi = G::weights(i);
+#pragma unroll
+        for (int d = 0; d < DIM; d++)
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            double* sl = &sF[(d * V + m) * BS + off[d]];
+            *sl = fma(F[d * V + m], wi, *sl);
+          }
+        if (a.ex_lFi) {
+          double* e = a.ex_lFi + (size_t)cell * n * nd * (DIM + 1) * V + ((size_t)(i * nd + p) * (DIM + 1)) * V;
+          for (int d = 0; d < DIM; d++)
+            for (int m = 0; m < V; m++) e[d * V + m] = F[d * V + m];
+          for (int m = 0; m < V; m++) e[DIM * V + m] = 0.0;
+        }
+      }
+      if (a.ex_lFhi) {
+        double* e = a.ex_lFhi + (size_t)cell * (DIM + 1) * nd * V;
+        for (int d = 0; d < DIM; d++) {
+          const int idx = node_line<DIM, n>(p, d) * n + co[d];
+          for (int m = 0; m < V; m++) e[(size_t)d * nd * V + idx * V + m] = sF[(d * V + m) * BS + off[d]];
+        }
+        for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = 0.0;
+      }
+    }
+    __syncthreads();
+
+    // ---------------- volume integral (volumeIntegralNonlinear :133-223) ----------------
+    if (live_node) {
+      double acc[V];
+#pragma unroll
+      for (int m = 0; m < V; m++) acc[m] = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        const int L = node_line<DIM, n>(p, d);
+        const int base = flux_off<DIM, n>(d, line_base<DIM, n>(d, L)), st = line_stride<n>(d);
+        const double wt = DIM == 3 ? G::weights(L / n) * G::weights(L % n) : G::weights(L);
+        const double us = wt * invdx[d];
+        const int k = co[d];
+#pragma unroll
+        for (int m = 0; m < V; m++)
+#pragma unroll
+          for (int mm = 0; mm < n; mm++) acc[m] += G::Kxi(k, mm) * sF[(d * V + m) * BS + base + mm * st] * us;
+      }
+      if (PDE::kSource && srcOn) {
+        double sa = 0.0;
+        for (int i = 0; i < n; i++) sa = fma(src_at(i), G::weights(i), sa);
+#pragma unroll
+        for (int m = 0; m < V; m++)
+          if (m == srcVar) acc[m] += w_sp * sa;
+      }
+      bool ok = true;
+      double* lduh = a.lduh + (size_t)cell * nd * V + (size_t)p * V;
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        lduh[m] = acc[m];
+        ok &= finite(acc[m]);
+      }
+      if (!ok && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+    }
+
+    // ---------------- extrapolation to the faces (:517-687) ----------------
+    for (int j = p; j < S::sizeQhb + S::sizeFhb; j += T::TPB) {
+      int r = j;
+      const bool isQ = r < S::sizeQhb;
+      if (!isQ) r -= S::sizeQhb;
+      const int W = isQ ? D : V;
+      const int m = r % W;
+      const int fn = (r / W) % nf;
+      const int face = r / (W * nf);
+      const int d = face >> 1, o = face & 1;
+      const int st = line_stride<n>(d);
+      double acc = 0.0;
+      if (isQ) {
+        if (!(DIM == 2 && d == 0 && m >= V)) {
+          const int base = line_base<DIM, n>(d, fn);
+#pragma unroll
+          for (int l = 0; l < n; l++) acc = fma(sQh[(size_t)(base + l * st) * D + m], o ? G::F1(l) : G::F0(l), acc);
+        }
+        a.lQhbnd[(size_t)cell * S::sizeQhb + r] = acc;
+      } else {
+        const double* src = sF + (size_t)(d * V + m) * BS + flux_off<DIM, n>(d, line_base<DIM, n>(d, fn));
+#pragma unroll
+        for (int l = 0; l < n; l++) acc = fma(src[l * st], o ? G::F1(l) : G::F0(l), acc);
+        a.lFhbnd[(size_t)cell * S::sizeFhb + r] = acc;
+      }
+    }
+    __syncthreads();  // shared memory and scratch are reused by the next cell
+  }
+}
+
+}  // namespace exa

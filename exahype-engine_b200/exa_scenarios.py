@@ -211,3 +211,37 @@ def ricker_source(dim, size, offset=None, f0=4.0, amplitude=1.0, width=None, var
     pos = list(off + at * size) + [0.0] * (3 - dim)
     w = float(width) if width is not None else float(0.04 * size.min())
     return tuple(pos) + (float(f0), 1.2 / float(f0), float(amplitude), w, float(variable))
+
+
+def elastic_layers(ncell, size, order, seed=0, nlayers=6, offset=None):
+    """The layered elastic configuration: nlayers horizontal layers (constant in x, y) with seeded
+    interface depths along z, per layer rho ~ U[2.0, 3.0], cp ~ U[4.0, 6.5], cs = cp / sqrt(3) *
+    U[0.9, 1.1]; parameters constant per cell (from the cell centre), the medium at rest.
+    Returns (luh [cells*nodes*12], layer table [nlayers][4] = z_top, rho, cp, cs)."""
+    rng = np.random.default_rng(seed)
+    off = np.zeros(3) if offset is None else np.asarray(offset, dtype=float)
+    size = np.asarray(size, dtype=float)
+    depths = np.sort(rng.uniform(0.0, 1.0, nlayers - 1)) * size[2] + off[2]
+    rho = rng.uniform(2.0, 3.0, nlayers)
+    cp = rng.uniform(4.0, 6.5, nlayers)
+    cs = cp / np.sqrt(3.0) * rng.uniform(0.9, 1.1, nlayers)
+    x = nodal_positions(ncell, size, order, offset)
+    cz = x.mean(axis=1)[:, 2]
+    layer = np.searchsorted(depths, cz)
+    Q = np.zeros(x.shape[:-1] + (12,))
+    Q[..., 9] = rho[layer][:, None]
+    Q[..., 10] = cp[layer][:, None]
+    Q[..., 11] = cs[layer][:, None]
+    table = np.stack([np.append(depths, size[2] + off[2]), rho, cp, cs], -1)
+    return Q.reshape(-1), table
+
+
+def elastic_source(size, seed=0, f0=10.0, width=None, variable=2, offset=None):
+    """Ricker point source at a seeded interior point (middle 60% of the box), on the vertical
+    velocity by default, delayed by 1.2 / f0; width defaults to 1% of the box."""
+    rng = np.random.default_rng(seed + 101)
+    off = np.zeros(3) if offset is None else np.asarray(offset, dtype=float)
+    size = np.asarray(size, dtype=float)
+    pos = off + size * rng.uniform(0.2, 0.8, 3)
+    w = float(width) if width is not None else float(0.01 * size.min())
+    return tuple(pos) + (float(f0), 1.2 / float(f0), 1.0, w, float(variable))

@@ -504,6 +504,7 @@ EXAREF_DEFINE_S(exaref3d_acoustic_o4_p2, AcousticPDE, 4, 2, false, true, false)
 EXAREF_DEFINE_S(exaref3d_elastic_o3_p3, ElasticPDE, 3, 3, false, true, false)
 EXAREF_DEFINE_S(exaref3d_acousticfixed_o4_p2, AcousticPDE, 4, 2, false, true, true)
 EXAREF_DEFINE_S(exaref3d_elasticfixed_o3_p3, ElasticPDE, 3, 3, false, true, true)
+EXAREF_DEFINE_S(exaref3d_elastic_o7_p3, ElasticPDE, 7, 3, false, true, false)
 EXAREF_DEFINE(exaref3d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref3d_euler_o5_p0, EulerPDE, 5, 0, false)

@@ -508,3 +508,28 @@ def test_patch_fixed_dt_many_steps_vs_oracle(exa):
             p.step_phase(ph, dt)
     assert rel(p.get_solution(), ref) < TOL
     p.close()
+
+
+@pytest.mark.parametrize("ncell,bc,steps,fixed", [((2, 3, 2), 3, 2, False), ((3, 2, 2), 0, 2, False),
+                                                  ((2, 2, 2), 1, 2, True)])
+def test_patch_elastic_order7_streamed_vs_oracle(exa, ncell, bc, steps, fixed):
+    """Order 7 (8^3 nodes x 12 data per cell): the streamed predictor (iterates in global scratch)."""
+    import exa_scenarios as sc
+    from pyoracle import PDE_ELASTIC
+    order, size = 7, [1.0, 1.2, 0.9]
+    luh0 = sc.layered_medium("elastic", ncell, size, order, seed=4)
+    src = sc.ricker_source(3, size, f0=4.0, variable=2, width=0.15)
+    src = src[:4] + (0.05,) + src[5:]
+    mp = order + 1 if fixed else 0
+    o = Oracle(3, order, PDE_ELASTIC, source=src, max_picard=mp)
+    ref = luh0.copy()
+    t_ref, _, pic = o.run(ref, ncell, size, steps, walls=bc, want_picard=True)
+    s = exa.Solver(exa.PDE_ELASTIC, 3, order, npar=3, max_picard=mp)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    p.set_point_source(src[:3], src[3], src[4], src[5], src[6], int(src[7]))
+    p.set_solution(luh0)
+    p.step(steps)
+    assert rel(p.get_solution(), ref) < TOL
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert p.status() == 0
+    p.close()

@@ -357,3 +357,26 @@ def test_linear_fixed_picard_count_vs_ref(name, order, npar, var):
     b = o.predictor(luh, dx, dt, centre=[src[0], src[1], src[2]], t=0.01)
     for key in ("lQhi", "lFhi", "lQhbnd", "lFhbnd"):
         assert relerr(b[key], a[key]) < 1e-13, key
+
+
+def test_elastic_order7_source_outflow_vs_ref():
+    """The order-7 elastic configuration (8^3 nodes, 9 variables + 3 parameters)."""
+    from exa_scenarios import layered_medium, ricker_source
+    from pyoracle import PDE_ELASTIC
+    size = [1.0, 1.0, 1.0]
+    src = ricker_source(3, size, f0=4.0, variable=3, width=0.15)
+    src = src[:4] + (0.05,) + src[5:]
+    try:
+        ref = RefKernels(3, 7, "elastic", 3, source=src)
+    except (FileNotFoundError, AttributeError, OSError) as e:
+        pytest.skip("reference kernels not built: %s" % e)
+    o = Oracle(3, 7, PDE_ELASTIC, source=src)
+    ncell = (2, 2, 3)
+    luh0 = layered_medium("elastic", ncell, size, 7, seed=1)
+    la, lb = luh0.copy(), luh0.copy()
+    ta, dta, pa = ref.run(la, ncell, size, 2, walls=3, want_picard=True)
+    tb, dtb, pb = o.run(lb, ncell, size, 2, walls=3, want_picard=True)
+    assert np.max(np.abs(dta - dtb) / dta) < 1e-13
+    assert np.array_equal(pa + 1, pb)
+    assert relerr(lb, la) < 1e-12
+    assert np.abs(lb - luh0).max() > 1e-4
