@@ -39,6 +39,9 @@ int cuda_fail(cudaError_t e, const char* what) {
   } while (0)
 
 // ADER-DG PNPM table by order (Toolkit/exahype/toolkit/solverController.py:17-23)
+// cell chunks of a host-buffer step (exa_patch_step_host)
+constexpr int kHostChunks = 16;
+
 double default_pnpm(int order) {
   static const double t[10] = {1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015};
   if (order < 10) return t[order];
@@ -130,7 +133,7 @@ struct OpsImpl final : Ops {
       if (e != cudaSuccess) return e;
       set = true;
     }
-    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
+    const unsigned blocks = (unsigned)((a.ncells - a.cell_begin + S::CPB - 1) / S::CPB);
     predictor_kernel<PDE, DIM, N, P, MM><<<blocks, S::TPB, smem, st>>>(a);
     return cudaGetLastError();
   }
@@ -180,7 +183,7 @@ struct OpsImpl final : Ops {
     sz_lFhi = (size_t)(DIM + 1) * S::nd * S::V;
   }
   cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed) override {
-    if (a.ncells <= 0) return cudaSuccess;
+    if (a.ncells <= a.cell_begin) return cudaSuccess;
     if constexpr (kStreamed) {
       using T = StreamShape<PDE, DIM, N, P>;
       if (mixed) return cudaErrorNotSupported;
@@ -190,7 +193,7 @@ struct OpsImpl final : Ops {
       if (dev < 0 || dev >= 64 || !scratch[dev]) return cudaErrorNotReady;  // reserve() first
       CellArgs b = a;
       b.scratch = scratch[dev];
-      const unsigned blocks = (unsigned)std::min<long long>(a.ncells, stream_grid[dev]);
+      const unsigned blocks = (unsigned)std::min<long long>(a.ncells - a.cell_begin, stream_grid[dev]);
       predictor_streamed_kernel<PDE, DIM, N, P><<<blocks, T::TPB, T::smem, st>>>(b);
       return cudaGetLastError();
     }
@@ -205,8 +208,8 @@ struct OpsImpl final : Ops {
     return cudaErrorNotSupported;
   }
   cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
-    if (a.ncells <= 0) return cudaSuccess;
-    const unsigned blocks = (unsigned)((a.ncells + S::CPB - 1) / S::CPB);
+    if (a.ncells <= a.cell_begin) return cudaSuccess;
+    const unsigned blocks = (unsigned)((a.ncells - a.cell_begin + S::CPB - 1) / S::CPB);
     if (surface && upd)
       update_kernel<PDE, DIM, N, P, true, true><<<blocks, S::TPB, 0, st>>>(a);
     else if (upd)
@@ -651,6 +654,10 @@ struct exa_patch {
   long long halo_lo_first = 0, halo_hi_first = 0;  // first real cell of the low / high boundary layer
   // discrete adjoint workspace (allocated on the first exa_patch_adjoint_step)
   double *adjQ = nullptr, *adjF = nullptr, *adj_iter = nullptr;
+  // host-buffer steps: copy stream and per-chunk events (created on the first exa_patch_step_host)
+  cudaStream_t copy_stream = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_out;
+  cudaEvent_t ev_begin = nullptr;
 };
 
 static void patch_free(exa_patch* p) {
@@ -661,6 +668,10 @@ static void patch_free(exa_patch* p) {
                   p->grid_geo, p->grid_first_d, p->src, p->btype, p->adjQ, p->adjF, p->adj_iter};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  for (cudaEvent_t e : p->ev_in) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->ev_out) cudaEventDestroy(e);
+  if (p->ev_begin) cudaEventDestroy(p->ev_begin);
+  if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
   if (p->stream) cudaStreamDestroy(p->stream);
 }
 
@@ -1360,6 +1371,91 @@ int exa_checkpoint_schedule(int steps, int snaps, exa_ck_action* out, int capaci
     out[i].a = acts[i].a;
     out[i].b = acts[i].b;
   }
+  return EXA_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// one step from and to host memory, copies overlapped with the cell kernels
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, double fixed_dt) {
+  if (!p || !luh_in || !luh_out) return fail(EXA_ERR_INVALID, "null argument");
+  if (p->halo_axis >= 0) return fail(EXA_ERR_INVALID, "a patch with EXA_BC_HALO steps through exa_patch_step_phase");
+  exa::Ops& o = *p->s->ops;
+  const int ng = (int)p->grids.size();
+  const bool cfl = !(fixed_dt > 0);
+  const long long nc = p->ncells;
+  const int K = (int)std::max<long long>(1, std::min<long long>(kHostChunks, nc));
+  if (!p->copy_stream) {
+    EXA_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    EXA_CUDA(cudaEventCreateWithFlags(&p->ev_begin, cudaEventDisableTiming));
+  }
+  while ((int)p->ev_in.size() < K) {
+    cudaEvent_t a, b;
+    EXA_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
+    EXA_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    p->ev_in.push_back(a);
+    p->ev_out.push_back(b);
+  }
+  auto first = [&](int j) { return (long long)((nc * j) / K); };
+  const size_t per = o.sz_luh;
+  // uploads wait for whatever the patch stream still has in flight
+  EXA_CUDA(cudaEventRecord(p->ev_begin, p->stream));
+  EXA_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_begin, 0));
+  for (int j = 0; j < K; j++) {
+    const long long c0 = first(j), c1 = first(j + 1);
+    EXA_CUDA(cudaMemcpyAsync(p->luh + c0 * per, luh_in + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
+                             cudaMemcpyHostToDevice, p->copy_stream));
+    EXA_CUDA(cudaEventRecord(p->ev_in[j], p->copy_stream));
+  }
+  if (!cfl && fixed_dt != p->fixed_dt) {
+    exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, fixed_dt);
+    EXA_CUDA(cudaGetLastError());
+    p->fixed_dt = fixed_dt;
+  }
+  if (cfl && p->fixed_dt > 0) {
+    // back from fixed steps: the CFL step of the uploaded state needs all of it first
+    EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[K - 1], 0));
+    if (int r = patch_initial_dt(p)) return r;
+    p->fixed_dt = -1.0;
+  }
+  // predictor + volume integral chunk by chunk as the chunks arrive
+  for (int j = 0; j < K; j++) {
+    EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[j], 0));
+    exa::CellArgs a = patch_args(p);
+    a.cell_begin = (int)first(j);
+    a.ncells = (int)first(j + 1);
+    EXA_CUDA(o.predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+  }
+  exa::FaceArgs f = patch_faces(p);
+  EXA_CUDA(o.riemann(f, p->stream));
+  if (p->nbfaces > 0) {
+    exa::FaceArgs b = f;
+    b.nfaces = p->nbfaces;
+    EXA_CUDA(o.boundary(b, p->stream));
+  }
+  // surface integral + update (+ CFL of the new state) chunk by chunk, each chunk downloaded as
+  // soon as it is final
+  for (int j = 0; j < K; j++) {
+    const long long c0 = first(j), c1 = first(j + 1);
+    exa::CellArgs u = patch_args(p);
+    u.cell_begin = (int)c0;
+    u.ncells = (int)c1;
+    if (cfl) u.grid_dt_next = p->grid_dt_next;
+    EXA_CUDA(o.update(u, true, true, p->stream));
+    EXA_CUDA(cudaEventRecord(p->ev_out[j], p->stream));
+    EXA_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_out[j], 0));
+    EXA_CUDA(cudaMemcpyAsync(luh_out + c0 * per, p->luh + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
+                             cudaMemcpyDeviceToHost, p->copy_stream));
+  }
+  exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt,
+                                                               cfl ? p->grid_dt_next : nullptr, p->steps);
+  EXA_CUDA(cudaGetLastError());
+  EXA_CUDA(cudaStreamSynchronize(p->copy_stream));
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
   return EXA_OK;
 }
 

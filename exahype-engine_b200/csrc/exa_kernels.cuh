@@ -120,7 +120,8 @@ struct Shape {
 
 // Arguments shared by the cell kernels (device pointers).
 struct CellArgs {
-  int ncells;
+  int ncells;               // end of the cell range the launch covers (exclusive)
+  int cell_begin;           // first cell of the range (launches cover [cell_begin, ncells))
   const double* luh;
   double* luh_out;          // update kernel: new solution (may alias luh)
   double* lduh;
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
   const int tid = threadIdx.x;
   const bool inr = tid < CPB * nd;
   const int lc = inr ? tid / nd : 0, p = inr ? tid % nd : 0;
-  const long cell = (long)blockIdx.x * CPB + lc;
+  const long cell = (long)a.cell_begin + (long)blockIdx.x * CPB + lc;
   const bool live = inr && cell < a.ncells;
   if (tid < n) {
     s_w[tid] = G::weights(tid);
@@ -431,8 +432,8 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
   if (tid < CPB) s_min[tid] = __longlong_as_double(0x7ff0000000000000ll);
   if (SURFACE) {
     for (int j = tid; j < CPB * S::sizeFhb; j += S::TPB) {
-      const long gc = (long)blockIdx.x * CPB + j / S::sizeFhb;
-      sFb[j] = gc < a.ncells ? a.lFhbnd[(size_t)blockIdx.x * CPB * S::sizeFhb + j] : 0.0;
+      const long gc = (long)a.cell_begin + (long)blockIdx.x * CPB + j / S::sizeFhb;
+      sFb[j] = gc < a.ncells ? a.lFhbnd[((size_t)a.cell_begin + (size_t)blockIdx.x * CPB) * S::sizeFhb + j] : 0.0;
     }
   }
   __syncthreads();

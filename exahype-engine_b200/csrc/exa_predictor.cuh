@@ -58,7 +58,7 @@ predictor_kernel(CellArgs a) {
   const bool inr = tid < CPB * nd;   // tail threads of the last warp only help in line loops
   const int lc = inr ? tid / nd : 0;
   const int p = inr ? tid % nd : 0;
-  const long cell = (long)blockIdx.x * CPB + lc;
+  const long cell = (long)a.cell_begin + (long)blockIdx.x * CPB + lc;
   const bool live = inr && cell < a.ncells;
 
   if (tid < n) s_w[tid] = G::weights(tid);
@@ -67,7 +67,7 @@ predictor_kernel(CellArgs a) {
     s_dudx[tid] = G::dudx(tid / n, tid % n);
   }
   if (tid < CPB) {
-    const long c = (long)blockIdx.x * CPB + tid;
+    const long c = (long)a.cell_begin + (long)blockIdx.x * CPB + tid;
     const int g = (c < a.ncells && a.cell_grid) ? a.cell_grid[c] : 0;
     s_dt[tid] = a.grid_dt ? a.grid_dt[g] : a.u_dt;
 #pragma unroll
@@ -565,7 +565,7 @@ predictor_kernel(CellArgs a) {
   // ---------------- extrapolation to the faces (:517-687) ----------------
   for (int j = tid; j < CPB * (S::sizeQhb + S::sizeFhb); j += S::TPB) {
     const int c = j / (S::sizeQhb + S::sizeFhb);
-    const long gc = (long)blockIdx.x * CPB + c;
+    const long gc = (long)a.cell_begin + (long)blockIdx.x * CPB + c;
     if (gc >= a.ncells) continue;
     int r = j % (S::sizeQhb + S::sizeFhb);
     const bool isQ = r < S::sizeQhb;

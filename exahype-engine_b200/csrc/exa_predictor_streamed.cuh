@@ -55,7 +55,7 @@ predictor_streamed_kernel(CellArgs a) {
   const size_t slab = (size_t)n * nd * V;
   double* slot = a.scratch + (size_t)blockIdx.x * T::slot_doubles;
 
-  for (long cell = blockIdx.x; cell < a.ncells; cell += gridDim.x) {
+  for (long cell = (long)a.cell_begin + blockIdx.x; cell < a.ncells; cell += gridDim.x) {
     const int g = a.cell_grid ? a.cell_grid[cell] : 0;
     const double dt = a.grid_dt ? a.grid_dt[g] : a.u_dt;
     double invdx[3];

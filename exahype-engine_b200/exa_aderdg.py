@@ -123,6 +123,7 @@ def load_library(path=None):
         "exa_build_face_lists": [i, i, ctypes.POINTER(GridDesc), ctypes.POINTER(FaceLists)],
         "exa_patch_set_point_source": [vp, ctypes.POINTER(PointSource)],
         "exa_patch_set_time": [vp, d],
+        "exa_patch_step_host": [vp, vp, vp, d],
         "exa_patch_adjoint_step": [vp, vp, d],
         "exa_checkpoint_schedule": [i, i, ctypes.POINTER(CkAction), i, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong)],
@@ -155,6 +156,11 @@ def _ptr(t):
     if not t.is_cuda or not t.is_contiguous():
         raise ExaError("expected a contiguous CUDA tensor")
     return ctypes.c_void_p(t.data_ptr())
+
+
+def torch_float64():
+    import torch
+    return torch.float64
 
 
 def _np_ptr(a):
@@ -370,6 +376,20 @@ class Patch:
 
     def dt_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_copy")
+
+    def step_host(self, luh_in, luh_out, fixed_dt=0.0):
+        """One step from host memory to host memory (numpy arrays or CPU torch tensors, pinned for
+        overlap), copies pipelined with the cell kernels."""
+        def hptr(x):
+            if isinstance(x, np.ndarray):
+                if x.dtype != np.float64 or not x.flags["C_CONTIGUOUS"]:
+                    raise ExaError("expected a contiguous float64 array")
+                return _np_ptr(x)
+            if x.is_cuda or not x.is_contiguous() or x.dtype != torch_float64():
+                raise ExaError("expected a contiguous float64 CPU tensor")
+            return ctypes.c_void_p(x.data_ptr())
+        _check(self.lib.exa_patch_step_host(self.h, hptr(luh_in), hptr(luh_out), float(fixed_dt)),
+               "exa_patch_step_host")
 
     def set_time(self, t):
         _check(self.lib.exa_patch_set_time(self.h, float(t)), "exa_patch_set_time")

@@ -282,6 +282,16 @@ typedef struct {
 } exa_face_lists;
 int exa_build_face_lists(int dim, int ngrids, const exa_grid_desc* grids, exa_face_lists* out);
 
+/* ---- one step from and to host memory -----------------------------------------------------
+ * Uploads luh_in (host, reference layout, all cells), runs one step, downloads the new state into
+ * luh_out (may equal luh_in). The copies run on a second stream in cell chunks, overlapped with
+ * the predictor (chunk j starts as soon as it has arrived) and with the update (chunk j is
+ * downloaded as soon as it is final); pinned host buffers make the overlap real. The time step is
+ * fixed_dt if > 0, else the patch's CFL step, which is the CFL step of luh_in when luh_in is the
+ * state the patch last produced or was given (exa_patch_set_solution, a previous step). Returns
+ * after luh_out is written. Patches with EXA_BC_HALO are refused. */
+int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, double fixed_dt);
+
 /* ---- discrete adjoint (acoustic and elastic systems) -----------------------------------------
  * No reference counterpart: the reference has no adjoint. The forward step differentiated is
  * exa_patch_step(p, 1, dt) with a fixed dt and a solver created with max_picard > 0 (the
