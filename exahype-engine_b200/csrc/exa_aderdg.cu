@@ -655,8 +655,8 @@ struct exa_patch {
   // discrete adjoint workspace (allocated on the first exa_patch_adjoint_step)
   double *adjQ = nullptr, *adjF = nullptr, *adj_iter = nullptr;
   // host-buffer steps: copy stream and per-chunk events (created on the first exa_patch_step_host)
-  cudaStream_t copy_stream = nullptr;
-  std::vector<cudaEvent_t> ev_in, ev_out;
+  cudaStream_t copy_stream = nullptr, d2h_stream = nullptr;
+  std::vector<cudaEvent_t> ev_in, ev_upd, ev_out;
   cudaEvent_t ev_begin = nullptr;
 };
 
@@ -670,8 +670,10 @@ static void patch_free(exa_patch* p) {
     if (q) cudaFree(q);
   for (cudaEvent_t e : p->ev_in) cudaEventDestroy(e);
   for (cudaEvent_t e : p->ev_out) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->ev_upd) cudaEventDestroy(e);
   if (p->ev_begin) cudaEventDestroy(p->ev_begin);
   if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
+  if (p->d2h_stream) cudaStreamDestroy(p->d2h_stream);
   if (p->stream) cudaStreamDestroy(p->stream);
 }
 
@@ -1381,9 +1383,10 @@ int exa_checkpoint_schedule(int steps, int snaps, exa_ck_action* out, int capaci
 // ------------------------------------------------------------------------------------------
 extern "C" {
 
-int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, double fixed_dt) {
-  if (!p || !luh_in || !luh_out) return fail(EXA_ERR_INVALID, "null argument");
+int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int nsteps, double fixed_dt) {
+  if (!p || !luh_in || !luh_out || nsteps < 0) return fail(EXA_ERR_INVALID, "bad argument");
   if (p->halo_axis >= 0) return fail(EXA_ERR_INVALID, "a patch with EXA_BC_HALO steps through exa_patch_step_phase");
+  if (nsteps == 0) return EXA_OK;
   exa::Ops& o = *p->s->ops;
   const int ng = (int)p->grids.size();
   const bool cfl = !(fixed_dt > 0);
@@ -1391,72 +1394,87 @@ int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, dou
   const int K = (int)std::max<long long>(1, std::min<long long>(kHostChunks, nc));
   if (!p->copy_stream) {
     EXA_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    EXA_CUDA(cudaStreamCreateWithFlags(&p->d2h_stream, cudaStreamNonBlocking));
     EXA_CUDA(cudaEventCreateWithFlags(&p->ev_begin, cudaEventDisableTiming));
   }
   while ((int)p->ev_in.size() < K) {
-    cudaEvent_t a, b;
+    cudaEvent_t a, b, c;
     EXA_CUDA(cudaEventCreateWithFlags(&a, cudaEventDisableTiming));
     EXA_CUDA(cudaEventCreateWithFlags(&b, cudaEventDisableTiming));
+    EXA_CUDA(cudaEventCreateWithFlags(&c, cudaEventDisableTiming));
     p->ev_in.push_back(a);
-    p->ev_out.push_back(b);
+    p->ev_upd.push_back(b);
+    p->ev_out.push_back(c);
   }
   auto first = [&](int j) { return (long long)((nc * j) / K); };
   const size_t per = o.sz_luh;
-  // uploads wait for whatever the patch stream still has in flight
+  // the copies wait for whatever the patch stream still has in flight
   EXA_CUDA(cudaEventRecord(p->ev_begin, p->stream));
   EXA_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_begin, 0));
-  for (int j = 0; j < K; j++) {
-    const long long c0 = first(j), c1 = first(j + 1);
-    EXA_CUDA(cudaMemcpyAsync(p->luh + c0 * per, luh_in + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
-                             cudaMemcpyHostToDevice, p->copy_stream));
-    EXA_CUDA(cudaEventRecord(p->ev_in[j], p->copy_stream));
-  }
-  if (!cfl && fixed_dt != p->fixed_dt) {
-    exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, fixed_dt);
+  EXA_CUDA(cudaStreamWaitEvent(p->d2h_stream, p->ev_begin, 0));
+  for (int k = 0; k < nsteps; k++) {
+    const double* src = k == 0 ? luh_in : luh_out;
+    // uploads: chunk j of step k > 0 is the host copy step k-1 wrote back
+    for (int j = 0; j < K; j++) {
+      const long long c0 = first(j), c1 = first(j + 1);
+      if (k > 0) EXA_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_out[j], 0));
+      EXA_CUDA(cudaMemcpyAsync(p->luh + c0 * per, src + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
+                               cudaMemcpyHostToDevice, p->copy_stream));
+      EXA_CUDA(cudaEventRecord(p->ev_in[j], p->copy_stream));
+    }
+    if (k == 0 && !cfl && fixed_dt != p->fixed_dt) {
+      exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, fixed_dt);
+      EXA_CUDA(cudaGetLastError());
+      p->fixed_dt = fixed_dt;
+    }
+    if (k == 0 && cfl && p->fixed_dt > 0) {
+      // back from fixed steps: the CFL step of the uploaded state needs all of it first
+      EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[K - 1], 0));
+      if (int r = patch_initial_dt(p)) return r;
+      p->fixed_dt = -1.0;
+    }
+    // predictor + volume integral chunk by chunk as the chunks arrive
+    for (int j = 0; j < K; j++) {
+      EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[j], 0));
+      exa::CellArgs a = patch_args(p);
+      a.cell_begin = (int)first(j);
+      a.ncells = (int)first(j + 1);
+      EXA_CUDA(o.predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+    }
+    exa::FaceArgs f = patch_faces(p);
+    EXA_CUDA(o.riemann(f, p->stream));
+    if (p->nbfaces > 0) {
+      exa::FaceArgs b = f;
+      b.nfaces = p->nbfaces;
+      EXA_CUDA(o.boundary(b, p->stream));
+    }
+    // surface integral + update (+ CFL of the new state) chunk by chunk; each chunk goes back to
+    // the host as soon as it is final, on its own stream (the link carries both directions)
+    for (int j = 0; j < K; j++) {
+      const long long c0 = first(j), c1 = first(j + 1);
+      exa::CellArgs u = patch_args(p);
+      u.cell_begin = (int)c0;
+      u.ncells = (int)c1;
+      if (cfl) u.grid_dt_next = p->grid_dt_next;
+      EXA_CUDA(o.update(u, true, true, p->stream));
+      EXA_CUDA(cudaEventRecord(p->ev_upd[j], p->stream));
+      EXA_CUDA(cudaStreamWaitEvent(p->d2h_stream, p->ev_upd[j], 0));
+      EXA_CUDA(cudaMemcpyAsync(luh_out + c0 * per, p->luh + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
+                               cudaMemcpyDeviceToHost, p->d2h_stream));
+      EXA_CUDA(cudaEventRecord(p->ev_out[j], p->d2h_stream));
+    }
+    exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt,
+                                                                 cfl ? p->grid_dt_next : nullptr, p->steps);
     EXA_CUDA(cudaGetLastError());
-    p->fixed_dt = fixed_dt;
   }
-  if (cfl && p->fixed_dt > 0) {
-    // back from fixed steps: the CFL step of the uploaded state needs all of it first
-    EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[K - 1], 0));
-    if (int r = patch_initial_dt(p)) return r;
-    p->fixed_dt = -1.0;
-  }
-  // predictor + volume integral chunk by chunk as the chunks arrive
-  for (int j = 0; j < K; j++) {
-    EXA_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in[j], 0));
-    exa::CellArgs a = patch_args(p);
-    a.cell_begin = (int)first(j);
-    a.ncells = (int)first(j + 1);
-    EXA_CUDA(o.predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
-  }
-  exa::FaceArgs f = patch_faces(p);
-  EXA_CUDA(o.riemann(f, p->stream));
-  if (p->nbfaces > 0) {
-    exa::FaceArgs b = f;
-    b.nfaces = p->nbfaces;
-    EXA_CUDA(o.boundary(b, p->stream));
-  }
-  // surface integral + update (+ CFL of the new state) chunk by chunk, each chunk downloaded as
-  // soon as it is final
-  for (int j = 0; j < K; j++) {
-    const long long c0 = first(j), c1 = first(j + 1);
-    exa::CellArgs u = patch_args(p);
-    u.cell_begin = (int)c0;
-    u.ncells = (int)c1;
-    if (cfl) u.grid_dt_next = p->grid_dt_next;
-    EXA_CUDA(o.update(u, true, true, p->stream));
-    EXA_CUDA(cudaEventRecord(p->ev_out[j], p->stream));
-    EXA_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_out[j], 0));
-    EXA_CUDA(cudaMemcpyAsync(luh_out + c0 * per, p->luh + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),
-                             cudaMemcpyDeviceToHost, p->copy_stream));
-  }
-  exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt,
-                                                               cfl ? p->grid_dt_next : nullptr, p->steps);
-  EXA_CUDA(cudaGetLastError());
+  EXA_CUDA(cudaStreamSynchronize(p->d2h_stream));
   EXA_CUDA(cudaStreamSynchronize(p->copy_stream));
   EXA_CUDA(cudaStreamSynchronize(p->stream));
   return EXA_OK;
+}
+
+int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, double fixed_dt) {
+  return exa_patch_run_host(p, luh_in, luh_out, 1, fixed_dt);
 }
 
 }  // extern "C"

@@ -124,6 +124,7 @@ def load_library(path=None):
         "exa_patch_set_point_source": [vp, ctypes.POINTER(PointSource)],
         "exa_patch_set_time": [vp, d],
         "exa_patch_step_host": [vp, vp, vp, d],
+        "exa_patch_run_host": [vp, vp, vp, i, d],
         "exa_patch_adjoint_step": [vp, vp, d],
         "exa_checkpoint_schedule": [i, i, ctypes.POINTER(CkAction), i, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong)],
@@ -377,9 +378,9 @@ class Patch:
     def dt_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_copy")
 
-    def step_host(self, luh_in, luh_out, fixed_dt=0.0):
-        """One step from host memory to host memory (numpy arrays or CPU torch tensors, pinned for
-        overlap), copies pipelined with the cell kernels."""
+    def step_host(self, luh_in, luh_out, fixed_dt=0.0, nsteps=1):
+        """nsteps steps of a host-resident state (numpy arrays or CPU torch tensors, pinned for
+        overlap): every step uploads, steps and downloads, copies pipelined with the kernels."""
         def hptr(x):
             if isinstance(x, np.ndarray):
                 if x.dtype != np.float64 or not x.flags["C_CONTIGUOUS"]:
@@ -388,8 +389,8 @@ class Patch:
             if x.is_cuda or not x.is_contiguous() or x.dtype != torch_float64():
                 raise ExaError("expected a contiguous float64 CPU tensor")
             return ctypes.c_void_p(x.data_ptr())
-        _check(self.lib.exa_patch_step_host(self.h, hptr(luh_in), hptr(luh_out), float(fixed_dt)),
-               "exa_patch_step_host")
+        _check(self.lib.exa_patch_run_host(self.h, hptr(luh_in), hptr(luh_out), int(nsteps), float(fixed_dt)),
+               "exa_patch_run_host")
 
     def set_time(self, t):
         _check(self.lib.exa_patch_set_time(self.h, float(t)), "exa_patch_set_time")

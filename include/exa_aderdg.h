@@ -291,6 +291,11 @@ int exa_build_face_lists(int dim, int ngrids, const exa_grid_desc* grids, exa_fa
  * state the patch last produced or was given (exa_patch_set_solution, a previous step). Returns
  * after luh_out is written. Patches with EXA_BC_HALO are refused. */
 int exa_patch_step_host(exa_patch* p, const double* luh_in, double* luh_out, double fixed_dt);
+/* nsteps such steps of a host-resident state: step 0 reads luh_in, every step writes its result to
+ * luh_out, steps >= 1 read luh_out. The upload of a chunk for step k waits only for that chunk's
+ * download of step k-1, so downloads and uploads run at the same time on the two copy directions
+ * and both overlap the kernels. */
+int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int nsteps, double fixed_dt);
 
 /* ---- discrete adjoint (acoustic and elastic systems) -----------------------------------------
  * No reference counterpart: the reference has no adjoint. The forward step differentiated is

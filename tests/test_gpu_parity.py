@@ -570,5 +570,15 @@ def test_step_host_matches_device_steps(exa, torch, case):
     assert rel(buf.numpy(), ref) < 1e-14
     t1, t2 = dev.time()[0], host.time()[0]
     assert np.allclose(t1, t2, rtol=1e-15, atol=0)
+    # all steps in one call: uploads of step k overlap the downloads of step k-1
+    multi = exa.Patch(s, grids)
+    src = torch.from_numpy(luh0.copy()).pin_memory()
+    out = torch.zeros_like(src).pin_memory()
+    multi.set_solution(src.numpy())
+    multi.step_host(src, out, fixed, nsteps=steps)
+    assert rel(out.numpy(), ref) < 1e-14
+    assert np.array_equal(src.numpy(), luh0)   # the input buffer is only read
+    assert np.allclose(multi.time()[0], t1, rtol=1e-15, atol=0)
     dev.close()
     host.close()
+    multi.close()
