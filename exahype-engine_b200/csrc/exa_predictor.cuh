@@ -50,6 +50,7 @@ predictor_kernel(CellArgs a) {
   double* sQ = smem;              // [CPB][n][nd][D]: old iterate (NCP), rhs slices, new iterate
   double* sF = smem + S::smemQ;   // [CPB][DIM][V][BS]: fluxes, contracted in place
   __shared__ double s_w[n], s_Kxi[n * n], s_dudx[n * n];
+  __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_lw[CPB * DIM * NL];  // w_a w_b dt / dx_d of every line
   __shared__ double s_dt[CPB], s_invdx[CPB][3], s_res[CPB];
   __shared__ int s_active[CPB];
@@ -61,7 +62,17 @@ predictor_kernel(CellArgs a) {
   const long cell = (long)a.cell_begin + (long)blockIdx.x * CPB + lc;
   const bool live = inr && cell < a.ncells;
 
-  if (tid < n) s_w[tid] = G::weights(tid);
+  if (tid < n) {
+    s_w[tid] = G::weights(tid);
+    double A = 0.0, B = 0.0;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+      A = fma(G::iK1(tid, i), G::F0(i), A);
+      B = fma(G::iK1(tid, i), G::weights(i), B);
+    }
+    s_A[tid] = A;
+    s_B[tid] = B;
+  }
   if (tid < n * n) {
     s_Kxi[tid] = G::Kxi(tid / n, tid % n);
     s_dudx[tid] = G::dudx(tid / n, tid % n);
@@ -255,6 +266,7 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
       for (int m = 0; m < V; m++) sh[m] = 0.0;
     }
+    double res = 0.0;
     if (s == 0) {
       // the iterate is luh at every time node: one flux, one set of contractions
       double F[DIM * V];
@@ -294,17 +306,30 @@ predictor_kernel(CellArgs a) {
           o[m] = acc;
           if (MIXED) o_s[m] = acc;
         }
+        // The sweep-0 rhs of time node i is (w_p F0[i] luh - w_i o + w_i w_p dt (S0 + src_i)) / w_p,
+        // so the iK1 time solve has the closed form
+        //   q1[t] = luh A[t] - o B[t] / w_p + dt S0 B[t] + dt sum_i iK1[t][i] w_i src_i
+        // with A[t] = sum_i iK1[t][i] F0[i] and B[t] = sum_i iK1[t][i] w_i.
+        double cs[n];
 #pragma unroll
-        for (int i = 0; i < n; i++) {
-          const double wi = G::weights(i);
-          const double f0 = G::F0(i);
-          const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
+        for (int t = 0; t < n; t++) cs[t] = 0.0;
+        if (PDE::kSource && srcOn) {
+          for (int i = 0; i < n; i++) {
+            const double wsi = G::weights(i) * dt * src_at(i);
 #pragma unroll
-          for (int m = 0; m < V; m++) {
-            double rhs = w_sp * f0 * u[m] - wi * o[m];
-            if (NCP) rhs += wi * w_sp * dt * S0[m];
-            if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
-            q_s[(i * nd + p) * D + m] = iweight * rhs;
+            for (int t = 0; t < n; t++) cs[t] = fma(G::iK1(t, i), wsi, cs[t]);
+          }
+        }
+#pragma unroll
+        for (int m = 0; m < V; m++) {
+#pragma unroll
+          for (int t = 0; t < n; t++) {
+            double q1 = u[m] * s_A[t] - iweight * o[m] * s_B[t];
+            if (NCP) q1 += dt * S0[m] * s_B[t];
+            if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
+            const double dl = q1 - u[m];
+            res = fma(dl, dl, res);
+            q_s[(t * nd + p) * D + m] = q1;
           }
         }
       }
@@ -392,8 +417,8 @@ predictor_kernel(CellArgs a) {
     }
     __syncthreads();
     // iK1 time solve (:370-405): new iterate, residual against the old one, staged in the slices
-    double res = 0.0;
-    if (work) {
+    // (sweep 0 solved in closed form above)
+    if (work && s > 0) {
 #pragma unroll
       for (int m = 0; m < V; m++) {
         double r[n];
@@ -480,34 +505,26 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
       for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
     } else {
-      // lFhi = sum_t w_t F(old iterate at t), accumulated in this node's own flux slots
+      // lFhi = sum_t w_t F(old iterate at t), accumulated in registers (the old iterate's time
+      // nodes die one by one as the loop consumes them) and stored once
+      double fa[DIM * V];
 #pragma unroll
-      for (int d = 0; d < DIM; d++)
+      for (int k = 0; k < DIM * V; k++) fa[k] = 0.0;
 #pragma unroll
-        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = 0.0;
-#pragma unroll 1
       for (int i = 0; i < n; i++) {
         double q[D], F[DIM * V];
 #pragma unroll
-        for (int m = 0; m < D; m++) q[m] = m < V ? qo[0][m] : u[m];
-#pragma unroll
-        for (int m = 0; m < V; m++) {
-          const double t0 = qo[0][m];
-#pragma unroll
-          for (int t = 0; t + 1 < n; t++) qo[t][m] = qo[t + 1][m];
-          qo[n - 1][m] = t0;
-        }
+        for (int m = 0; m < D; m++) q[m] = m < V ? qo[i][m] : u[m];
         PDE::template flux<DIM>(q, F);
         const double wi = G::weights(i);
 #pragma unroll
-        for (int d = 0; d < DIM; d++)
-#pragma unroll
-          for (int m = 0; m < V; m++) {
-            double* slot = &f_s[(d * V + m) * BS + off[d]];
-            *slot = fma(F[d * V + m], wi, *slot);
-          }
+        for (int k = 0; k < DIM * V; k++) fa[k] = fma(F[k], wi, fa[k]);
         if (live && a.ex_lFi) export_flux(i, F, nullptr);
       }
+#pragma unroll
+      for (int d = 0; d < DIM; d++)
+#pragma unroll
+        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[d * V + m];
     }
   }
   if (live && a.ex_lQhi) {
