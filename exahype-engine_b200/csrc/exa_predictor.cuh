@@ -580,34 +580,53 @@ predictor_kernel(CellArgs a) {
   }
 
   // ---------------- extrapolation to the faces (:517-687) ----------------
-  for (int j = tid; j < CPB * (S::sizeQhb + S::sizeFhb); j += S::TPB) {
-    const int c = j / (S::sizeQhb + S::sizeFhb);
+  // one thread per (cell, lQhbnd or lFhbnd, direction, line): both faces of the line from one
+  // read of it; the D (or V) values of a face node are contiguous in HBM
+  constexpr int LQ = DIM * NL;
+  for (int j = tid; j < CPB * 2 * LQ; j += S::TPB) {
+    const int c = j / (2 * LQ);
     const long gc = (long)a.cell_begin + (long)blockIdx.x * CPB + c;
     if (gc >= a.ncells) continue;
-    int r = j % (S::sizeQhb + S::sizeFhb);
-    const bool isQ = r < S::sizeQhb;
-    if (!isQ) r -= S::sizeQhb;
-    const int W = isQ ? D : V;
-    const int m = r % W;
-    const int fn = (r / W) % nf;
-    const int face = r / (W * nf);
-    const int d = face >> 1, o = face & 1;
+    const int r = j % (2 * LQ);
+    const bool isQ = r < LQ;
+    const int rl = isQ ? r : r - LQ;
+    const int d = rl / NL, L = rl % NL;
     const int st = d == 0 ? 1 : (d == 1 ? n : n * n);
-    double acc = 0.0;
     if (isQ) {
-      // 2D x faces extrapolate only the evolved variables (2d/spaceTimePredictorNonlinear.cpph:436-445)
-      if (!(DIM == 2 && d == 0 && m >= V)) {
-        const double* src = smem + (size_t)c * n * nd * D;
-        const int base = line_base<DIM, n>(d, fn);
+      const double* src = smem + (size_t)c * n * nd * D + (size_t)line_base<DIM, n>(d, L) * D;
+      double* o0 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d) * nf + L) * D;
+      double* o1 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d + 1) * nf + L) * D;
 #pragma unroll
-        for (int l = 0; l < n; l++) acc = fma(src[(base + l * st) * D + m], o ? G::F1(l) : G::F0(l), acc);
+      for (int m = 0; m < D; m++) {
+        double a0 = 0.0, a1 = 0.0;
+        // 2D x faces extrapolate only the evolved variables (2d/spaceTimePredictorNonlinear.cpph:436-445)
+        if (!(DIM == 2 && d == 0 && m >= V)) {
+#pragma unroll
+          for (int l = 0; l < n; l++) {
+            const double x = src[(size_t)l * st * D + m];
+            a0 = fma(x, G::F0(l), a0);
+            a1 = fma(x, G::F1(l), a1);
+          }
+        }
+        o0[m] = a0;
+        o1[m] = a1;
       }
-      a.lQhbnd[(size_t)gc * S::sizeQhb + r] = acc;
     } else {
-      const double* src = sF + ((size_t)(c * DIM + d) * V + m) * BS + pline_base<DIM, n>(d, fn);
+      const double* src = sF + (size_t)(c * DIM + d) * V * BS + pline_base<DIM, n>(d, L);
+      double* o0 = a.lFhbnd + (size_t)gc * S::sizeFhb + (size_t)((2 * d) * nf + L) * V;
+      double* o1 = a.lFhbnd + (size_t)gc * S::sizeFhb + (size_t)((2 * d + 1) * nf + L) * V;
 #pragma unroll
-      for (int l = 0; l < n; l++) acc = fma(src[l * st], o ? G::F1(l) : G::F0(l), acc);
-      a.lFhbnd[(size_t)gc * S::sizeFhb + r] = acc;
+      for (int m = 0; m < V; m++) {
+        double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+          const double x = src[(size_t)m * BS + l * st];
+          a0 = fma(x, G::F0(l), a0);
+          a1 = fma(x, G::F1(l), a1);
+        }
+        o0[m] = a0;
+        o1[m] = a1;
+      }
     }
   }
 }
