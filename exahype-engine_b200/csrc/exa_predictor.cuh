@@ -156,7 +156,9 @@ predictor_kernel(CellArgs a) {
   }
   // mixed precision: the sweep-0 contraction of F(luh), per node and variable (summed over d)
   double* o_s = sQ + S::smemQ + S::smemF + S::smemU + ((size_t)lc * nd + p) * V;
-  double qo[n][V];  // old iterate; set to luh at the end of sweep 0, before the time solve
+  // new iterate of the sweep, accumulated in registers time node by time node (the iK1 time
+  // solve distributed over phase 3); the old iterate is staged in the slices q_s [t][node][D]
+  double qn[n][V];
   double* q_s = sQ + (size_t)lc * n * nd * D;
   double* f_s = sF + (size_t)lc * DIM * V * BS;
   if (NCP && inr) {  // neighbours' old iterate is read by the gradients
@@ -255,6 +257,7 @@ predictor_kernel(CellArgs a) {
   const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
   int sweeps = 0;
   bool done = false;
+  bool last_old_is_luh = true;  // the last sweep started from lQi = luh (sweep 0)
   for (int s = 0; s < maxIter; s++) {
     if (s_active[lc] == 0) done = true;
     const bool work = live && !done;
@@ -329,24 +332,23 @@ predictor_kernel(CellArgs a) {
             if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
             const double dl = q1 - u[m];
             res = fma(dl, dl, res);
-            q_s[(t * nd + p) * D + m] = q1;
+            qn[t][m] = q1;
           }
         }
       }
-#pragma unroll
-      for (int t = 0; t < n; t++)
-#pragma unroll
-        for (int m = 0; m < V; m++) qo[t][m] = u[m];
     } else {
-      // The time loop is not unrolled: qo is rotated by one time node per iteration so that the
-      // current node always sits in qo[0] (compile-time register index), and after n
-      // iterations the rotation is back at its start.
+      if (work) {
+#pragma unroll
+        for (int t = 0; t < n; t++)
+#pragma unroll
+          for (int m = 0; m < V; m++) qn[t][m] = 0.0;
+      }
 #pragma unroll
       for (int i = 0; i < n; i++) {
         // phase 1: flux (and NCP source) of the old iterate at time node i (:196-227, :323-367)
         double q[D];
 #pragma unroll
-        for (int m = 0; m < D; m++) q[m] = m < V ? qo[i][m] : u[m];
+        for (int m = 0; m < D; m++) q[m] = m < V ? q_s[(i * nd + p) * D + m] : u[m];
         double F[DIM * V];
         double Si[V];
         PDE::template flux<DIM>(q, F);
@@ -408,33 +410,27 @@ predictor_kernel(CellArgs a) {
               for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * BS + off[d]];
             }
             if (NCP) rhs += wi * w_sp * dt * Si[m];
-            q_s[(i * nd + p) * D + m] = iweight * rhs;
+            // iK1 time solve (:370-405), one time node of the rhs at a time
+            const double r = iweight * rhs;
+#pragma unroll
+            for (int t = 0; t < n; t++) qn[t][m] = fma(r, G::iK1(t, i), qn[t][m]);
           }
         }
-        // no barrier: the next phase 1 rewrites only this thread's own flux slots, and the NCP
-        // gradients read slice i+1, which still holds the old iterate
+        // no barrier: the next phase 1 rewrites only this thread's own flux slots, and the slices
+        // hold the old iterate for the whole sweep
+      }
+      // residual against the old iterate
+      if (work) {
+#pragma unroll
+        for (int t = 0; t < n; t++)
+#pragma unroll
+          for (int m = 0; m < V; m++) {
+            const double dl = qn[t][m] - q_s[(t * nd + p) * D + m];
+            res = fma(dl, dl, res);
+          }
       }
     }
     __syncthreads();
-    // iK1 time solve (:370-405): new iterate, residual against the old one, staged in the slices
-    // (sweep 0 solved in closed form above)
-    if (work && s > 0) {
-#pragma unroll
-      for (int m = 0; m < V; m++) {
-        double r[n];
-#pragma unroll
-        for (int i = 0; i < n; i++) r[i] = q_s[(i * nd + p) * D + m];
-#pragma unroll
-        for (int t = 0; t < n; t++) {
-          double qn = 0.0;
-#pragma unroll
-          for (int i = 0; i < n; i++) qn = fma(r[i], G::iK1(t, i), qn);
-          const double dl = qn - qo[t][m];
-          res = fma(dl, dl, res);
-          q_s[(t * nd + p) * D + m] = qn;
-        }
-      }
-    }
     // per-cell residual: segmented warp tree, one shared atomic per segment head
     if (tid < CPB) s_res[tid] = 0.0;
     __syncthreads();
@@ -461,7 +457,9 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
         for (int t = 0; t < n; t++)
 #pragma unroll
-          for (int m = 0; m < V; m++) qo[t][m] = q_s[(t * nd + p) * D + m];
+          for (int m = 0; m < V; m++) q_s[(t * nd + p) * D + m] = qn[t][m];
+      } else {
+        last_old_is_luh = s == 0;
       }
     }
     __syncthreads();
@@ -476,19 +474,42 @@ predictor_kernel(CellArgs a) {
   if (live && p == 0 && a.max_picard <= 0 && !done && a.status) atomicOr(a.status, ST_PICARD_CAP);
 
   // ---------------- time averaging (:441-515) ----------------
-  // lQhi from the new iterate (staged in the slices); lFhi from the flux of the old iterate
+  // lQhi from the new iterate (registers); lFhi from the flux of the old iterate (the slices, or
+  // luh when the last sweep was sweep 0)
   double qh[D];
 #pragma unroll
   for (int m = 0; m < D; m++) {
     double acc = 0.0;
 #pragma unroll
-    for (int t = 0; t < n; t++) acc = fma(m < V ? q_s[(t * nd + p) * D + m] : u[m], G::weights(t), acc);
+    for (int t = 0; t < n; t++) acc = fma(m < V ? qn[t][m] : u[m], G::weights(t), acc);
     qh[m] = acc;
   }
   if (live && a.ex_lQi) {
     double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
+#pragma unroll
     for (int t = 0; t < n; t++)
-      for (int m = 0; m < D; m++) e[t * D + m] = m < V ? q_s[(t * nd + p) * D + m] : u[m];
+#pragma unroll
+      for (int m = 0; m < D; m++) e[t * D + m] = m < V ? qn[t][m] : u[m];
+  }
+  // the old iterate of the last sweep, before its slot 0 takes lQhi (each thread reads and
+  // writes only its own node, so no barrier is needed in between)
+  double fa[NCP ? 1 : DIM * V];
+  (void)fa;
+  if (!NCP && inr) {
+    // lFhi = sum_t w_t F(old iterate at t), accumulated in registers
+#pragma unroll
+    for (int k = 0; k < (NCP ? 1 : DIM * V); k++) fa[k] = 0.0;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+      double q[D], F[DIM * V];
+#pragma unroll
+      for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? q_s[(i * nd + p) * D + m] : u[m];
+      PDE::template flux<DIM>(q, F);
+      const double wi = G::weights(i);
+#pragma unroll
+      for (int k = 0; k < (NCP ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
+      if (live && a.ex_lFi) export_flux(i, F, nullptr);
+    }
   }
   __syncthreads();
   // stage lQhi [node][D] and lShi [node][V] in the slice region, lFhi in the flux blocks
@@ -505,26 +526,10 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
       for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
     } else {
-      // lFhi = sum_t w_t F(old iterate at t), accumulated in registers (the old iterate's time
-      // nodes die one by one as the loop consumes them) and stored once
-      double fa[DIM * V];
-#pragma unroll
-      for (int k = 0; k < DIM * V; k++) fa[k] = 0.0;
-#pragma unroll
-      for (int i = 0; i < n; i++) {
-        double q[D], F[DIM * V];
-#pragma unroll
-        for (int m = 0; m < D; m++) q[m] = m < V ? qo[i][m] : u[m];
-        PDE::template flux<DIM>(q, F);
-        const double wi = G::weights(i);
-#pragma unroll
-        for (int k = 0; k < DIM * V; k++) fa[k] = fma(F[k], wi, fa[k]);
-        if (live && a.ex_lFi) export_flux(i, F, nullptr);
-      }
 #pragma unroll
       for (int d = 0; d < DIM; d++)
 #pragma unroll
-        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[d * V + m];
+        for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(NCP ? 0 : d * V + m)];
     }
   }
   if (live && a.ex_lQhi) {
