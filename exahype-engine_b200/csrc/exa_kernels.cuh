@@ -60,6 +60,10 @@ struct FluxLayout<3, 4> {  // N=3: conflict-free
   EXA_FLUX_LAYOUT(16, 16, 1, 4, 0, 0, 0)
 };
 template <>
+struct FluxLayout<3, 8> {  // N=7: 9792 -> 5184 wavefronts per time node (conflict-free per direction)
+  EXA_FLUX_LAYOUT(16, 64, 1, 8, 0, 0, 0)
+};
+template <>
 struct FluxLayout<3, 5> {  // N=4: unpadded lines, block stride 137
   EXA_FLUX_LAYOUT(0, 0, 0, 0, 0, 0, 12)
 };

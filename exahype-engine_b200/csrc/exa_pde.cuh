@@ -19,6 +19,10 @@
 
 namespace exa {
 
+// correctly rounded reciprocal: the same value as 1 / x (IEEE round to nearest), fewer instructions
+__device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }
+__device__ __forceinline__ float recip(float x) { return 1.0f / x; }
+
 // Compressible Euler, gamma = 1.4 (ApplicationExamples/Euler/Euler_ADERDG/EulerSolver_ADERDG.cpp
 // :61-146). nVar = 5 in 2D and 3D; the 2D system carries the unused z-momentum Q[3].
 struct EulerPDE {
@@ -31,7 +35,7 @@ struct EulerPDE {
   template <int DIM, class T>
   static __device__ __forceinline__ void flux(const T* Q, T* F) {
     const T gamma = T(1.4);
-    const T irho = T(1) / Q[0];
+    const T irho = recip(Q[0]);
     const T j2 = DIM == 3 ? Q[1] * Q[1] + Q[2] * Q[2] + Q[3] * Q[3] : Q[1] * Q[1] + Q[2] * Q[2];
     const T p = (gamma - T(1)) * (Q[4] - T(0.5) * irho * j2);
 #pragma unroll

@@ -192,23 +192,35 @@ predictor_kernel(CellArgs a) {
   };
   // phase 2: contraction of every line with Kxi, in place, scaled by wi * w_a w_b dt/dx_d (:248-321)
   auto contract = [&](double wi) {
+    // two lines at a time: both lines' loads are issued before either line's math
 #pragma unroll
-    for (int r = 0; r < S::rounds; r++) {
-      const int pk = it_pack[r];
-      if (pk < 0) continue;
-      double* f = sF + (pk & 0x3ffff);
-      const int dd = (pk >> 18) & 3;
-      const int st = dd == 0 ? 1 : (dd == 1 ? n : n * n);
-      const double coef = wi * s_lw[(unsigned)pk >> 20];
-      double x[n];
+    for (int r = 0; r < S::rounds; r += 2) {
+      const int pk0 = it_pack[r];
+      const int pk1 = r + 1 < S::rounds ? it_pack[r + 1] : -1;
+      if (pk0 < 0) continue;
+      double* f0 = sF + (pk0 & 0x3ffff);
+      double* f1 = sF + (pk1 < 0 ? (pk0 & 0x3ffff) : (pk1 & 0x3ffff));
+      const int d0 = (pk0 >> 18) & 3, d1 = pk1 < 0 ? d0 : ((pk1 >> 18) & 3);
+      const int st0 = d0 == 0 ? 1 : (d0 == 1 ? n : n * n);
+      const int st1 = d1 == 0 ? 1 : (d1 == 1 ? n : n * n);
+      const double c0 = wi * s_lw[(unsigned)pk0 >> 20];
+      const double c1 = pk1 < 0 ? 0.0 : wi * s_lw[(unsigned)pk1 >> 20];
+      double x0[n], x1[n];
 #pragma unroll
-      for (int k = 0; k < n; k++) x[k] = f[k * st];
+      for (int k = 0; k < n; k++) {
+        x0[k] = f0[k * st0];
+        x1[k] = f1[k * st1];
+      }
 #pragma unroll
       for (int l = 0; l < n; l++) {
-        double acc = 0.0;
+        double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; k++) acc = fma(x[k], G::Kxi(k, l), acc);
-        f[l * st] = coef * acc;
+        for (int k = 0; k < n; k++) {
+          a0 = fma(x0[k], G::Kxi(k, l), a0);
+          a1 = fma(x1[k], G::Kxi(k, l), a1);
+        }
+        f0[l * st0] = c0 * a0;
+        if (pk1 >= 0) f1[l * st1] = c1 * a1;
       }
     }
   };

@@ -39,6 +39,7 @@ predictor_streamed_kernel(CellArgs a) {
   double* sF = smem;                        // [DIM][V][BS]
   double* sQh = smem + (size_t)DIM * V * BS;  // [nd][D]: lQhi in the tail
   __shared__ double s_lw[DIM * NL];
+  __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_red[T::TPB / 32];
   __shared__ double s_res;
 
@@ -53,6 +54,16 @@ predictor_streamed_kernel(CellArgs a) {
 #pragma unroll
   for (int d = 0; d < DIM; d++) off[d] = flux_off<DIM, n>(d, live_node ? p : 0);
   const size_t slab = (size_t)n * nd * V;
+  if (p < n) {
+    double A = 0.0, B = 0.0;
+#pragma unroll
+    for (int i = 0; i < n; i++) {
+      A = fma(G::iK1(p, i), G::F0(i), A);
+      B = fma(G::iK1(p, i), G::weights(i), B);
+    }
+    s_A[p] = A;
+    s_B[p] = B;
+  }
   double* slot = a.scratch + (size_t)blockIdx.x * T::slot_doubles;
 
   for (long cell = (long)a.cell_begin + blockIdx.x; cell < a.ncells; cell += gridDim.x) {
@@ -129,25 +140,38 @@ predictor_streamed_kernel(CellArgs a) {
     int sweeps = 0;
     bool last_old_is_luh = true;   // the last sweep started from lQi = luh
     for (int s = 0; s < maxIter; s++) {
+      double res = 0.0;
       if (s == 0) {
-        // lQi[., t] = luh (:71-82): one flux and one set of contractions for every time node
+        // lQi[., t] = luh (:71-82): one flux and one set of contractions for every time node.
+        // The rhs of time node i is (w_p F0[i] luh - w_i o + w_i w_p dt src_i) / w_p, so the iK1
+        // time solve has the closed form q1[t] = luh A[t] - o B[t] / w_p + dt sum_i iK1[t][i] w_i src_i.
         store_flux(u);
         __syncthreads();
         contract(1.0);
         __syncthreads();
         if (live_node) {
+          double cs[n];
 #pragma unroll
-          for (int i = 0; i < n; i++) {
-            const double wi = G::weights(i);
-            const double si = (PDE::kSource && srcOn) ? src_at(i) : 0.0;
+          for (int t = 0; t < n; t++) cs[t] = 0.0;
+          if (PDE::kSource && srcOn) {
+            for (int i = 0; i < n; i++) {
+              const double wsi = G::weights(i) * dt * src_at(i);
 #pragma unroll
-            for (int m = 0; m < V; m++) {
-              double o = 0.0;
+              for (int t = 0; t < n; t++) cs[t] = fma(G::iK1(t, i), wsi, cs[t]);
+            }
+          }
+#pragma unroll 1
+          for (int m = 0; m < V; m++) {
+            double o = 0.0;
 #pragma unroll
-              for (int d = 0; d < DIM; d++) o += sF[(d * V + m) * BS + off[d]];
-              double rhs = w_sp * G::F0(i) * u[m] - wi * o;
-              if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
-              R[((size_t)i * nd + p) * V + m] = iweight * rhs;
+            for (int d = 0; d < DIM; d++) o += sF[(d * V + m) * BS + off[d]];
+#pragma unroll
+            for (int t = 0; t < n; t++) {
+              double q1 = u[m] * s_A[t] - iweight * o * s_B[t];
+              if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
+              const double dl = q1 - u[m];
+              res = fma(dl, dl, res);
+              qn[((size_t)t * nd + p) * V + m] = q1;
             }
           }
         }
@@ -176,8 +200,7 @@ predictor_streamed_kernel(CellArgs a) {
         }
       }
       // iK1 time solve (:370-405) per node, residual against the old iterate
-      double res = 0.0;
-      if (live_node) {
+      if (live_node && s > 0) {
 #pragma unroll 1
         for (int m = 0; m < V; m++) {
           double r[n];
@@ -188,7 +211,7 @@ predictor_streamed_kernel(CellArgs a) {
             double q = 0.0;
 #pragma unroll
             for (int i = 0; i < n; i++) q = fma(r[i], G::iK1(t, i), q);
-            const double old = s == 0 ? u[m] : qo[((size_t)t * nd + p) * V + m];
+            const double old = qo[((size_t)t * nd + p) * V + m];
             const double dl = q - old;
             res = fma(dl, dl, res);
             qn[((size_t)t * nd + p) * V + m] = q;
@@ -313,29 +336,47 @@ predictor_streamed_kernel(CellArgs a) {
     }
 
     // ---------------- extrapolation to the faces (:517-687) ----------------
-    for (int j = p; j < S::sizeQhb + S::sizeFhb; j += T::TPB) {
-      int r = j;
-      const bool isQ = r < S::sizeQhb;
-      if (!isQ) r -= S::sizeQhb;
-      const int W = isQ ? D : V;
-      const int m = r % W;
-      const int fn = (r / W) % nf;
-      const int face = r / (W * nf);
-      const int d = face >> 1, o = face & 1;
+    // one thread per (lQhbnd or lFhbnd, direction, line): both faces of the line from one read
+    constexpr int LQ = DIM * NL;
+    for (int j = p; j < 2 * LQ; j += T::TPB) {
+      const bool isQ = j < LQ;
+      const int rl = isQ ? j : j - LQ;
+      const int d = rl / NL, L = rl % NL;
       const int st = line_stride<n>(d);
-      double acc = 0.0;
       if (isQ) {
-        if (!(DIM == 2 && d == 0 && m >= V)) {
-          const int base = line_base<DIM, n>(d, fn);
+        const double* src = sQh + (size_t)line_base<DIM, n>(d, L) * D;
+        double* o0 = a.lQhbnd + (size_t)cell * S::sizeQhb + (size_t)((2 * d) * nf + L) * D;
+        double* o1 = a.lQhbnd + (size_t)cell * S::sizeQhb + (size_t)((2 * d + 1) * nf + L) * D;
+#pragma unroll 1
+        for (int m = 0; m < D; m++) {
+          double a0 = 0.0, a1 = 0.0;
+          if (!(DIM == 2 && d == 0 && m >= V)) {
 #pragma unroll
-          for (int l = 0; l < n; l++) acc = fma(sQh[(size_t)(base + l * st) * D + m], o ? G::F1(l) : G::F0(l), acc);
+            for (int l = 0; l < n; l++) {
+              const double x = src[(size_t)l * st * D + m];
+              a0 = fma(x, G::F0(l), a0);
+              a1 = fma(x, G::F1(l), a1);
+            }
+          }
+          o0[m] = a0;
+          o1[m] = a1;
         }
-        a.lQhbnd[(size_t)cell * S::sizeQhb + r] = acc;
       } else {
-        const double* src = sF + (size_t)(d * V + m) * BS + flux_off<DIM, n>(d, line_base<DIM, n>(d, fn));
+        const double* src = sF + (size_t)d * V * BS + flux_off<DIM, n>(d, line_base<DIM, n>(d, L));
+        double* o0 = a.lFhbnd + (size_t)cell * S::sizeFhb + (size_t)((2 * d) * nf + L) * V;
+        double* o1 = a.lFhbnd + (size_t)cell * S::sizeFhb + (size_t)((2 * d + 1) * nf + L) * V;
+#pragma unroll 1
+        for (int m = 0; m < V; m++) {
+          double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-        for (int l = 0; l < n; l++) acc = fma(src[l * st], o ? G::F1(l) : G::F0(l), acc);
-        a.lFhbnd[(size_t)cell * S::sizeFhb + r] = acc;
+          for (int l = 0; l < n; l++) {
+            const double x = src[(size_t)m * BS + l * st];
+            a0 = fma(x, G::F0(l), a0);
+            a1 = fma(x, G::F1(l), a1);
+          }
+          o0[m] = a0;
+          o1[m] = a1;
+        }
       }
     }
     __syncthreads();  // shared memory and scratch are reused by the next cell
