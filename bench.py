@@ -109,8 +109,8 @@ def flops_per_cell_step(sweeps):
 
 PRED_BYTES_PER_CELL = 8.0 * (1080 + 1080 + 1080 + 1080)  # luh in; lduh, lQhbnd, lFhbnd out
 # DRAM bytes per cell of one predictor launch measured by ncu on a 27^3 block (19,683 cells):
-# 170.87 MB read + 456.64 MB written
-PRED_DRAM_BYTES_PER_CELL = (170.872832e6 + 456.639744e6) / 19683
+# 172.00 MB read + 466.63 MB written
+PRED_DRAM_BYTES_PER_CELL = (172.001024e6 + 466.628864e6) / 19683
 
 
 def cpu_baseline(steps=20, kind="reference"):
