@@ -434,6 +434,19 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
     s_F1[tid] = G::F1(tid);
   }
   if (tid < CPB) s_min[tid] = __longlong_as_double(0x7ff0000000000000ll);
+  // this node's state and volume update, loaded before the face fluxes are staged so that the
+  // three input streams are in flight together
+  double q[D], du[UPDATE ? V : 1];
+  if (live) {
+    const double* luh = a.luh + (size_t)cell * nd * D + (size_t)p * D;
+#pragma unroll
+    for (int m = 0; m < D; m++) q[m] = luh[m];
+    if (UPDATE) {
+      const double* lduh = a.lduh + (size_t)cell * nd * V + (size_t)p * V;
+#pragma unroll
+      for (int m = 0; m < (UPDATE ? V : 1); m++) du[m] = lduh[m];
+    }
+  }
   if (SURFACE) {
     for (int j = tid; j < CPB * S::sizeFhb; j += S::TPB) {
       const long gc = (long)a.cell_begin + (long)blockIdx.x * CPB + j / S::sizeFhb;
@@ -447,17 +460,9 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
   for (int d = 0; d < 3; d++) invDx[d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
   int co[3];
   node_coords<DIM, n>(p, co);
-  double q[D];
   bool ok = true;
   if (live) {
-    const double* luh = a.luh + (size_t)cell * nd * D + (size_t)p * D;
-#pragma unroll
-    for (int m = 0; m < D; m++) q[m] = luh[m];
     if (UPDATE) {
-      double du[V];
-      const double* lduh = a.lduh + (size_t)cell * nd * V + (size_t)p * V;
-#pragma unroll
-      for (int m = 0; m < V; m++) du[m] = lduh[m];
       if (SURFACE) {
         const double* Fb = sFb + lc * S::sizeFhb;
 #pragma unroll
@@ -468,7 +473,7 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
           const int k = co[d];
 #pragma unroll
           for (int m = 0; m < V; m++)
-            du[m] -= (Fb[((2 * d + 1) * nf + fn) * V + m] * s_F1[k] - Fb[((2 * d) * nf + fn) * V + m] * s_F0[k]) * us;
+            du[UPDATE ? m : 0] -= (Fb[((2 * d + 1) * nf + fn) * V + m] * s_F1[k] - Fb[((2 * d) * nf + fn) * V + m] * s_F0[k]) * us;
         }
       }
       const double w_sp = DIM == 3 ? s_w[co[2]] * s_w[co[1]] * s_w[co[0]] : s_w[co[1]] * s_w[co[0]];
@@ -476,7 +481,7 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(Cell
       double* out = a.luh_out + (size_t)cell * nd * D + (size_t)p * D;
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        q[m] = q[m] + du[m] * updateSize;
+        q[m] = q[m] + du[UPDATE ? m : 0] * updateSize;
         ok &= finite(q[m]);
         out[m] = q[m];
       }
