@@ -243,6 +243,7 @@ __global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predi
 
   // ---------------- recomputation of the Picard iterates q^1 .. q^{S-1} ----------------
   for (int s = 0; s + 1 < S_; s++) {
+#pragma unroll
     for (int i = 0; i < n; i++) {
       if (live) {
         double q[D], F[DIM * V];
@@ -411,6 +412,7 @@ __global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predi
         }
       }
     }
+#pragma unroll
     for (int i = 0; i < n; i++) {
       if (live) {
 #pragma unroll
