@@ -1335,9 +1335,12 @@ int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
     EXA_CUDA(cudaGetLastError());
     p->fixed_dt = dt;
   }
-  // forward predictor at u_k: the face traces the Rusanov adjoint linearises around
+  // forward predictor at u_k: the face traces the Rusanov adjoint linearises around, and the
+  // Picard iterates the reverse sweeps need (written into the adjoint scratch)
   exa::CellArgs c = patch_args(p);
+  c.ex_iter = p->adj_iter;
   EXA_CUDA(o.predictor(c, p->stream, false));
+  c.ex_iter = nullptr;
   exa::AdjArgs a;
   a.c = c;
   a.f = patch_faces(p);
@@ -1346,6 +1349,7 @@ int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
   a.adjF = p->adjF;
   a.iter = p->adj_iter;
   a.sweeps = S;
+  a.have_iter = 1;
   EXA_CUDA(p->s->ops->adjoint(a, p->stream));
   return EXA_OK;
 }

@@ -34,6 +34,7 @@ struct AdjArgs {
   double* adjF;    // [cell][2 DIM][nf][V]: adjoint of the predictor's lFhbnd (before Riemann)
   double* iter;    // [cell][S][n][nd][V]: Picard iterates 1..S-1 of the recomputation
   int sweeps;      // fixed Picard sweep count S >= 1
+  int have_iter;   // iter already holds q^1 .. q^{S-1} (written by the forward predictor)
 };
 
 template <class PDE, int DIM, int N, int P>
@@ -242,7 +243,8 @@ __global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predi
   __syncthreads();
 
   // ---------------- recomputation of the Picard iterates q^1 .. q^{S-1} ----------------
-  for (int s = 0; s + 1 < S_; s++) {
+  // (skipped when the forward predictor at u_k has exported them)
+  for (int s = 0; s + 1 < (a.have_iter ? 1 : S_); s++) {
 #pragma unroll
     for (int i = 0; i < n; i++) {
       if (live) {
