@@ -40,7 +40,7 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 // ADER-DG PNPM table by order (Toolkit/exahype/toolkit/solverController.py:17-23)
 // cell chunks of a host-buffer step (exa_patch_step_host)
-constexpr int kHostChunks = 16;
+constexpr int kHostChunks = 32;
 
 double default_pnpm(int order) {
   static const double t[10] = {1.0, 0.33, 0.17, 0.1, 0.069, 0.045, 0.038, 0.03, 0.02, 0.015};
