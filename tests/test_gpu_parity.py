@@ -582,3 +582,29 @@ def test_step_host_matches_device_steps(exa, torch, case):
     dev.close()
     host.close()
     multi.close()
+
+
+def test_step_host_fixed_then_cfl_and_halo_refusal(exa, torch):
+    """Host-buffer steps with a fixed dt followed by CFL steps follow the device-resident sequence
+    (the CFL step of the uploaded state is recomputed after fixed steps); halo patches are refused."""
+    rng = np.random.default_rng(21)
+    order, ncell, size = 3, (4, 3, 3), [1.0, 0.75, 0.75]
+    luh0 = euler_cells(rng, 36, 64, amp=0.05).reshape(-1)
+    s = exa.Solver(exa.PDE_EULER, 3, order)
+    dev = exa.Patch(s, [dict(ncell=ncell, size=size)])
+    dev.set_solution(luh0)
+    dev.step(2, 2e-3)
+    dev.step(2)
+    ref = dev.get_solution()
+    host = exa.Patch(s, [dict(ncell=ncell, size=size)])
+    buf = torch.from_numpy(luh0.copy()).pin_memory()
+    host.set_solution(buf.numpy())
+    host.step_host(buf, buf, 2e-3, nsteps=2)
+    host.step_host(buf, buf, 0.0, nsteps=2)
+    assert rel(buf.numpy(), ref) < 1e-14
+    assert np.allclose(host.time()[0], dev.time()[0], rtol=1e-15, atol=0)
+    halo = exa.Patch(s, [dict(ncell=ncell, size=size, bc=[exa.BC_PERIODIC, exa.BC_PERIODIC, exa.BC_HALO])])
+    with pytest.raises(exa.ExaError):
+        halo.step_host(buf, buf)
+    for p in (dev, host, halo):
+        p.close()
