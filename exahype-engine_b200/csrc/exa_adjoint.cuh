@@ -18,10 +18,11 @@
 //   adjoint_face_kernel       one warp per interior face: transposed surface integral of both
 //                             cells' lambda, transposed Rusanov -> adjoints of the predictor's
 //                             face traces (adjQ, adjF), both sides;
-//   adjoint_predictor_kernel  one CTA per cell, one thread per node: recomputes the Picard
-//                             iterates (stored in a global scratch), then runs the transposed
-//                             extrapolation, volume integral, time averaging and Picard sweeps in
-//                             reverse, and adds the result to lambda in place.
+//   adjoint_predictor_kernel  one CTA per cell, one thread per node: takes the Picard iterates
+//                             from a global scratch (written there by the forward predictor
+//                             launch when have_iter is set, else recomputed first), then runs
+//                             the transposed extrapolation, volume integral, time averaging and
+//                             Picard sweeps in reverse, and adds the result to lambda in place.
 #pragma once
 
 namespace exa {

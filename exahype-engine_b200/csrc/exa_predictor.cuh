@@ -13,15 +13,19 @@
 //            and writes it to shared memory,
 //   phase 2  every thread contracts whole lines (direction, variable, line) with Kxi, in place
 //            and already scaled by w_t w_a w_b dt/dx_d,
-//   phase 3  each thread forms its node's rhs and stores it, scaled by 1/w_xyz, as slice i.
-// The iK1 time solve runs once per sweep from the stored slices; the old iterate stays in
-// registers (the only per-node state carried across phases), the new one is staged in shared
-// memory until the per-cell residual decides whether the cell has converged.
+//   phase 3  each thread forms its node's rhs of time node i, scaled by 1/w_xyz, and folds it
+//            into the new iterate at every time node t through iK1[t][i] (the iK1 time solve
+//            distributed over the time nodes).
+// The new iterate lives in registers (n*V doubles per thread); the old iterate stays in the
+// shared slices [t][node][D] for the whole sweep (phase 1 and the residual read only the
+// thread's own node; the NCP gradients read neighbours) and is overwritten by the new one once
+// the per-cell residual has decided that another sweep follows.
 //
 // Sweep 0 starts from lQi[., t] = luh (:71-82), which is constant in time, so its flux and
-// contractions are computed once and weighted per time node (an exact identity, not an
-// approximation). For PDEs without NCP the time-averaged flux lFhi is re-evaluated from the final
-// old iterate after convergence instead of being carried through every sweep.
+// contractions are computed once and its time solve has a closed form (an exact identity, not
+// an approximation). For PDEs without NCP the time-averaged flux lFhi is accumulated in
+// registers from the final old iterate after the loop instead of being carried through every
+// sweep.
 #pragma once
 
 namespace exa {
