@@ -3,12 +3,18 @@
 // Picard iterate per cell). Same algorithm, same references and same results as
 // predictor_kernel (exa_predictor.cuh); only where the state lives differs:
 //
-//   shared memory  the flux blocks of one time node [dir][var][node] (contracted in place), and
-//                  in the tail the time-averaged state lQhi [node][D];
-//   registers      the node's luh;
-//   global scratch per resident CTA: the old and the new Picard iterate and the rhs slices,
-//                  [t][node][V] each. With one CTA per SM the scratch of all CTAs (148 x 3 x
-//                  8 x 512 x 9 doubles = 131 MB) stays mostly in L2.
+//   shared memory  the flux blocks of one time node [dir][var][node] (contracted in place),
+//                  and in the tail the time-averaged state lQhi [node][D];
+//                  The node's luh sits in its own row of the lQhi block until the tail
+//                  (registers are the limit at 512 threads; a runtime-indexed register array
+//                  would go to local memory, which misses L1 next to the scratch traffic).
+//   global scratch per resident CTA, two slabs [t][V][node]: the old Picard iterate, and the
+//                  rhs slices, which the time solve overwrites in place with the new iterate
+//                  (each thread reads all n slices of its own (node, variable) before writing).
+//                  Node-fastest, so that a warp's access to one (t, variable) is one coalesced
+//                  256-byte run.
+//                  With one CTA per SM the scratch of all CTAs (148 x 2 x 8 x 512 x 9 doubles =
+//                  87 MB) fits in L2.
 //
 // The kernel is persistent: gridDim.x CTAs walk the cells, CTA b using scratch slot b. One CTA
 // holds one cell, one thread per node (n^3 <= 1024). PDEs without NCP only.
@@ -22,8 +28,8 @@ struct StreamShape {
   static constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, NL = S::NL, BS = S::BS;
   static constexpr int TPB = (nd + 31) / 32 * 32;
   static constexpr int items = DIM * V * NL;
-  static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)nd * D);
-  static constexpr size_t slot_doubles = 3 * (size_t)n * nd * V;  // old, new, rhs
+  static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)TPB * D);
+  static constexpr size_t slot_doubles = 2 * (size_t)n * nd * V;  // old iterate; rhs, then new iterate
 };
 
 template <class PDE, int DIM, int N, int P>
@@ -36,8 +42,8 @@ predictor_streamed_kernel(CellArgs a) {
   static_assert(!PDE::kNCP, "the streamed predictor is built for PDEs without NCP");
   static_assert(T::TPB <= 1024, "one thread per node");
   extern __shared__ double smem[];
-  double* sF = smem;                        // [DIM][V][BS]
-  double* sQh = smem + (size_t)DIM * V * BS;  // [nd][D]: lQhi in the tail
+  double* sF = smem;                          // [DIM][V][BS]
+  double* sQh = smem + (size_t)DIM * V * BS;  // [TPB][D]: each node's luh, lQhi in the tail
   __shared__ double s_lw[DIM * NL];
   __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_red[T::TPB / 32];
@@ -75,9 +81,10 @@ predictor_streamed_kernel(CellArgs a) {
     for (int j = p; j < DIM * NL; j += T::TPB) {
       const int d = j / NL, L = j % NL;
       const double wt = DIM == 3 ? G::weights(L / n) * G::weights(L % n) : G::weights(L);
-      s_lw[j] = wt * dt * invdx[d];
+      s_lw[j] = wt * dt * (d == 0 ? invdx[0] : (d == 1 ? invdx[1] : invdx[2]));  // no runtime-indexed array
     }
-    double u[D];
+    // the node's luh, read by this thread only (the previous cell's tail ended with a barrier)
+    double* u = sQh + (size_t)p * D;
     {
       const double* luh = a.luh + (size_t)cell * nd * D + (size_t)(live_node ? p : 0) * D;
 #pragma unroll
@@ -133,9 +140,10 @@ predictor_streamed_kernel(CellArgs a) {
       }
     };
 
-    double* qo = slot;             // old iterate [t][node][V]
-    double* qn = slot + slab;      // new iterate
-    double* R = slot + 2 * slab;   // rhs slices, scaled by 1/w_p
+    double* qo = slot;             // old iterate [t][V][node]
+    double* qn = slot + slab;      // rhs slices (scaled by 1/w_p), then the new iterate
+    // entry (t, m) of this thread's node in a slab
+    auto at = [&](int t, int m) -> size_t { return ((size_t)t * V + m) * nd + p; };
     const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
     int sweeps = 0;
     bool last_old_is_luh = true;   // the last sweep started from lQi = luh
@@ -160,26 +168,28 @@ predictor_streamed_kernel(CellArgs a) {
               for (int t = 0; t < n; t++) cs[t] = fma(G::iK1(t, i), wsi, cs[t]);
             }
           }
-#pragma unroll 1
+#pragma unroll
           for (int m = 0; m < V; m++) {
             double o = 0.0;
+            const double um = u[m];
 #pragma unroll
             for (int d = 0; d < DIM; d++) o += sF[(d * V + m) * BS + off[d]];
 #pragma unroll
             for (int t = 0; t < n; t++) {
-              double q1 = u[m] * s_A[t] - iweight * o * s_B[t];
+              double q1 = um * s_A[t] - iweight * o * s_B[t];
               if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
-              const double dl = q1 - u[m];
+              const double dl = q1 - um;
               res = fma(dl, dl, res);
-              qn[((size_t)t * nd + p) * V + m] = q1;
+              qn[at(t, m)] = q1;
             }
           }
         }
       } else {
+        double* R = qn;
         for (int i = 0; i < n; i++) {
           double q[D];
 #pragma unroll
-          for (int m = 0; m < D; m++) q[m] = (m < V && live_node) ? qo[((size_t)i * nd + p) * V + m] : u[m];
+          for (int m = 0; m < D; m++) q[m] = (m < V && live_node) ? qo[at(i, m)] : u[m];
           store_flux(q);
           __syncthreads();
           contract(G::weights(i));
@@ -193,28 +203,33 @@ predictor_streamed_kernel(CellArgs a) {
 #pragma unroll
               for (int d = 0; d < DIM; d++) rhs -= sF[(d * V + m) * BS + off[d]];
               if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
-              R[((size_t)i * nd + p) * V + m] = iweight * rhs;
+              R[at(i, m)] = iweight * rhs;
             }
           }
           __syncthreads();  // the next time node overwrites the flux blocks
         }
       }
-      // iK1 time solve (:370-405) per node, residual against the old iterate
+      // iK1 time solve (:370-405) per node, in place over the rhs slices (all n slices of a
+      // (node, variable) are read before any is overwritten), residual against the old iterate
       if (live_node && s > 0) {
 #pragma unroll 1
         for (int m = 0; m < V; m++) {
-          double r[n];
+          // both columns are loaded before the first store: a store to qn may alias a later qo
+          // load as far as the compiler knows, which would serialise one round trip per load
+          double r[n], ol[n];
 #pragma unroll
-          for (int i = 0; i < n; i++) r[i] = R[((size_t)i * nd + p) * V + m];
+          for (int i = 0; i < n; i++) {
+            r[i] = qn[at(i, m)];
+            ol[i] = qo[at(i, m)];
+          }
 #pragma unroll
           for (int t = 0; t < n; t++) {
             double q = 0.0;
 #pragma unroll
             for (int i = 0; i < n; i++) q = fma(r[i], G::iK1(t, i), q);
-            const double old = qo[((size_t)t * nd + p) * V + m];
-            const double dl = q - old;
+            const double dl = q - ol[t];
             res = fma(dl, dl, res);
-            qn[((size_t)t * nd + p) * V + m] = q;
+            qn[at(t, m)] = q;
           }
         }
       }
@@ -248,20 +263,19 @@ predictor_streamed_kernel(CellArgs a) {
 
     // ---------------- time averaging (:441-515) ----------------
     // lQhi from the new iterate; lFhi = sum_t w_t F(old iterate of the last sweep at t)
-    double qh[D];
+    double qh[D] = {};
     if (live_node) {
 #pragma unroll
       for (int m = 0; m < D; m++) {
         double acc = 0.0;
 #pragma unroll
-        for (int t = 0; t < n; t++) acc = fma(m < V ? qn[((size_t)t * nd + p) * V + m] : u[m], G::weights(t), acc);
+        for (int t = 0; t < n; t++) acc = fma(m < V ? qn[at(t, m)] : u[m], G::weights(t), acc);
         qh[m] = acc;
-        sQh[(size_t)p * D + m] = acc;
       }
       if (a.ex_lQi) {
         double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
         for (int t = 0; t < n; t++)
-          for (int m = 0; m < D; m++) e[t * D + m] = m < V ? qn[((size_t)t * nd + p) * V + m] : u[m];
+          for (int m = 0; m < D; m++) e[t * D + m] = m < V ? qn[at(t, m)] : u[m];
       }
       if (a.ex_lQhi)
         for (int m = 0; m < D; m++) a.ex_lQhi[(size_t)cell * nd * D + p * D + m] = qh[m];
@@ -273,7 +287,7 @@ predictor_streamed_kernel(CellArgs a) {
       for (int i = 0; i < n; i++) {
         double q[D], F[DIM * V];
 #pragma unroll
-        for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? qo[((size_t)i * nd + p) * V + m] : u[m];
+        for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? qo[at(i, m)] : u[m];
         PDE::template flux<DIM>(q, F);
         const double wi = G::weights(i);
 #pragma unroll
@@ -298,6 +312,9 @@ predictor_streamed_kernel(CellArgs a) {
         }
         for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = 0.0;
       }
+      // lQhi replaces the node's luh row only now: the flux loop above still read luh
+#pragma unroll
+      for (int m = 0; m < D; m++) u[m] = qh[m];
     }
     __syncthreads();
 
