@@ -28,7 +28,9 @@ struct StreamShape {
   static constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, NL = S::NL, BS = S::BS;
   static constexpr int TPB = (nd + 31) / 32 * 32;
   static constexpr int items = DIM * V * NL;
-  static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)TPB * D);
+  // row stride of the luh / lQhi block: odd, so that a warp's rows fall in distinct bank pairs
+  static constexpr int DP = D | 1;
+  static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)TPB * DP);
   static constexpr size_t slot_doubles = 2 * (size_t)n * nd * V;  // old iterate; rhs, then new iterate
 };
 
@@ -43,14 +45,19 @@ predictor_streamed_kernel(CellArgs a) {
   static_assert(T::TPB <= 1024, "one thread per node");
   extern __shared__ double smem[];
   double* sF = smem;                          // [DIM][V][BS]
-  double* sQh = smem + (size_t)DIM * V * BS;  // [TPB][D]: each node's luh, lQhi in the tail
+  constexpr int DP = T::DP;
+  double* sQh = smem + (size_t)DIM * V * BS;  // [TPB][DP]: each node's luh, lQhi in the tail
   __shared__ double s_lw[DIM * NL];
   __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_red[T::TPB / 32];
   __shared__ double s_res;
+  // per-cell constants read after the set-up (kept out of registers, which are the limit at
+  // 512 threads): dt, 1/dx[3], dx[3] (as 1/(1/dx), the value the source geometry uses), t
+  __shared__ double s_cd[8];
+  __shared__ int s_grid;
 
   const int p = threadIdx.x;
-  const bool live_node = p < nd;
+  const bool live_node = T::TPB == nd || p < nd;  // whole warps of nodes: every thread has one
   int co[3] = {0, 0, 0};
   node_coords<DIM, n>(live_node ? p : 0, co);
   const double w_sp = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
@@ -84,7 +91,7 @@ predictor_streamed_kernel(CellArgs a) {
       s_lw[j] = wt * dt * (d == 0 ? invdx[0] : (d == 1 ? invdx[1] : invdx[2]));  // no runtime-indexed array
     }
     // the node's luh, read by this thread only (the previous cell's tail ended with a barrier)
-    double* u = sQh + (size_t)p * D;
+    double* u = sQh + (size_t)p * DP;
     {
       const double* luh = a.luh + (size_t)cell * nd * D + (size_t)(live_node ? p : 0) * D;
 #pragma unroll
@@ -100,13 +107,24 @@ predictor_streamed_kernel(CellArgs a) {
       srcOn = source_near<DIM>(a.src, cc, dxv);
       tcell = a.grid_t ? a.grid_t[g] : a.u_t;
     }
+    if (p == 0) {
+      s_cd[0] = dt;
+#pragma unroll
+      for (int d = 0; d < 3; d++) {
+        s_cd[1 + d] = invdx[d];
+        s_cd[4 + d] = dxv[d];
+      }
+      s_cd[7] = tcell;
+      s_grid = g;
+    }
     const int srcVar = (PDE::kSource && a.src) ? (int)a.src[7] : -1;
     auto src_at = [&](int i) -> double {
+      const double dxs[3] = {s_cd[4], s_cd[5], s_cd[6]};
       double cc[3], x[3];
-      cell_centre(a, cell, g, dxv, cc);
+      cell_centre(a, cell, s_grid, dxs, cc);
 #pragma unroll
-      for (int d = 0; d < 3; d++) x[d] = cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5);
-      return point_source<DIM>(a.src, x, tcell + G::nodes(i) * dt);
+      for (int d = 0; d < 3; d++) x[d] = cc[d] + dxs[d] * (G::nodes(co[d]) - 0.5);
+      return point_source<DIM>(a.src, x, s_cd[7] + G::nodes(i) * s_cd[0]);
     };
     __syncthreads();
 
@@ -163,7 +181,7 @@ predictor_streamed_kernel(CellArgs a) {
           for (int t = 0; t < n; t++) cs[t] = 0.0;
           if (PDE::kSource && srcOn) {
             for (int i = 0; i < n; i++) {
-              const double wsi = G::weights(i) * dt * src_at(i);
+              const double wsi = G::weights(i) * s_cd[0] * src_at(i);
 #pragma unroll
               for (int t = 0; t < n; t++) cs[t] = fma(G::iK1(t, i), wsi, cs[t]);
             }
@@ -202,7 +220,7 @@ predictor_streamed_kernel(CellArgs a) {
               double rhs = w_sp * G::F0(i) * u[m];
 #pragma unroll
               for (int d = 0; d < DIM; d++) rhs -= sF[(d * V + m) * BS + off[d]];
-              if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
+              if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * s_cd[0] * si;
               R[at(i, m)] = iweight * rhs;
             }
           }
@@ -328,7 +346,7 @@ predictor_streamed_kernel(CellArgs a) {
         const int L = node_line<DIM, n>(p, d);
         const int base = flux_off<DIM, n>(d, line_base<DIM, n>(d, L)), st = line_stride<n>(d);
         const double wt = DIM == 3 ? G::weights(L / n) * G::weights(L % n) : G::weights(L);
-        const double us = wt * invdx[d];
+        const double us = wt * s_cd[1 + d];
         const int k = co[d];
 #pragma unroll
         for (int m = 0; m < V; m++)
@@ -361,7 +379,7 @@ predictor_streamed_kernel(CellArgs a) {
       const int d = rl / NL, L = rl % NL;
       const int st = line_stride<n>(d);
       if (isQ) {
-        const double* src = sQh + (size_t)line_base<DIM, n>(d, L) * D;
+        const double* src = sQh + (size_t)line_base<DIM, n>(d, L) * DP;
         double* o0 = a.lQhbnd + (size_t)cell * S::sizeQhb + (size_t)((2 * d) * nf + L) * D;
         double* o1 = a.lQhbnd + (size_t)cell * S::sizeQhb + (size_t)((2 * d + 1) * nf + L) * D;
 #pragma unroll 1
@@ -370,7 +388,7 @@ predictor_streamed_kernel(CellArgs a) {
           if (!(DIM == 2 && d == 0 && m >= V)) {
 #pragma unroll
             for (int l = 0; l < n; l++) {
-              const double x = src[(size_t)l * st * D + m];
+              const double x = src[(size_t)l * st * DP + m];
               a0 = fma(x, G::F0(l), a0);
               a1 = fma(x, G::F1(l), a1);
             }
