@@ -28,8 +28,10 @@ struct StreamShape {
   static constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, NL = S::NL, BS = S::BS;
   static constexpr int TPB = (nd + 31) / 32 * 32;
   static constexpr int items = DIM * V * NL;
-  // row stride of the luh / lQhi block: odd, so that a warp's rows fall in distinct bank pairs
-  static constexpr int DP = D | 1;
+  // row of the luh / lQhi block: D entries, then w_p and 1/w_p of the node (read from shared
+  // memory where they are needed instead of occupying registers); the stride is odd, so that a
+  // warp's rows fall in distinct bank pairs
+  static constexpr int DP = (D + 2) | 1;
   static constexpr size_t smem = sizeof(double) * ((size_t)DIM * V * BS + (size_t)TPB * DP);
   static constexpr size_t slot_doubles = 2 * (size_t)n * nd * V;  // old iterate; rhs, then new iterate
 };
@@ -60,9 +62,12 @@ predictor_streamed_kernel(CellArgs a) {
   const bool live_node = T::TPB == nd || p < nd;  // whole warps of nodes: every thread has one
   int co[3] = {0, 0, 0};
   node_coords<DIM, n>(live_node ? p : 0, co);
-  const double w_sp = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
-                               : G::weights(co[1]) * G::weights(co[0]);
-  const double iweight = 1.0 / w_sp;
+  {
+    const double w = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
+                              : G::weights(co[1]) * G::weights(co[0]);
+    sQh[(size_t)p * DP + D] = w;
+    sQh[(size_t)p * DP + D + 1] = 1.0 / w;
+  }
   int off[DIM];
 #pragma unroll
   for (int d = 0; d < DIM; d++) off[d] = flux_off<DIM, n>(d, live_node ? p : 0);
@@ -79,7 +84,7 @@ predictor_streamed_kernel(CellArgs a) {
   }
   double* slot = a.scratch + (size_t)blockIdx.x * T::slot_doubles;
 
-  for (long cell = (long)a.cell_begin + blockIdx.x; cell < a.ncells; cell += gridDim.x) {
+  for (int cell = a.cell_begin + (int)blockIdx.x; cell < a.ncells; cell += (int)gridDim.x) {
     const int g = a.cell_grid ? a.cell_grid[cell] : 0;
     const double dt = a.grid_dt ? a.grid_dt[g] : a.u_dt;
     double invdx[3];
@@ -92,6 +97,8 @@ predictor_streamed_kernel(CellArgs a) {
     }
     // the node's luh, read by this thread only (the previous cell's tail ended with a barrier)
     double* u = sQh + (size_t)p * DP;
+    const double& w_sp = u[D];         // w_p (the tail overwrites only entries 0..D-1)
+    const double& iweight = u[D + 1];  // 1 / w_p
     {
       const double* luh = a.luh + (size_t)cell * nd * D + (size_t)(live_node ? p : 0) * D;
 #pragma unroll
@@ -186,7 +193,7 @@ predictor_streamed_kernel(CellArgs a) {
               for (int t = 0; t < n; t++) cs[t] = fma(G::iK1(t, i), wsi, cs[t]);
             }
           }
-#pragma unroll
+#pragma unroll 1
           for (int m = 0; m < V; m++) {
             double o = 0.0;
             const double um = u[m];
