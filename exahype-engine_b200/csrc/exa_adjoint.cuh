@@ -33,7 +33,7 @@ struct AdjArgs {
   double* lam;     // in: dJ/du_{k+1}; out: dJ/du_k (luh layout, D entries per node)
   double* adjQ;    // [cell][2 DIM][nf][D]: adjoint of the predictor's lQhbnd
   double* adjF;    // [cell][2 DIM][nf][V]: adjoint of the predictor's lFhbnd (before Riemann)
-  double* iter;    // [cell][S][n][nd][V]: Picard iterates 1..S-1 of the recomputation
+  double* iter;    // [cell][S][n][V][nd]: Picard iterates 1..S-1 (node-fastest: coalesced)
   int sweeps;      // fixed Picard sweep count S >= 1
   int have_iter;   // iter already holds q^1 .. q^{S-1} (written by the forward predictor)
 };
@@ -305,7 +305,7 @@ __global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predi
 #pragma unroll
           for (int i = 0; i < n; i++) qn = fma(r[i], G::iK1(t, i), qn);
           sQ[(t * nd + p) * V + m] = qn;
-          iter[((size_t)(s + 1) * n + t) * nd * V + (size_t)p * V + m] = qn;
+          iter[(((size_t)(s + 1) * n + t) * V + m) * nd + p] = qn;
         }
       }
     }
@@ -316,7 +316,7 @@ __global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predi
   auto iterate = [&](int s, int i, double* q) {
 #pragma unroll
     for (int m = 0; m < D; m++)
-      q[m] = (s == 0 || m >= V) ? u[m] : iter[((size_t)s * n + i) * nd * V + (size_t)p * V + m];
+      q[m] = (s == 0 || m >= V) ? u[m] : iter[(((size_t)s * n + i) * V + m) * nd + p];
   };
 
   // ---------------- reverse ----------------

@@ -151,7 +151,7 @@ struct CellArgs {
   // optional export of the predictor's internals, reference layouts (per-cell shims, tests)
   // scratch of the streamed predictor: one slot per resident CTA (set by the launcher)
   double* scratch;
-  // optional export of every sweep's new iterate [cell][S][n][nd][V] (slot s holds q^s; the
+  // optional export of every sweep's new iterate [cell][S][n][V][nd] (slot s holds q^s; the
   // adjoint reads them back instead of recomputing the Picard sweeps)
   double* ex_iter;
   double* ex_lQi;

@@ -475,11 +475,12 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
           for (int m = 0; m < V; m++) q_s[(t * nd + p) * D + m] = qn[t][m];
         if (a.ex_iter) {
-          double* e = a.ex_iter + ((size_t)cell * maxIter + s + 1) * n * nd * V + (size_t)p * V;
+          // [cell][sweep][t][V][node]: node-fastest, one coalesced run per (t, variable)
+          double* e = a.ex_iter + ((size_t)cell * maxIter + s + 1) * n * nd * V + p;
 #pragma unroll
           for (int t = 0; t < n; t++)
 #pragma unroll
-            for (int m = 0; m < V; m++) e[(size_t)t * nd * V + m] = qn[t][m];
+            for (int m = 0; m < V; m++) e[(size_t)(t * V + m) * nd] = qn[t][m];
         }
       } else {
         last_old_is_luh = s == 0;
