@@ -50,6 +50,9 @@ struct AdjShape {
   static constexpr int smemR = n * nd * V;
   static constexpr int smemF = DIM * V * nd;
   static constexpr size_t smem = sizeof(double) * (smemQ + smemR + smemF);
+  // four resident CTAs where the per-thread state (n*V adjoint accumulators) fits 128 registers
+  // without spilling (acoustic N=4: 166 -> 128 registers, 3 -> 4 CTAs per SM)
+  static constexpr int MinBlocks = (V <= 4 && TPB <= 128 && 4 * (smem + 2048) <= 228 * 1024) ? 4 : 1;
 };
 
 // ------------------------------------------------------------------------------------------
@@ -177,7 +180,8 @@ __device__ __forceinline__ void adj_contract(double* sF, const double* coef_line
 }
 
 template <class PDE, int DIM, int N, int P>
-__global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB)) adjoint_predictor_kernel(AdjArgs a) {
+__global__ void __launch_bounds__((AdjShape<PDE, DIM, N, P>::TPB), (AdjShape<PDE, DIM, N, P>::MinBlocks))
+adjoint_predictor_kernel(AdjArgs a) {
   using A = AdjShape<PDE, DIM, N, P>;
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
