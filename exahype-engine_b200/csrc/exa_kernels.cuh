@@ -419,8 +419,17 @@ __global__ void __launch_bounds__(256) boundary_kernel(FaceArgs f) {
 // ------------------------------------------------------------------------------------------
 // Surface integral + solution update + CFL of the new state
 // ------------------------------------------------------------------------------------------
+// Memory-bound: the register cap keeps enough CTAs resident to cover the loads (one 512-thread
+// cell per CTA: 2 CTAs per SM; at most 6 entries per node: 6 CTAs), at the cost of a few
+// spilled bytes; wider nodes in smaller CTAs keep the uncapped allocation (they would spill more).
+template <class PDE, int DIM, int N, int P>
+struct UpdateOcc {
+  using S = Shape<PDE, DIM, N, P>;
+  static constexpr int value = S::TPB >= 512 ? 2 : (S::D <= 6 ? 6 : 1);
+};
 template <class PDE, int DIM, int N, int P, bool SURFACE, bool UPDATE>
-__global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_kernel(CellArgs a) {
+__global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB, (UpdateOcc<PDE, DIM, N, P>::value))
+update_kernel(CellArgs a) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, CPB = S::CPB;
