@@ -2,13 +2,14 @@
 
 One "step" is one ADER-DG time step of the whole grid: CFL dt (fused into the previous step's
 update), fused space-time predictor + volume integral, Rusanov on every face, surface integral +
-solution update. Seeded synthetic entropy-wave state (BASELINE workload "3D Euler N=5 81^3"),
+solution update. Seeded synthetic entropy-wave state (the headline workload, 3D Euler N=5 81^3),
 inputs resident in HBM; 4.6 GB of luh per step, far above the 126 MB L2, so no L2 flush is needed.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Prints one JSON line (rank 0). With --gpus N > 1 (torchrun) every rank advances its own
-81^3 grid (weak scaling, no data-path collective; timing is the max over ranks).
+Prints one JSON line (rank 0). With --gpus N > 1 (torchrun) the grid is 81 x 81 x 81N cells cut
+into one 81^3 slab per rank (weak scaling): each step exchanges the slabs' face traces with the
+neighbours and all-reduces the CFL dt over NCCL; timing is the max over ranks.
 """
 import argparse
 import json
