@@ -511,9 +511,12 @@ def test_patch_fixed_dt_many_steps_vs_oracle(exa):
 
 
 @pytest.mark.parametrize("ncell,bc,steps,fixed", [((2, 3, 2), 3, 2, False), ((3, 2, 2), 0, 2, False),
-                                                  ((2, 2, 2), 1, 2, True)])
+                                                  ((2, 2, 2), 1, 2, True), ((6, 5, 6), 3, 2, False),
+                                                  ((8, 5, 8), 1, 2, True)])
 def test_patch_elastic_order7_streamed_vs_oracle(exa, ncell, bc, steps, fixed):
-    """Order 7 (8^3 nodes x 12 data per cell): the streamed predictor (iterates in global scratch)."""
+    """Order 7 (8^3 nodes x 12 data per cell): the streamed predictor (iterates in global scratch).
+    The persistent grid has one CTA per SM (148 on a B200): the 180- and 320-cell grids make CTAs
+    walk two or three cells, reusing their scratch slot and per-cell shared state."""
     import exa_scenarios as sc
     from pyoracle import PDE_ELASTIC
     order, size = 7, [1.0, 1.2, 0.9]
