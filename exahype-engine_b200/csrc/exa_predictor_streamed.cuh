@@ -45,6 +45,7 @@ predictor_streamed_kernel(CellArgs a) {
   constexpr int n = T::n, V = T::V, D = T::D, nd = T::nd, NL = T::NL, BS = T::BS, nf = S::nf;
   static_assert(!PDE::kNCP, "the streamed predictor is built for PDEs without NCP");
   static_assert(T::TPB <= 1024, "one thread per node");
+  static_assert(T::TPB == nd, "each flux slot is written and read by its own node's thread");
   extern __shared__ double smem[];
   double* sF = smem;                          // [DIM][V][BS]
   constexpr int DP = T::DP;
@@ -231,7 +232,8 @@ predictor_streamed_kernel(CellArgs a) {
               R[at(i, m)] = iweight * rhs;
             }
           }
-          __syncthreads();  // the next time node overwrites the flux blocks
+          // no barrier: the next phase 1 rewrites only this thread's own flux slots, which this
+          // thread has just read (every node has its own thread: TPB == nd is asserted below)
         }
       }
       // iK1 time solve (:370-405) per node, in place over the rhs slices (all n slices of a
