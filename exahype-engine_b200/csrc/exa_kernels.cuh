@@ -104,18 +104,31 @@ struct Shape {
   static constexpr int maxSweeps = 2 * n;
   // flux/partials block of one (cell, dir, var), laid out by FluxLayout
   static constexpr int BS = flux_block<DIM, n>();
-  // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][D] + flux/partials
-  static constexpr int smemQ = CPB * n * nd * D;
   static constexpr int smemF = CPB * DIM * V * BS;
+  static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
+  // predictor shared memory for a given per-node stride dq of the iterate slices and the luh
+  // block, without / with the mixed-precision buffer
+  static constexpr size_t smem_for(int dq, bool mixed) {
+    return sizeof(double) * (size_t)(CPB * n * nd * dq + smemF + CPB * nd * dq + (mixed ? smemO : 0));
+  }
+  // resident CTAs per SM: two when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
+  static constexpr int blocks_for(int dq) { return 2 * (smem_for(dq, true) + 3 * 1024) <= 228 * 1024 ? 2 : 1; }
+  static constexpr bool fits_cta(size_t bytes) { return bytes + 4096 <= 227 * 1024; }
+  // per-node stride of the iterate slices and the luh block in shared memory: D rounded up to an
+  // odd count (an even stride puts several lanes of a warp on one bank), unless the padding
+  // would cost a resident CTA or push a form of the kernel past one CTA's shared memory
+  static constexpr bool pad_ok = D % 2 == 0 && blocks_for(D | 1) >= blocks_for(D) &&
+                                 fits_cta(smem_for(D | 1, false)) >= fits_cta(smem_for(D, false)) &&
+                                 fits_cta(smem_for(D | 1, true)) >= fits_cta(smem_for(D, true));
+  static constexpr int DQ = pad_ok ? (D | 1) : D;
+  // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][DQ] + flux/partials
+  static constexpr int smemQ = CPB * n * nd * DQ;
   static constexpr int items = CPB * DIM * V * NL;             // line contractions per time node
   static constexpr int rounds = (items + TPB - 1) / TPB;       // per thread
-  static constexpr int smemU = CPB * nd * D;                   // luh of the CTA's cells
-  static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
+  static constexpr int smemU = CPB * nd * DQ;                  // luh of the CTA's cells
   static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF + smemU);
   static constexpr size_t predictor_smem_mixed = sizeof(double) * (smemQ + smemF + smemU + smemO);
-  // two resident CTAs per SM when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
-  static constexpr int MinBlocks =
-      2 * (sizeof(double) * (smemQ + smemF + smemU + smemO) + 3 * 1024) <= 228 * 1024 ? 2 : 1;
+  static constexpr int MinBlocks = blocks_for(DQ);
   // registers are split over the SM's four 16K-register partitions: B blocks of W warps need
   // ceil(B*W/4) warps' worth of registers in one partition
   static constexpr int WarpsPerSmsp = (MinBlocks * (TPB / 32) + 3) / 4;

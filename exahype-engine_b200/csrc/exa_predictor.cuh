@@ -48,10 +48,11 @@ predictor_kernel(CellArgs a) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, NL = S::NL, CPB = S::CPB, BS = S::BS;
+  constexpr int DQ = S::DQ;  // per-node stride of the iterate slices and the luh block (odd)
   constexpr bool NCP = PDE::kNCP;
   static_assert(!(MIXED && NCP), "the mixed-precision sweeps are built for PDEs without NCP");
   extern __shared__ double smem[];
-  double* sQ = smem;              // [CPB][n][nd][D]: old iterate (NCP), rhs slices, new iterate
+  double* sQ = smem;              // [CPB][n][nd][DQ]: old iterate slices, lQhi in the tail
   double* sF = smem + S::smemQ;   // [CPB][DIM][V][BS]: fluxes, contracted in place
   __shared__ double s_w[n], s_Kxi[n * n], s_dudx[n * n];
   __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
@@ -152,7 +153,7 @@ predictor_kernel(CellArgs a) {
 
   // luh of this node, kept in shared memory (read once per phase, not worth 2*D registers);
   // the old iterate starts as lQi[., t] = luh (:71-82)
-  double* u = sQ + S::smemQ + S::smemF + ((size_t)lc * nd + p) * D;
+  double* u = sQ + S::smemQ + S::smemF + ((size_t)lc * nd + p) * DQ;
   if (inr) {
     const double* luh = a.luh + (size_t)cell * nd * D + (size_t)p * D;
 #pragma unroll
@@ -163,13 +164,13 @@ predictor_kernel(CellArgs a) {
   // new iterate of the sweep, accumulated in registers time node by time node (the iK1 time
   // solve distributed over phase 3); the old iterate is staged in the slices q_s [t][node][D]
   double qn[n][V];
-  double* q_s = sQ + (size_t)lc * n * nd * D;
+  double* q_s = sQ + (size_t)lc * n * nd * DQ;
   double* f_s = sF + (size_t)lc * DIM * V * BS;
   if (NCP && inr) {  // neighbours' old iterate is read by the gradients
 #pragma unroll
     for (int t = 0; t < n; t++)
 #pragma unroll
-      for (int m = 0; m < D; m++) q_s[(t * nd + p) * D + m] = u[m];
+      for (int m = 0; m < D; m++) q_s[(t * nd + p) * DQ + m] = u[m];
   }
   double fh[NCP ? DIM : 1][V];   // time-averaged flux / source of the sweep (NCP path only)
   double sh[V];
@@ -189,7 +190,7 @@ predictor_kernel(CellArgs a) {
       for (int m = 0; m < V; m++) {
         double g = 0.0;
 #pragma unroll
-        for (int k = 0; k < n; k++) g += 1.0 * invDx[d] * q_s[(ti * nd + base + k * st) * D + m] * s_dudx[l * n + k];
+        for (int k = 0; k < n; k++) g += 1.0 * invDx[d] * q_s[(ti * nd + base + k * st) * DQ + m] * s_dudx[l * n + k];
         gq[d * V + m] = g;
       }
     }
@@ -364,7 +365,7 @@ predictor_kernel(CellArgs a) {
         // phase 1: flux (and NCP source) of the old iterate at time node i (:196-227, :323-367)
         double q[D];
 #pragma unroll
-        for (int m = 0; m < D; m++) q[m] = m < V ? q_s[(i * nd + p) * D + m] : u[m];
+        for (int m = 0; m < D; m++) q[m] = m < V ? q_s[(i * nd + p) * DQ + m] : u[m];
         double F[DIM * V];
         double Si[V];
         PDE::template flux<DIM>(q, F);
@@ -441,7 +442,7 @@ predictor_kernel(CellArgs a) {
         for (int t = 0; t < n; t++)
 #pragma unroll
           for (int m = 0; m < V; m++) {
-            const double dl = qn[t][m] - q_s[(t * nd + p) * D + m];
+            const double dl = qn[t][m] - q_s[(t * nd + p) * DQ + m];
             res = fma(dl, dl, res);
           }
       }
@@ -473,7 +474,7 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
         for (int t = 0; t < n; t++)
 #pragma unroll
-          for (int m = 0; m < V; m++) q_s[(t * nd + p) * D + m] = qn[t][m];
+          for (int m = 0; m < V; m++) q_s[(t * nd + p) * DQ + m] = qn[t][m];
         if (a.ex_iter) {
           // [cell][sweep][t][V][node]: node-fastest, one coalesced run per (t, variable)
           double* e = a.ex_iter + ((size_t)cell * maxIter + s + 1) * n * nd * V + p;
@@ -527,7 +528,7 @@ predictor_kernel(CellArgs a) {
     for (int i = 0; i < n; i++) {
       double q[D], F[DIM * V];
 #pragma unroll
-      for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? q_s[(i * nd + p) * D + m] : u[m];
+      for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? q_s[(i * nd + p) * DQ + m] : u[m];
       PDE::template flux<DIM>(q, F);
       const double wi = G::weights(i);
 #pragma unroll
@@ -536,12 +537,12 @@ predictor_kernel(CellArgs a) {
     }
   }
   __syncthreads();
-  // stage lQhi [node][D] and lShi [node][V] in the slice region, lFhi in the flux blocks
+  // stage lQhi [node][DQ] and lShi [node][V] in the slice region, lFhi in the flux blocks
   double* qh_s = q_s;
-  double* sh_s = q_s + nd * D;
+  double* sh_s = q_s + nd * DQ;
   if (inr) {
 #pragma unroll
-    for (int m = 0; m < D; m++) qh_s[p * D + m] = qh[m];
+    for (int m = 0; m < D; m++) qh_s[p * DQ + m] = qh[m];
     if (NCP) {
 #pragma unroll
       for (int d = 0; d < DIM; d++)
@@ -622,7 +623,7 @@ predictor_kernel(CellArgs a) {
     const int d = rl / NL, L = rl % NL;
     const int st = d == 0 ? 1 : (d == 1 ? n : n * n);
     if (isQ) {
-      const double* src = smem + (size_t)c * n * nd * D + (size_t)line_base<DIM, n>(d, L) * D;
+      const double* src = smem + (size_t)c * n * nd * DQ + (size_t)line_base<DIM, n>(d, L) * DQ;
       double* o0 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d) * nf + L) * D;
       double* o1 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d + 1) * nf + L) * D;
 #pragma unroll
@@ -632,7 +633,7 @@ predictor_kernel(CellArgs a) {
         if (!(DIM == 2 && d == 0 && m >= V)) {
 #pragma unroll
           for (int l = 0; l < n; l++) {
-            const double x = src[(size_t)l * st * D + m];
+            const double x = src[(size_t)l * st * DQ + m];
             a0 = fma(x, G::F0(l), a0);
             a1 = fma(x, G::F1(l), a1);
           }
