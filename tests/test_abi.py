@@ -45,3 +45,20 @@ def test_host_only_calls():
     cfg = exa_aderdg._Config(3, 8, 0, 0, 0.9, 0.0, 0, 0)
     assert lib.exa_solver_create(ctypes.byref(cfg), ctypes.byref(h)) == 2  # not instantiated
     assert lib.exa_solver_create(None, ctypes.byref(h)) == 1
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    """Without the compiled library the binding raises; there is no CPU fallback to run instead."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r)\n"
+            "import exa_aderdg\n"
+            "try:\n"
+            "    exa_aderdg.load_library(%r)\n"
+            "except exa_aderdg.ExaError as e:\n"
+            "    print('raised:', e)\n"
+            "    sys.exit(0)\n"
+            "sys.exit(1)\n") % (os.path.join(REPO, "exahype-engine_b200"), str(tmp_path / "libexa_aderdg.so"))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "missing" in r.stdout
