@@ -216,16 +216,22 @@ predictor_kernel(CellArgs a) {
         x0[k] = f0[k * st0];
         x1[k] = f1[k * st1];
       }
+      // k outermost: 2n independent accumulation chains instead of two (the DFMA latency is
+      // hidden inside the warp); each output still sums k = 0..n-1 in order
+      double a0[n], a1[n];
+#pragma unroll
+      for (int l = 0; l < n; l++) a0[l] = a1[l] = 0.0;
+#pragma unroll
+      for (int k = 0; k < n; k++)
+#pragma unroll
+        for (int l = 0; l < n; l++) {
+          a0[l] = fma(x0[k], G::Kxi(k, l), a0[l]);
+          a1[l] = fma(x1[k], G::Kxi(k, l), a1[l]);
+        }
 #pragma unroll
       for (int l = 0; l < n; l++) {
-        double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < n; k++) {
-          a0 = fma(x0[k], G::Kxi(k, l), a0);
-          a1 = fma(x1[k], G::Kxi(k, l), a1);
-        }
-        f0[l * st0] = c0 * a0;
-        if (pk1 >= 0) f1[l * st1] = c1 * a1;
+        f0[l * st0] = c0 * a0[l];
+        if (pk1 >= 0) f1[l * st1] = c1 * a1[l];
       }
     }
   };
