@@ -112,7 +112,7 @@ def flops_per_cell_step(sweeps):
 PRED_BYTES_PER_CELL = 8.0 * (1080 + 1080 + 1080 + 1080)  # luh in; lduh, lQhbnd, lFhbnd out
 # DRAM bytes per cell of one predictor launch measured by ncu on a 27^3 block (19,683 cells):
 # 172.00 MB read + 466.63 MB written
-PRED_DRAM_BYTES_PER_CELL = (172.001024e6 + 466.628864e6) / 19683
+PRED_DRAM_BYTES_PER_CELL = (171.954432e6 + 462.412288e6) / 19683
 
 
 def cpu_baseline(steps=20, kind="reference"):
