@@ -3,11 +3,12 @@
 // Picard iterate per cell). Same algorithm, same references and same results as
 // predictor_kernel (exa_predictor.cuh); only where the state lives differs:
 //
-//   shared memory  the flux blocks of one time node [dir][var][node] (contracted in place),
-//                  and in the tail the time-averaged state lQhi [node][D];
-//                  The node's luh sits in its own row of the lQhi block until the tail
-//                  (registers are the limit at 512 threads; a runtime-indexed register array
-//                  would go to local memory, which misses L1 next to the scratch traffic).
+//   shared memory  the flux blocks of one time node [dir][var][node] (contracted in place);
+//                  one row per node [node][DP]: its luh during the sweeps, lQhi in the tail,
+//                  and w_p, 1/w_p in the spare entries; the per-cell constants. Registers are
+//                  the limit at 512 threads, so these stay out of them (a runtime-indexed
+//                  register array would go to local memory, which misses L1 next to the
+//                  scratch traffic).
 //   global scratch per resident CTA, two slabs [t][V][node]: the old Picard iterate, and the
 //                  rhs slices, which the time solve overwrites in place with the new iterate
 //                  (each thread reads all n slices of its own (node, variable) before writing).
