@@ -104,7 +104,11 @@ struct Shape {
   static constexpr int maxSweeps = 2 * n;
   // flux/partials block of one (cell, dir, var), laid out by FluxLayout
   static constexpr int BS = flux_block<DIM, n>();
-  static constexpr int smemF = CPB * DIM * V * BS;
+  // stride between the flux blocks of the CTA's cells: in 2D, where a warp spans parts of two
+  // cells, one pad double makes it odd, so the next cell's lanes land on other bank pairs than
+  // the ones the first cell's lanes already use twice
+  static constexpr int FCS = DIM * V * BS + ((DIM == 2 && CPB > 1 && (DIM * V * BS) % 2 == 0) ? 1 : 0);
+  static constexpr int smemF = CPB * FCS;
   static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
   // predictor shared memory for a given per-node stride dq of the iterate slices and the luh
   // block, without / with the mixed-precision buffer

@@ -49,11 +49,12 @@ predictor_kernel(CellArgs a) {
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, NL = S::NL, CPB = S::CPB, BS = S::BS;
   constexpr int DQ = S::DQ;  // per-node stride of the iterate slices and the luh block (odd)
+  constexpr int FCS = S::FCS;  // stride between the cells' flux blocks
   constexpr bool NCP = PDE::kNCP;
   static_assert(!(MIXED && NCP), "the mixed-precision sweeps are built for PDEs without NCP");
   extern __shared__ double smem[];
   double* sQ = smem;              // [CPB][n][nd][DQ]: old iterate slices, lQhi in the tail
-  double* sF = smem + S::smemQ;   // [CPB][DIM][V][BS]: fluxes, contracted in place
+  double* sF = smem + S::smemQ;   // [CPB][FCS >= DIM*V*BS]: fluxes, contracted in place
   __shared__ double s_w[n], s_Kxi[n * n], s_dudx[n * n];
   __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_lw[CPB * DIM * NL];  // w_a w_b dt / dx_d of every line
@@ -144,7 +145,7 @@ predictor_kernel(CellArgs a) {
       const int m = (it / NL) % V;
       const int d = (it / (NL * V)) % DIM;
       const int c = it / (NL * V * DIM);
-      it_pack[r] = (((c * DIM + d) * V + m) * BS + pline_base<DIM, n>(d, L)) | (d << 18) |
+      it_pack[r] = (c * FCS + (d * V + m) * BS + pline_base<DIM, n>(d, L)) | (d << 18) |
                    (((c * DIM + d) * NL + L) << 20);
     } else {
       it_pack[r] = -1;
@@ -165,7 +166,7 @@ predictor_kernel(CellArgs a) {
   // solve distributed over phase 3); the old iterate is staged in the slices q_s [t][node][D]
   double qn[n][V];
   double* q_s = sQ + (size_t)lc * n * nd * DQ;
-  double* f_s = sF + (size_t)lc * DIM * V * BS;
+  double* f_s = sF + (size_t)lc * FCS;
   if (NCP && inr) {  // neighbours' old iterate is read by the gradients
 #pragma unroll
     for (int t = 0; t < n; t++)
@@ -244,9 +245,9 @@ predictor_kernel(CellArgs a) {
       const int pk = it_pack[r];
       if (pk < 0) continue;
       // the packed offset counts doubles; the float view of cell c's flux block starts at float
-      // index 2*c*DIM*V*BS (the floats of every cell sit in the first half of its own block)
+      // index 2*c*FCS (the floats of every cell sit in the first half of its own block)
       const int bd = pk & 0x3ffff;
-      float* f = sFf + bd + (bd / (DIM * V * BS)) * (DIM * V * BS);
+      float* f = sFf + bd + (bd / FCS) * FCS;
       const int dd = (pk >> 18) & 3;
       const int st = dd == 0 ? 1 : (dd == 1 ? n : n * n);
       const float coef = wi * (float)s_lw[(unsigned)pk >> 20];
@@ -648,7 +649,7 @@ predictor_kernel(CellArgs a) {
         o1[m] = a1;
       }
     } else {
-      const double* src = sF + (size_t)(c * DIM + d) * V * BS + pline_base<DIM, n>(d, L);
+      const double* src = sF + (size_t)c * FCS + (size_t)d * V * BS + pline_base<DIM, n>(d, L);
       double* o0 = a.lFhbnd + (size_t)gc * S::sizeFhb + (size_t)((2 * d) * nf + L) * V;
       double* o1 = a.lFhbnd + (size_t)gc * S::sizeFhb + (size_t)((2 * d + 1) * nf + L) * V;
 #pragma unroll
