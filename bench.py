@@ -244,7 +244,7 @@ def run_swe_batched(args):
                                    "reflective walls, per-grid CFL dt, one CUDA graph per step",
                        "cells": cells, "dof_per_step": dof_step},
             "picard_sweeps_mean": sweeps, "status_bits": patch.status(),
-            "roofline": {"bound": "tensor", "kernel": "predictor_kernel (SWE, NCP)", "achieved": achieved,
+            "roofline": {"bound": "fp64", "kernel": "predictor_kernel (SWE, NCP)", "achieved": achieved,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run", "traffic": None,
                          "launch_ms": pred_ms, "algorithmic_flops_per_launch": flops_launch},
@@ -463,7 +463,7 @@ def run_elastic3d(args):
                        "cells": cells, "dof_per_step": dof_step, "l2": "inputs 5.4 GB > L2, no flush needed"},
             "picard_sweeps_mean": sweeps, "status_bits": patch.status(),
             "initial_state": "smooth random velocity field" if args.elastic_active else "at rest (source-driven)",
-            "roofline": {"bound": "tensor", "kernel": "predictor_streamed_kernel", "achieved": achieved,
+            "roofline": {"bound": "fp64", "kernel": "predictor_streamed_kernel", "achieved": achieved,
                          "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                          "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run", "traffic": None,
                          "launch_ms": pred_ms, "algorithmic_flops_per_launch": flops_launch},
@@ -681,13 +681,12 @@ def main():
         "accuracy": {"t": float(t_now[0]), "l2_rho_vs_exact": l2_exact, "linf_rho_vs_exact": linf_exact,
                      "sample": "every 37th cell, exact entropy wave at t"},
         "other_precision": other,
-        "roofline": {"bound": "tensor", "kernel": "predictor_kernel (fused Picard + volume integral)",
+        "roofline": {"bound": "fp64", "kernel": "predictor_kernel (fused Picard + volume integral)",
                      "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
                      "peak_source": "FP64 cuBLAS DGEMM 8192^3 measured in this run",
                      "traffic": PRED_DRAM_BYTES_PER_CELL * cells,
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch "
-                                       "on a 27^3 block (profiles/predictor_euler3d_n5_27cubed_ncu.md), scaled "
-                                       "by cells",
+                                       "on a 27^3 block, scaled by cells",
                      "algorithmic_flops_per_launch": flops_launch, "launch_ms": pred_ms,
                      "hbm_gbs_of_launch": cells * PRED_BYTES_PER_CELL / (pred_ms * 1e-3) / 1e9,
                      "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},

@@ -1283,12 +1283,11 @@ extern "C" int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, i
     a.ncells = ncells;
     a.luh = luh;
     a.cell_dt = d_cell;
+    a.grid_dt_next = d_min;  // every cell counts as grid 0: per-cell minima atomic-min into d_min
     a.status = d_status;
     a.cfl_pnpm = (cfg->cfl > 0 ? cfg->cfl : 0.9) * (cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order));
     for (int d = 0; d < 3; d++) a.u_dx[d] = d < cfg->dim ? dx[d] : 1.0;
     EXA_CUDA(ops->update(a, false, false, st));
-    exa::min_reduce_kernel<<<1, 1024, 0, st>>>(ncells, d_cell, d_min);
-    EXA_CUDA(cudaGetLastError());
     if (cell_dt) EXA_CUDA(cudaMemcpyAsync(cell_dt, d_cell, sizeof(double) * ncells, cudaMemcpyDeviceToDevice, st));
   }
   unsigned bits = 0;

@@ -534,7 +534,11 @@ update_kernel(CellArgs a) {
       den += mx * invDx[d];
     }
     dtp = a.cfl_pnpm / den;
-    if (!(dtp > 0.0)) {  // NaN or non-positive
+    // a non-finite state gives no time step (fmax drops NaN eigenvalues, so den alone can look fine)
+    bool qok = true;
+#pragma unroll
+    for (int m = 0; m < D; m++) qok &= finite(q[m]);
+    if (!(dtp > 0.0) || !qok) {  // NaN, non-positive, or from a non-finite state
       if (a.status) atomicOr(a.status, ST_BAD_DT);
       dtp = __longlong_as_double(0x7ff0000000000000ll);
     }
@@ -569,23 +573,6 @@ __global__ void advance_kernel(int ngrids, double* t, double* dt, double* dt_nex
     dt_next[g] = __longlong_as_double(0x7ff0000000000000ll);
   }
   if (g == 0 && steps) steps[0] += 1;
-}
-
-// Deterministic min of count values by one block (grid-stride, then a warp and block tree).
-__global__ void __launch_bounds__(1024) min_reduce_kernel(int count, const double* x, double* out) {
-  __shared__ double part[32];
-  double v = __longlong_as_double(0x7ff0000000000000ll);
-  for (int i = threadIdx.x; i < count; i += blockDim.x) v = fmin(v, x[i]);
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
-  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    v = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : __longlong_as_double(0x7ff0000000000000ll);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, off));
-    if (threadIdx.x == 0) out[0] = v;
-  }
 }
 
 __global__ void fill_kernel(int count, double* x, double v) {

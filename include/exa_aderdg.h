@@ -144,7 +144,10 @@ int exa_solution_update(exa_solver* s, int ncells, double* luh, const double* lu
 /* Replaces stableTimeStepSize (3d/stableTimeStepSize.cpph:14-62) and the min-reduction over
  * cells (ADERDGSolver::updateAdmissibleTimeStepSize, ADERDGSolver.cpp:458-462). cell_dt
  * (device, nullable) receives every cell's value; *dt_min (host, nullable) the minimum --
- * requesting it synchronises the stream. */
+ * requesting it synchronises the stream. Cells whose state is non-finite or gives dt <= 0 set
+ * bits in the solver's status word (exa_solver_status) and count as +inf; unlike
+ * exa_stable_time_step_size_noalloc, the call itself still returns EXA_OK, because the status
+ * word also collects the bits of the solver's other kernels. */
 int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
                               double* dt_min, void* stream);
 
@@ -166,9 +169,18 @@ int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, cons
  *   - ncells > EXA_NOALLOC_MAX_CELLS is rejected with EXA_ERR_INVALID before any device work.
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) and
  *     caches it for that device; make that first call before any stream capture.
+ *   - With lazy module loading (the CUDA default), the call that first loads the library's
+ *     module on a device is what places the array in device memory. A caller whose device memory
+ *     another runtime reserves should make its first call per device (or set
+ *     CUDA_MODULE_LOADING=EAGER) before that runtime reserves the pool.
+ *   - The cached address is only valid for the context it was looked up in: after
+ *     cudaDeviceReset the module is loaded again and the array may move, so do not call this
+ *     entry point after a device reset in the same process.
  *   - All calls share the one array and each call resets what it reads, but calls that overlap
  *     on the GPU (other streams, other host threads) race on it: serialise them.
- * Returns EXA_ERR_NUMERICS when a cell's state is non-finite or gives dt <= 0 (dt_min requested). */
+ * Returns EXA_ERR_NUMERICS when a cell's state is non-finite or gives dt <= 0 and dt_min was
+ * requested (the call then reads the status word after synchronising). With dt_min == NULL the
+ * call does not synchronise and reports no numerical status; such cells get +inf in cell_dt. */
 #define EXA_NOALLOC_MAX_CELLS 1048576
 int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, int ncells, const double* luh, const double* dx,
                                       double* cell_dt, double* dt_min, void* stream);
@@ -210,8 +222,8 @@ typedef struct {
 
 typedef struct {
   long long steps;          /* steps taken since creation */
-  double picard_mean;       /* mean Picard sweeps per cell over all steps (needs track_picard) */
-  int picard_hist[32];      /* sweeps histogram of the last step (needs track_picard) */
+  double picard_mean;       /* mean Picard sweeps per cell of the last step */
+  int picard_hist[32];      /* sweeps histogram of the last step (index = sweeps, capped at 31) */
 } exa_patch_stats;
 
 int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_patch** out);
@@ -228,7 +240,7 @@ double* exa_patch_luh(exa_patch* p);
 int exa_patch_step(exa_patch* p, int nsteps, double fixed_dt);
 int exa_patch_sync(exa_patch* p);
 int exa_patch_time(exa_patch* p, double* t, double* dt);   /* host arrays of ngrids (synchronises) */
-int exa_patch_track_picard(exa_patch* p, int on);
+int exa_patch_track_picard(exa_patch* p, int on);       /* kept for compatibility: sweeps are always recorded */
 int exa_patch_stats_get(exa_patch* p, exa_patch_stats* st);
 int exa_patch_status(exa_patch* p, unsigned* bits);       /* reads and clears (synchronises) */
 void* exa_patch_stream(exa_patch* p);                     /* the cudaStream_t the patch runs on */

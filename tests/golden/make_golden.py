@@ -1,9 +1,9 @@
 """Generate the committed golden fixtures under tests/golden/.
 
-Run in a container that has the reference checkout (default /root/reference) and the built
+Run where the reference checkout is present (--ref, or the EXAHYPE_REF environment variable) and the built
 checker library oracle/_ref (``make -C oracle ref``):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref PATH_TO_EXAHYPE_CHECKOUT]
 
 Outputs
 -------
@@ -149,7 +149,7 @@ def picard_fixture(dim, order, seed=7, ncase=4):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("EXAHYPE_REF", "/root/reference"))
     args = ap.parse_args()
     td = parse_testdata(os.path.join(args.ref, "ExaHyPE/exahype/tests/kernels/testdata/generic_euler_testdata.cpp"))
     for dim in ("2d", "3d"):

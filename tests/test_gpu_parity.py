@@ -338,6 +338,43 @@ def test_swe_batched_grids_vs_oracle(exa):
     assert p.status() == 0
 
 
+def test_swe_batched_grids_vs_reference_kernels(exa):
+    """Batched shallow water against the reference's OWN generic kernels (oracle/_ref, the SWE
+    app's solver: NCP g h grad b, reflective walls), grid by grid, with equal Picard sweeps."""
+    import exa_scenarios as sc
+    from pyoracle import RefKernels
+    try:
+        ref_k = RefKernels(2, 4, "swe")
+    except (FileNotFoundError, AttributeError, OSError) as e:
+        pytest.skip("reference kernels not built: %s" % e)
+    specs, states = sc.swe_batched(ngrids=4, order=4, seed=8, nmin=5, nmax=12)
+    s = exa.Solver(exa.PDE_SWE, 2, 4)
+    p = exa.Patch(s, specs)
+    p.set_solution(np.concatenate(states))
+    p.step(4)
+    got = p.get_solution()
+    t, _ = p.time()
+    off = 0
+    for g, (sp, st) in enumerate(zip(specs, states)):
+        ref = st.copy()
+        t_ref, _, _ = ref_k.run(ref, sp["ncell"], sp["size"], 4, walls=True, want_picard=True)
+        assert rel(got[off:off + ref.size], ref) < TOL, (g, rel(got[off:off + ref.size], ref))
+        assert abs(t[g] - t_ref) <= 1e-13 * t_ref
+        assert np.abs(ref - st).max() > 1e-3
+        off += ref.size
+    assert p.status() == 0
+    # Picard sweeps of the last step: the GPU's histogram equals the reference's counts, which
+    # are the loop index MaxIterations+2 for converged cells (2D return quirk) -> use the
+    # restatement's sweep counts, pinned to the reference above, for the histogram
+    o = Oracle(2, 4, pde=PDE_SWE)
+    hist = np.zeros(32, dtype=int)
+    for sp, st in zip(specs, states):
+        _, _, pic_o = o.run(st.copy(), sp["ncell"], sp["size"], 4, walls=True, want_picard=True)
+        hist += np.bincount(pic_o[-1], minlength=32)[:32]
+    assert list(hist) == p.stats()["picard_hist"]
+    assert hist[2:].sum() == hist.sum() and hist[3:].sum() > 0  # non-trivial iterations
+
+
 @pytest.mark.parametrize("nz,split", [(6, 3), (5, 2)])
 def test_two_slabs_with_halo_match_whole_grid(exa, torch, nz, split):
     """The slab-decomposition path on one GPU: two halo patches (lower and upper slab of a periodic

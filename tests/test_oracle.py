@@ -380,3 +380,91 @@ def test_elastic_order7_source_outflow_vs_ref():
     assert np.array_equal(pa + 1, pb)
     assert relerr(lb, la) < 1e-12
     assert np.abs(lb - luh0).max() > 1e-4
+
+
+# ---------------------------------------------------------------------------------------------
+# Shallow water with bathymetry (NCP path): the restatement against the reference's kernels
+# instantiated for the SWE app's solver (SWE_ADERDG/MySWESolver.cpp:43-62, 103-152). This pins
+# the gradient of the old iterate (dudx, 2d/spaceTimePredictorNonlinear.cpph:95-140), the
+# fusedSource sign S = -NCP (fusedMethods.cpph:65-80) and the Rusanov NCP split
+# (2d/riemannSolverNonlinear.cpph:37-133).
+# ---------------------------------------------------------------------------------------------
+
+def _swe_ref_or_skip(order):
+    try:
+        return RefKernels(2, order, "swe")
+    except (FileNotFoundError, AttributeError, OSError) as e:
+        pytest.skip("reference kernels not built: %s" % e)
+
+
+def swe_cells(rng, ncells, nd, vel=0.2):
+    """h = 1 + bumps, velocities U[-vel, vel], smooth-ish random bathymetry (h, hu, hv, b)."""
+    Q = np.zeros((ncells, nd, 4))
+    Q[..., 0] = 1.0 + 0.3 * rng.uniform(0, 1, (ncells, nd))
+    Q[..., 1] = Q[..., 0] * rng.uniform(-vel, vel, (ncells, nd))
+    Q[..., 2] = Q[..., 0] * rng.uniform(-vel, vel, (ncells, nd))
+    Q[..., 3] = 0.1 * rng.uniform(0, 1, (ncells, nd))
+    return Q
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_swe_predictor_vs_ref(order):
+    from pyoracle import PDE_SWE
+    ref = _swe_ref_or_skip(order)
+    o = Oracle(2, order, PDE_SWE)
+    rng = np.random.default_rng(40 + order)
+    nd = (order + 1) ** 2
+    dx = np.array([0.05, 0.04])
+    for trial in range(4):
+        luh = swe_cells(rng, 1, nd, vel=0.05 * (trial + 1)).reshape(-1)
+        dt_r, dt_o = ref.dt(luh, dx), o.dt(luh, dx)
+        assert abs(dt_r - dt_o) <= 1e-15 * dt_r
+        a = ref.predictor(luh, dx, dt_r, centre=[0.4, 0.6])
+        b = o.predictor(luh, dx, dt_r, centre=[0.4, 0.6])
+        assert a["ret"] == b["ret"]
+        for key in ("lQi", "lFi", "lQhi", "lFhi", "lQhbnd", "lFhbnd"):
+            assert relerr(b[key], a[key]) < 1e-13, (key, relerr(b[key], a[key]))
+        # the source slot of lFhi is the time-averaged -NCP: non-zero for a non-flat bottom
+        assert np.abs(a["lFhi"][2 * nd * 4:]).max() > 1e-6
+        assert relerr(o.volume(b["lFhi"], dx), ref.volume(a["lFhi"], dx)) < 1e-13
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_swe_riemann_ncp_split_vs_ref(order):
+    from pyoracle import PDE_SWE
+    ref = _swe_ref_or_skip(order)
+    o = Oracle(2, order, PDE_SWE)
+    rng = np.random.default_rng(7 + order)
+    nf = order + 1
+    dx = np.array([0.05, 0.04])
+    for d in range(2):
+        for _ in range(3):
+            QL = swe_cells(rng, 1, nf).reshape(-1)
+            QR = swe_cells(rng, 1, nf).reshape(-1)
+            FL = rng.normal(size=nf * 4)
+            FR = rng.normal(size=nf * 4)
+            ra = ref.riemann(FL, FR, QL, QR, dx, d)
+            rb = o.riemann(FL, FR, QL, QR, dx, d)
+            assert relerr(rb[0], ra[0]) < 1e-14 and relerr(rb[1], ra[1]) < 1e-14
+            # the NCP makes the two sides differ (FL = F + ncp/2, FR = F - ncp/2)
+            assert np.abs(ra[0] - ra[1]).max() > 1e-8
+
+
+@pytest.mark.parametrize("order,ncell", [(4, (5, 4)), (2, (6, 5))])
+def test_swe_wall_patch_run_vs_ref(order, ncell):
+    """Four steps of a wall-bounded grid with bumps and bathymetry (the batched-SWE state)."""
+    from exa_scenarios import swe_bumps_state
+    from pyoracle import PDE_SWE
+    ref = _swe_ref_or_skip(order)
+    o = Oracle(2, order, PDE_SWE)
+    luh0 = swe_bumps_state(ncell, order, np.random.default_rng(3))
+    la, lb = luh0.copy(), luh0.copy()
+    ta, dta, pa = ref.run(la, ncell, [1.0, 1.0], 4, walls=True, want_picard=True)
+    tb, dtb, pb = o.run(lb, ncell, [1.0, 1.0], 4, walls=True, want_picard=True)
+    assert np.max(np.abs(dta - dtb) / dta) < 1e-13
+    # the 2D reference returns MaxIterations+2 when a cell converged (2d/...:303-305), else the cap
+    n = order + 1
+    assert np.all((pa == 2 * n + 2) | ((pa == 2 * n) & (pb == 2 * n)))
+    assert pb.min() >= 2 and pb.max() <= 2 * n
+    assert relerr(lb, la) < 1e-12
+    assert np.abs(lb - luh0).max() > 1e-3  # the bumps moved
