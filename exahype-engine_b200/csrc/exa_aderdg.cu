@@ -16,8 +16,7 @@
 #include <vector>
 
 #include "../../include/exa_aderdg.h"
-#include "exa_kernels.cuh"
-#include "exa_adjoint.cuh"
+#include "exa_ops.cuh"
 #include "exa_checkpoint.h"
 
 namespace {
@@ -54,187 +53,29 @@ double default_pnpm(int order) {
 
 namespace exa {
 
-// One instantiation (PDE, DIM, N, P): launchers of every kernel.
-struct Ops {
-  int dim, order, nvar, npar, nd, nf, cpb;
-  size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
-  bool ncp;
-  virtual ~Ops() {}
-  bool mixed_ok = false;  // mixed-precision predictor instantiated
-  virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed = false) = 0;
-  // device scratch the predictor needs for a launch over ncells (outside stream capture)
-  virtual cudaError_t reserve(long long ncells) = 0;
-  virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
-  virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
-  virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
-  // discrete adjoint of one step (linear systems only)
-  bool adjoint_ok = false;
-  virtual cudaError_t adjoint(const AdjArgs& a, cudaStream_t st) = 0;
-};
-
-template <class PDE, int DIM, int N, int P>
-struct OpsImpl final : Ops {
-  using S = Shape<PDE, DIM, N, P>;
-  bool smem_set = false, smem_set_mixed = false;
-  // cells whose space-time state does not fit a CTA run the streamed predictor
-  static constexpr bool kStreamed = S::predictor_smem + 4096 > 227 * 1024;
-  // the mixed form needs PDEs without NCP and its larger shared-memory footprint must fit a CTA
-  static constexpr bool kMixed = !kStreamed && !PDE::kNCP && S::predictor_smem_mixed + 4096 <= 227 * 1024;
-  static constexpr bool kAdj = PDE::kAdjoint && !PDE::kNCP && AdjShape<PDE, DIM, N, P>::smem <= 227 * 1024;
-  // streamed predictor: scratch per device, grown on demand
-  std::mutex scratch_mu;
-  double* scratch[64] = {};
-  size_t scratch_slots[64] = {};
-  int stream_grid[64] = {};
-  cudaError_t reserve(long long ncells) override {
-    if constexpr (kStreamed) {
-      using T = StreamShape<PDE, DIM, N, P>;
-      static_assert(T::smem + 4096 <= 227 * 1024, "streamed predictor shared memory exceeds one CTA");
-      int dev = 0;
-      cudaError_t e = cudaGetDevice(&dev);
-      if (e != cudaSuccess) return e;
-      if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-      std::lock_guard<std::mutex> lk(scratch_mu);
-      if (!smem_set) {
-        e = cudaFuncSetAttribute(predictor_streamed_kernel<PDE, DIM, N, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)T::smem);
-        if (e != cudaSuccess) return e;
-        smem_set = true;
-      }
-      int sms = 0, occ = 0;
-      if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-      if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, predictor_streamed_kernel<PDE, DIM, N, P>, T::TPB,
-                                                             T::smem)) != cudaSuccess)
-        return e;
-      const long long want = std::max(1LL, std::min<long long>(ncells, (long long)sms * std::max(occ, 1)));
-      if ((size_t)want > scratch_slots[dev]) {
-        if (scratch[dev]) cudaFree(scratch[dev]);
-        scratch[dev] = nullptr;
-        scratch_slots[dev] = 0;
-        e = cudaMalloc(&scratch[dev], (size_t)want * T::slot_doubles * sizeof(double));
-        if (e != cudaSuccess) return e;
-        scratch_slots[dev] = (size_t)want;
-      }
-      stream_grid[dev] = (int)scratch_slots[dev];
-    } else {
-      (void)ncells;
-    }
-    return cudaSuccess;
-  }
-  template <bool M>
-  cudaError_t launch_predictor(const CellArgs& a, cudaStream_t st, bool& set) {
-    static_assert(!kStreamed, "cells of this size run the streamed predictor");
-    static_assert(S::predictor_smem + 4096 <= 227 * 1024, "predictor shared memory exceeds one CTA");
-    constexpr bool MM = M && kMixed;
-    const size_t smem = MM ? S::predictor_smem_mixed : S::predictor_smem;
-    if (!set) {
-      cudaError_t e = cudaFuncSetAttribute(predictor_kernel<PDE, DIM, N, P, MM>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      set = true;
-    }
-    const unsigned blocks = (unsigned)((a.ncells - a.cell_begin + S::CPB - 1) / S::CPB);
-    predictor_kernel<PDE, DIM, N, P, MM><<<blocks, S::TPB, smem, st>>>(a);
-    return cudaGetLastError();
-  }
-  bool adj_smem_set = false;
-  cudaError_t adjoint(const AdjArgs& a, cudaStream_t st) override {
-    if constexpr (kAdj) {
-      using A = AdjShape<PDE, DIM, N, P>;
-      static_assert(A::smem <= 227 * 1024, "adjoint shared memory exceeds one CTA");
-      if (a.f.nfaces > 0) {
-        adjoint_face_kernel<PDE, DIM, N, P><<<(unsigned)((a.f.nfaces + 7) / 8), 256, 0, st>>>(a);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return e;
-      }
-      if (a.c.ncells <= 0) return cudaSuccess;
-      if (!adj_smem_set) {
-        cudaError_t e = cudaFuncSetAttribute(adjoint_predictor_kernel<PDE, DIM, N, P>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)A::smem);
-        if (e != cudaSuccess) return e;
-        adj_smem_set = true;
-      }
-      adjoint_predictor_kernel<PDE, DIM, N, P><<<(unsigned)a.c.ncells, A::TPB, A::smem, st>>>(a);
-      return cudaGetLastError();
-    } else {
-      (void)a;
-      (void)st;
-      return cudaErrorNotSupported;
-    }
-  }
-  OpsImpl() {
-    adjoint_ok = kAdj;
-    mixed_ok = kMixed;
-    dim = DIM;
-    order = N;
-    nvar = S::V;
-    npar = P;
-    nd = S::nd;
-    nf = S::nf;
-    cpb = S::CPB;
-    ncp = PDE::kNCP;
-    sz_luh = (size_t)S::nd * S::D;
-    sz_lduh = (size_t)S::nd * S::V;
-    sz_qhb = S::sizeQhb;
-    sz_fhb = S::sizeFhb;
-    sz_lQi = (size_t)S::nd * S::n * S::D;
-    sz_lFi = (size_t)S::n * S::nd * (DIM + 1) * S::V;
-    sz_lQhi = (size_t)S::nd * S::D;
-    sz_lFhi = (size_t)(DIM + 1) * S::nd * S::V;
-  }
-  cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed) override {
-    if (a.ncells <= a.cell_begin) return cudaSuccess;
-    if constexpr (kStreamed) {
-      using T = StreamShape<PDE, DIM, N, P>;
-      if (mixed) return cudaErrorNotSupported;
-      int dev = 0;
-      cudaError_t e = cudaGetDevice(&dev);
-      if (e != cudaSuccess) return e;
-      if (dev < 0 || dev >= 64 || !scratch[dev]) return cudaErrorNotReady;  // reserve() first
-      CellArgs b = a;
-      b.scratch = scratch[dev];
-      const unsigned blocks = (unsigned)std::min<long long>(a.ncells - a.cell_begin, stream_grid[dev]);
-      predictor_streamed_kernel<PDE, DIM, N, P><<<blocks, T::TPB, T::smem, st>>>(b);
-      return cudaGetLastError();
-    }
-    if (mixed) {
-      if constexpr (!kMixed) {
-        return cudaErrorNotSupported;
-      } else {
-        return launch_predictor<true>(a, st, smem_set_mixed);
-      }
-    }
-    if constexpr (!kStreamed) return launch_predictor<false>(a, st, smem_set);
-    return cudaErrorNotSupported;
-  }
-  cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
-    if (a.ncells <= a.cell_begin) return cudaSuccess;
-    const unsigned blocks = (unsigned)((a.ncells - a.cell_begin + S::CPB - 1) / S::CPB);
-    if (surface && upd)
-      update_kernel<PDE, DIM, N, P, true, true><<<blocks, S::TPB, 0, st>>>(a);
-    else if (upd)
-      update_kernel<PDE, DIM, N, P, false, true><<<blocks, S::TPB, 0, st>>>(a);
-    else
-      update_kernel<PDE, DIM, N, P, false, false><<<blocks, S::TPB, 0, st>>>(a);
-    return cudaGetLastError();
-  }
-  cudaError_t riemann(const FaceArgs& f, cudaStream_t st) override {
-    if (f.nfaces <= 0) return cudaSuccess;
-    const unsigned blocks = (unsigned)((f.nfaces + 7) / 8);
-    riemann_kernel<PDE, DIM, N, P><<<blocks, 256, 0, st>>>(f);
-    return cudaGetLastError();
-  }
-  cudaError_t boundary(const FaceArgs& f, cudaStream_t st) override {
-    if (f.nfaces <= 0) return cudaSuccess;
-    const unsigned blocks = (unsigned)((f.nfaces + 7) / 8);
-    boundary_kernel<PDE, DIM, N, P><<<blocks, 256, 0, st>>>(f);
-    return cudaGetLastError();
-  }
-};
-
 // The instantiations this library carries: one function-local static launcher object each
 // (constructed on first use, never on the heap; shared by every solver handle).
+// instantiations registered by applications (exa_register_pde), ids >= EXA_PDE_USER_BASE
+struct UserOps {
+  int pde, dim, order, npar;
+  Ops* ops;
+};
+std::mutex& user_mu() {
+  static std::mutex m;
+  return m;
+}
+std::vector<UserOps>& user_ops() {
+  static std::vector<UserOps> v;
+  return v;
+}
+
 Ops* find_ops(int pde, int dim, int order, int npar) {
+  if (pde >= EXA_PDE_USER_BASE) {
+    std::lock_guard<std::mutex> lk(user_mu());
+    for (const UserOps& u : user_ops())
+      if (u.pde == pde && u.dim == dim && u.order == order && u.npar == npar) return u.ops;
+    return nullptr;
+  }
 #define EXA_CASE(PDEID, PDET, D_, N_, P_)                         \
   if (pde == PDEID && dim == D_ && order == N_ && npar == P_) {    \
     static OpsImpl<PDET, D_, N_, P_> inst;                         \
@@ -269,6 +110,7 @@ struct exa_solver {
   double* d_scratch = nullptr;
   size_t scratch_doubles = 0;
   int* d_iscratch = nullptr;
+  int pred_variant = -1;  // predictor launch variant (-1: the measured one)
 };
 
 static exa::CellArgs base_args(exa_solver* s, int ncells) {
@@ -284,6 +126,19 @@ static exa::CellArgs base_args(exa_solver* s, int ncells) {
 extern "C" {
 
 const char* exa_last_error(void) { return g_err.c_str(); }
+
+int exa_register_pde(int pde, int dim, int order, int npar, void* ops) {
+  exa::Ops* o = static_cast<exa::Ops*>(ops);
+  if (!o || pde < EXA_PDE_USER_BASE) return fail(EXA_ERR_INVALID, "user PDE ids start at EXA_PDE_USER_BASE");
+  if (o->dim != dim || o->order != order || o->npar != npar)
+    return fail(EXA_ERR_INVALID, "registration arguments do not match the instantiation");
+  std::lock_guard<std::mutex> lk(exa::user_mu());
+  for (const exa::UserOps& u : exa::user_ops())
+    if (u.pde == pde && u.dim == dim && u.order == order && u.npar == npar)
+      return fail(EXA_ERR_INVALID, "this (pde, dim, order, npar) is registered already");
+  exa::user_ops().push_back({pde, dim, order, npar, o});
+  return EXA_OK;
+}
 const char* exa_version(void) { return "exa_aderdg 0.1 (sm_100a)"; }
 
 int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
@@ -318,6 +173,18 @@ int exa_solver_destroy(exa_solver* s) {
   cudaFree(s->d_scratch);
   cudaFree(s->d_iscratch);
   delete s;
+  return EXA_OK;
+}
+
+int exa_solver_set_predictor_variant(exa_solver* s, int variant) {
+  if (!s || variant < -1 || variant > 1) return fail(EXA_ERR_INVALID, "variant must be -1, 0 or 1");
+  s->pred_variant = variant;
+  return EXA_OK;
+}
+
+int exa_solver_predictor_variant(exa_solver* s, int* variant) {
+  if (!s || !variant) return fail(EXA_ERR_INVALID, "null argument");
+  *variant = s->pred_variant >= 0 ? s->pred_variant : s->ops->tuned_variant(s->cfg.precision == EXA_PREC_MIXED);
   return EXA_OK;
 }
 
@@ -367,7 +234,7 @@ int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double*
   a.picard = picard_sweeps;
   set_uniform(a, s, dx, dt);
   EXA_CUDA(s->ops->reserve(ncells));
-  EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream, s->cfg.precision == EXA_PREC_MIXED));
+  EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream, s->cfg.precision == EXA_PREC_MIXED, s->pred_variant));
   return EXA_OK;
 }
 
@@ -501,7 +368,7 @@ int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbn
   for (int k = 0; k < s->cfg.dim; k++) dx[k] = 1.0 / invDx[k];
   set_uniform(a, s, dx, dt);
   cudaError_t e = s->ops->reserve(1);
-  if (e == cudaSuccess) e = s->ops->predictor(a, 0, s->cfg.precision == EXA_PREC_MIXED);
+  if (e == cudaSuccess) e = s->ops->predictor(a, 0, s->cfg.precision == EXA_PREC_MIXED, s->pred_variant);
   if (e != cudaSuccess) {
     cuda_fail(e, "predictor");
     return -1;
@@ -708,13 +575,19 @@ static exa::FaceArgs patch_faces(exa_patch* p) {
   f.bcell = p->bcell;
   f.bface = p->bface;
   f.btype = p->btype;
+  f.cell_grid = p->grids.size() > 1 ? p->cell_grid : nullptr;
+  f.grid_dx = p->grid_dx;
+  f.grid_geo = p->grid_geo;
+  f.grid_first = p->grid_first_d;
+  f.grid_t = p->grid_t;
+  f.grid_dt = p->grid_dt;
   return f;
 }
 
 // enqueue one step on p->stream (used for capture)
 static int patch_enqueue_step(exa_patch* p, bool cfl) {
   exa::CellArgs a = patch_args(p);
-  EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+  EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED, p->s->pred_variant));
   exa::FaceArgs f = patch_faces(p);
   EXA_CUDA(p->s->ops->riemann(f, p->stream));
   if (p->nbfaces > 0) {
@@ -776,7 +649,7 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
     for (int d = 0; d < dim; d++) {
       if (nc[d] <= 0 || !(G.size[d] > 0)) return fail(EXA_ERR_INVALID, "grid extents must be positive");
       if (G.bc[d] != EXA_BC_PERIODIC && G.bc[d] != EXA_BC_WALL && G.bc[d] != EXA_BC_HALO &&
-          G.bc[d] != EXA_BC_OUTFLOW)
+          G.bc[d] != EXA_BC_OUTFLOW && G.bc[d] != EXA_BC_USER)
         return fail(EXA_ERR_INVALID, "unknown boundary");
       if (G.bc[d] == EXA_BC_HALO && (d != dim - 1 || ngrids != 1))
         return fail(EXA_ERR_INVALID, "EXA_BC_HALO is supported on the last axis of a single-grid patch");
@@ -811,7 +684,7 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
             if (j[d] == nc[d]) {
               if (G.bc[d] == EXA_BC_PERIODIC) {
                 j[d] = 0;
-              } else if (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW) {
+              } else if (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW || G.bc[d] == EXA_BC_USER) {
                 fb.bc.push_back((int)c);
                 fb.bf.push_back((int8_t)(2 * d + 1));
                 fb.bt.push_back((int8_t)G.bc[d]);
@@ -826,7 +699,7 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
               fb.fR.push_back((int)idx(j[0], j[1], j[2]));
               fb.fd.push_back((int8_t)d);
             }
-            if (i_d == 0 && (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW)) {
+            if (i_d == 0 && (G.bc[d] == EXA_BC_WALL || G.bc[d] == EXA_BC_OUTFLOW || G.bc[d] == EXA_BC_USER)) {
               fb.bc.push_back((int)c);
               fb.bf.push_back((int8_t)(2 * d));
               fb.bt.push_back((int8_t)G.bc[d]);
@@ -875,6 +748,9 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   p->grids.assign(grids, grids + ngrids);
   FaceBuild fb;
   if (int r = build_faces(dim, ngrids, grids, fb)) return r;
+  for (int8_t t : fb.bt)
+    if (t == EXA_BC_USER && !s->ops->user_bc_ok)
+      return fail(EXA_ERR_UNSUPPORTED, "EXA_BC_USER needs a PDE functor with boundary_values");
   std::vector<int>& hcell_grid = fb.cell_grid;
   std::vector<int>& fL = fb.fL;
   std::vector<int>& fR = fb.fR;
@@ -1003,6 +879,11 @@ int exa_patch_set_solution(exa_patch* p, const double* luh, int on_device) {
   if (r) return r;
   // grid_dt now holds the CFL step of the new state: a following fixed-dt step must refill it
   p->fixed_dt = -1.0;
+  // first state on this device: time the predictor variants on it (halo patches: real cells only)
+  if (p->s->pred_variant < 0) {
+    exa::CellArgs a = patch_args(p);
+    EXA_CUDA(p->s->ops->tune(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+  }
   EXA_CUDA(cudaStreamSynchronize(p->stream));
   return EXA_OK;
 }
@@ -1102,7 +983,7 @@ int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt) {
   switch (phase) {
     case EXA_PHASE_PREDICTOR: {
       exa::CellArgs a = patch_args(p);
-      EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+      EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED, p->s->pred_variant));
       return EXA_OK;
     }
     case EXA_PHASE_FACES: {
@@ -1200,6 +1081,18 @@ int exa_patch_set_point_source(exa_patch* p, const exa_point_source* src) {
   if (p->graph_cfl) cudaGraphExecDestroy(p->graph_cfl);
   if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
   p->graph_cfl = p->graph_fixed = nullptr;
+  return EXA_OK;
+}
+
+int exa_patch_adjust_solution(exa_patch* p) {
+  if (!p) return fail(EXA_ERR_INVALID, "null patch");
+  if (!p->s->ops->adjust_ok) return fail(EXA_ERR_UNSUPPORTED, "the PDE functor has no adjust_point_solution");
+  exa::CellArgs a = patch_args(p);
+  a.luh_out = p->luh;
+  EXA_CUDA(p->s->ops->adjust(a, p->stream));
+  if (int r = patch_initial_dt(p)) return r;
+  p->fixed_dt = -1.0;
+  EXA_CUDA(cudaStreamSynchronize(p->stream));
   return EXA_OK;
 }
 
@@ -1338,7 +1231,7 @@ int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
   // Picard iterates the reverse sweeps need (written into the adjoint scratch)
   exa::CellArgs c = patch_args(p);
   c.ex_iter = p->adj_iter;
-  EXA_CUDA(o.predictor(c, p->stream, false));
+  EXA_CUDA(o.predictor(c, p->stream, false, p->s->pred_variant));
   c.ex_iter = nullptr;
   exa::AdjArgs a;
   a.c = c;
@@ -1442,7 +1335,7 @@ int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int 
       exa::CellArgs a = patch_args(p);
       a.cell_begin = (int)first(j);
       a.ncells = (int)first(j + 1);
-      EXA_CUDA(o.predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED));
+      EXA_CUDA(o.predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED, p->s->pred_variant));
     }
     exa::FaceArgs f = patch_faces(p);
     EXA_CUDA(o.riemann(f, p->stream));

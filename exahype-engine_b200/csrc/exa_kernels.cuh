@@ -21,6 +21,7 @@
 #pragma once
 #include <cstdint>
 
+#include "exa_async.cuh"
 #include "exa_pde.cuh"
 #include "exa_tables.cuh"
 
@@ -31,6 +32,7 @@ enum : unsigned {
   ST_PICARD_CAP = 2u,
   ST_NONFINITE_UPDATE = 4u,
   ST_BAD_DT = 8u,
+  ST_TIMEOUT = 16u,  // a bounded wait (bulk copy) ran out; the launch's results are not valid
 };
 
 // Shared-memory layout of the predictor's flux blocks (one block per cell, direction, variable).
@@ -109,29 +111,32 @@ struct Shape {
   // the ones the first cell's lanes already use twice
   static constexpr int FCS = DIM * V * BS + ((DIM == 2 && CPB > 1 && (DIM * V * BS) % 2 == 0) ? 1 : 0);
   static constexpr int smemF = CPB * FCS;
-  static constexpr int smemO = CPB * nd * V;                   // mixed precision: sweep-0 contraction
+  static constexpr int smemStage = CPB * nd * D;               // bulk-copy target of the next cells' luh
+  static constexpr int even(int x) { return (x + 1) / 2 * 2; }  // 16-byte boundary in doubles
   // predictor shared memory for a given per-node stride dq of the iterate slices and the luh
-  // block, without / with the mixed-precision buffer
-  static constexpr size_t smem_for(int dq, bool mixed) {
-    return sizeof(double) * (size_t)(CPB * n * nd * dq + smemF + CPB * nd * dq + (mixed ? smemO : 0));
+  // block; the staging buffer of the persistent form comes last
+  static constexpr size_t smem_for(int dq) {
+    return sizeof(double) * (size_t)(even(CPB * n * nd * dq + smemF + CPB * nd * dq) + smemStage);
   }
   // resident CTAs per SM: two when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
-  static constexpr int blocks_for(int dq) { return 2 * (smem_for(dq, true) + 3 * 1024) <= 228 * 1024 ? 2 : 1; }
+  static constexpr int blocks_for(int dq) { return 2 * (smem_for(dq) + 3 * 1024) <= 228 * 1024 ? 2 : 1; }
   static constexpr bool fits_cta(size_t bytes) { return bytes + 4096 <= 227 * 1024; }
   // per-node stride of the iterate slices and the luh block in shared memory: D rounded up to an
   // odd count (an even stride puts several lanes of a warp on one bank), unless the padding
   // would cost a resident CTA or push a form of the kernel past one CTA's shared memory
   static constexpr bool pad_ok = D % 2 == 0 && blocks_for(D | 1) >= blocks_for(D) &&
-                                 fits_cta(smem_for(D | 1, false)) >= fits_cta(smem_for(D, false)) &&
-                                 fits_cta(smem_for(D | 1, true)) >= fits_cta(smem_for(D, true));
+                                 fits_cta(smem_for(D | 1)) >= fits_cta(smem_for(D));
   static constexpr int DQ = pad_ok ? (D | 1) : D;
   // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][DQ] + flux/partials
   static constexpr int smemQ = CPB * n * nd * DQ;
   static constexpr int items = CPB * DIM * V * NL;             // line contractions per time node
   static constexpr int rounds = (items + TPB - 1) / TPB;       // per thread
   static constexpr int smemU = CPB * nd * DQ;                  // luh of the CTA's cells
+  // offset of the luh staging buffer (doubles, even: 16-byte aligned for the bulk copy)
+  static constexpr int stage_off() { return even(smemQ + smemF + smemU); }
+  // dynamic shared memory of the one-group-per-CTA form (no staging buffer) and the persistent one
   static constexpr size_t predictor_smem = sizeof(double) * (smemQ + smemF + smemU);
-  static constexpr size_t predictor_smem_mixed = sizeof(double) * (smemQ + smemF + smemU + smemO);
+  static constexpr size_t predictor_smem_persist = sizeof(double) * (stage_off() + smemStage);
   static constexpr int MinBlocks = blocks_for(DQ);
   // registers are split over the SM's four 16K-register partitions: B blocks of W warps need
   // ceil(B*W/4) warps' worth of registers in one partition
@@ -175,6 +180,9 @@ struct CellArgs {
   double* ex_lFi;
   double* ex_lQhi;
   double* ex_lFhi;
+  // the predictor may fetch luh with 16-byte bulk copies (luh 16-byte aligned and nd*D even;
+  // set by the launcher)
+  int bulk_luh;
 };
 
 struct FaceArgs {
@@ -187,7 +195,17 @@ struct FaceArgs {
   // boundary faces
   const int* bcell;         // cell owning the boundary face
   const int8_t* bface;      // face index 2*dir + orientation
-  const int8_t* btype;      // boundary type (EXA_BC_WALL, EXA_BC_OUTFLOW)
+  const int8_t* btype;      // boundary type (EXA_BC_WALL, EXA_BC_OUTFLOW, EXA_BC_USER)
+  // geometry and time of the boundary faces' cells (EXA_BC_USER: the functor's boundary_values
+  // is evaluated at the face nodes' coordinates); nullable grid arrays as in CellArgs
+  const int* cell_grid;
+  const double* grid_dx;
+  const double* grid_geo;
+  const long long* grid_first;
+  const double* grid_t;
+  const double* grid_dt;
+  double u_dx[3];
+  double u_t, u_dt;
 };
 
 // ------------------------------------------------------------------------------------------
@@ -268,6 +286,7 @@ __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
 }  // namespace exa
 
 #include "exa_predictor.cuh"
+#include "exa_predictor_mixed.cuh"
 #include "exa_predictor_streamed.cuh"
 
 namespace exa {
@@ -287,9 +306,13 @@ __device__ __forceinline__ void ghost_state(const double* qin, int normal, doubl
   }
 }
 
-template <class PDE, int DIM, int N, int P>
+// Rusanov flux of one face (riemannSolverNonlinear :37-128), in place on FL / FR. ghostL / ghostR:
+// that side is the outside of a domain face; ghost(fn, qin, fin, qout, fout) then supplies the outer
+// state (D values) and its normal flux (V values) at face node fn from the inner ones, as the
+// reference's boundaryConditions + boundaryValues do (3d/boundaryConditions.cpph:29-122).
+template <class PDE, int DIM, int N, int P, class Ghost>
 __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR, double* FL, double* FR, int d,
-                                             int lane, bool ghostL, bool ghostR, int ghost_normal) {
+                                             int lane, bool ghostL, bool ghostR, Ghost ghost) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nf = S::nf;
@@ -305,14 +328,10 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
       ql[m] = QL[fn * D + m];
       qr[m] = QR[fn * D + m];
     }
-    if (ghostL) ghost_state<PDE, DIM, D>(qr, ghost_normal, ql);
-    if (ghostR) ghost_state<PDE, DIM, D>(ql, ghost_normal, qr);
     if (ghostL || ghostR) {
-#pragma unroll
-      for (int m = V; m < D; m++) {
-        ql[m] = ghostL ? qr[m] : ql[m];
-        qr[m] = ghostR ? ql[m] : qr[m];
-      }
+      double fg[V];
+      if (ghostL) ghost(fn, qr, FR + fn * V, ql, fg);
+      if (ghostR) ghost(fn, ql, FL + fn * V, qr, fg);
     }
 #pragma unroll
     for (int m = 0; m < D; m++) {
@@ -345,25 +364,14 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
       ql[m] = QL[fn * D + m];
       qr[m] = QR[fn * D + m];
     }
-    if (ghostL) ghost_state<PDE, DIM, D>(qr, ghost_normal, ql);
-    if (ghostR) ghost_state<PDE, DIM, D>(ql, ghost_normal, qr);
     if (ghostL || ghostR) {
-#pragma unroll
-      for (int m = V; m < D; m++) {
-        ql[m] = ghostL ? qr[m] : ql[m];
-        qr[m] = ghostR ? ql[m] : qr[m];
-      }
-      // boundaryValues returns the flux of the ghost state in the normal direction
-      double Fg[DIM * V];
-      PDE::template flux<DIM>(ghostL ? ql : qr, Fg);
+      double fg[V];
+      if (ghostL) ghost(fn, qr, FR + fn * V, ql, fg);
+      if (ghostR) ghost(fn, ql, FL + fn * V, qr, fg);
 #pragma unroll
       for (int m = 0; m < V; m++) {
-        double fg = Fg[m];
-#pragma unroll
-        for (int k = 1; k < DIM; k++)
-          if (k == d) fg = Fg[k * V + m];
-        fl[m] = ghostL ? fg : FL[fn * V + m];
-        fr[m] = ghostR ? fg : FR[fn * V + m];
+        fl[m] = ghostL ? fg[m] : FL[fn * V + m];
+        fr[m] = ghostR ? fg[m] : FR[fn * V + m];
       }
     } else {
 #pragma unroll
@@ -397,6 +405,60 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
   }
 }
 
+// the built-in domain faces: a reflective wall (the functor's wall, its normal flux) or outflow
+// (normal < 0: the inner state itself); material parameters are copied from the inside
+template <class PDE, int DIM, int N, int P>
+struct BuiltinGhost {
+  int normal, d;
+  __device__ __forceinline__ void operator()(int, const double* qin, const double*, double* qout, double* fout) const {
+    constexpr int V = PDE::V, D = Shape<PDE, DIM, N, P>::D;
+    ghost_state<PDE, DIM, D>(qin, normal, qout);
+#pragma unroll
+    for (int m = V; m < D; m++) qout[m] = qin[m];
+    double Fg[DIM * V];
+    PDE::template flux<DIM>(qout, Fg);
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      double f = Fg[m];
+#pragma unroll
+      for (int k = 1; k < DIM; k++)
+        if (k == d) f = Fg[k * V + m];
+      fout[m] = f;
+    }
+  }
+};
+
+// EXA_BC_USER faces: the functor's boundary_values at the face node's position x (the reference's
+// node coordinates, 3d/boundaryConditions.cpph:79-103: the normal coordinate on the face, the
+// tangential ones at the Gauss-Legendre nodes of the cell)
+template <class PDE, int DIM, int N, int P>
+struct UserGhost {
+  double centre[3], dx[3], t, dt;
+  int face, d;
+  __device__ __forceinline__ void operator()(int fn, const double* qin, const double* fin, double* qout,
+                                             double* fout) const {
+    if constexpr (has_boundary_values<PDE, DIM>::value) {
+      using G = GL<N>;
+      constexpr int n = N + 1, D = Shape<PDE, DIM, N, P>::D;
+      double x[3] = {centre[0], centre[1], centre[2]};
+      x[d] = centre[d] + (-0.5 + (face & 1)) * dx[d];
+      // tangential axes, slower first: (z, y) for x faces, (z, x) for y faces, (y, x) for z faces
+      const int d1 = d == 0 ? 1 : 0, d2 = DIM == 3 ? (d == 2 ? 1 : 2) : -1;
+      if (DIM == 3) {
+        x[d2] = centre[d2] + dx[d2] * (G::nodes(fn / n) - 0.5);
+        x[d1] = centre[d1] + dx[d1] * (G::nodes(fn % n) - 0.5);
+      } else {
+        x[d1] = centre[d1] + dx[d1] * (G::nodes(fn) - 0.5);
+      }
+#pragma unroll
+      for (int m = 0; m < D; m++) qout[m] = qin[m];
+      PDE::template boundary_values<DIM>(x, t, dt, face, d, fin, qin, fout, qout);
+    } else {
+      (void)fn, (void)qin, (void)fin, (void)qout, (void)fout;
+    }
+  }
+};
+
 template <class PDE, int DIM, int N, int P>
 __global__ void __launch_bounds__(256) riemann_kernel(FaceArgs f) {
   using S = Shape<PDE, DIM, N, P>;
@@ -409,7 +471,7 @@ __global__ void __launch_bounds__(256) riemann_kernel(FaceArgs f) {
   const double* QR = f.lQhbnd + cr * S::sizeQhb + (2 * d) * S::nf * S::D;
   double* FL = f.lFhbnd + cl * S::sizeFhb + (2 * d + 1) * S::nf * S::V;
   double* FR = f.lFhbnd + cr * S::sizeFhb + (2 * d) * S::nf * S::V;
-  rusanov_face<PDE, DIM, N, P>(QL, QR, FL, FR, d, lane, false, false, d);
+  rusanov_face<PDE, DIM, N, P>(QL, QR, FL, FR, d, lane, false, false, BuiltinGhost<PDE, DIM, N, P>{d, d});
 }
 
 // Domain-boundary faces with a reflective wall: the ghost state is the mirrored inner state,
@@ -426,11 +488,66 @@ __global__ void __launch_bounds__(256) boundary_kernel(FaceArgs f) {
   const double* Q = f.lQhbnd + c * S::sizeQhb + face * S::nf * S::D;
   double* F = f.lFhbnd + c * S::sizeFhb + face * S::nf * S::V;
   // orientation 0: the cell is on the right of the face (ghost left); 1: ghost right
-  const bool outflow = f.btype && f.btype[warp] == 3;  // EXA_BC_OUTFLOW: ghost = inner state
+  const int type = f.btype ? f.btype[warp] : 1;
+  if (has_boundary_values<PDE, DIM>::value && type == 4) {  // EXA_BC_USER
+    UserGhost<PDE, DIM, N, P> gh;
+    const int g = f.cell_grid ? f.cell_grid[c] : 0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) gh.dx[k] = k < DIM ? (f.grid_dx ? f.grid_dx[g * 3 + k] : f.u_dx[k]) : 1.0;
+    const double* Gg = f.grid_geo + 6 * g;
+    const long long loc = c - (f.grid_first ? f.grid_first[g] : 0);
+    const long long nx = (long long)Gg[3], ny = (long long)Gg[4];
+    const long long ix = loc % nx, iy = (loc / nx) % ny, iz = loc / (nx * ny);
+    gh.centre[0] = Gg[0] + (ix + 0.5) * gh.dx[0];
+    gh.centre[1] = Gg[1] + (iy + 0.5) * gh.dx[1];
+    gh.centre[2] = Gg[2] + (iz + 0.5) * gh.dx[2];
+    gh.t = f.grid_t ? f.grid_t[g] : f.u_t;
+    gh.dt = f.grid_dt ? f.grid_dt[g] : f.u_dt;
+    gh.face = face;
+    gh.d = d;
+    if (o == 0)
+      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh);
+    else
+      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh);
+    return;
+  }
+  // EXA_BC_OUTFLOW (3): ghost = inner state; otherwise the functor's reflective wall
+  const BuiltinGhost<PDE, DIM, N, P> gh{type == 3 ? -1 : d, d};
   if (o == 0)
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, outflow ? -1 : d);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh);
   else
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, outflow ? -1 : d);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh);
+}
+
+// adjustPointSolution at every node (3d/solutionAdjustment.cpph:17-58): x = cell centre +
+// dx (node - 0.5) per axis, the grid's time t and step dt; in place on luh_out
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) adjust_kernel(CellArgs a) {
+  if constexpr (has_adjust_point_solution<PDE, DIM>::value) {
+    using S = Shape<PDE, DIM, N, P>;
+    using G = GL<N>;
+    constexpr int n = S::n, nd = S::nd, D = S::D;
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (long long)a.ncells * nd) return;
+    const long long cell = k / nd;
+    const int p = (int)(k % nd);
+    const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+    double dx[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) dx[d] = d < DIM ? (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 1.0;
+    double c[3];
+    cell_centre(a, cell, g, dx, c);
+    int co[3];
+    node_coords<DIM, n>(p, co);
+    double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) x[d] = c[d] + dx[d] * (G::nodes(co[d]) - 0.5);
+    const double t = a.grid_t ? a.grid_t[g] : a.u_t;
+    const double dt = a.grid_dt ? a.grid_dt[g] : a.u_dt;
+    PDE::template adjust_point_solution<DIM>(x, t, dt, a.luh_out + (size_t)k * D);
+  } else {
+    (void)a;
+  }
 }
 
 // ------------------------------------------------------------------------------------------

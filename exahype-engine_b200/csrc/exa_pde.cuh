@@ -13,11 +13,35 @@
 //   flux_vjp<DIM>(Q, lF, lQ)         lQ[k] += sum_{d,m} lF[d*V + m] dF_d[m]/dQ[k], k < V + P
 //   max_speed_grad<DIM>(Q, d, g)     returns max_m |lambda_m(Q)| and sets g[k] = its dQ[k] gradient
 //
+// Optional hooks (detected at compile time; functors without them keep the built-in behaviour):
+//   adjust_point_solution<DIM>(x, t, dt, Q)      adjustPointSolution: sets / modifies the D values
+//                                                of the node at position x (initial conditions)
+//   boundary_values<DIM>(x, t, dt, faceIndex, normal, Fin, Qin, Fout, Qout)
+//                                                boundaryValues for faces of type EXA_BC_USER:
+//                                                Qout (D values, pre-filled with Qin) and Fout (V,
+//                                                the normal flux of the outer state) at face node x
+//
 // The bodies restate the reference applications' formulas in the same operation order so that
 // the FP64 path agrees with the reference to rounding.
 #pragma once
+#include <type_traits>
 
 namespace exa {
+
+template <class PDE, int DIM, class = void>
+struct has_adjust_point_solution : std::false_type {};
+template <class PDE, int DIM>
+struct has_adjust_point_solution<PDE, DIM,
+                                 std::void_t<decltype(PDE::template adjust_point_solution<DIM>(
+                                     (const double*)nullptr, 0.0, 0.0, (double*)nullptr))>> : std::true_type {};
+
+template <class PDE, int DIM, class = void>
+struct has_boundary_values : std::false_type {};
+template <class PDE, int DIM>
+struct has_boundary_values<PDE, DIM,
+                           std::void_t<decltype(PDE::template boundary_values<DIM>(
+                               (const double*)nullptr, 0.0, 0.0, 0, 0, (const double*)nullptr, (const double*)nullptr,
+                               (double*)nullptr, (double*)nullptr))>> : std::true_type {};
 
 // correctly rounded reciprocal: the same value as 1 / x (IEEE round to nearest), fewer instructions
 __device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }

@@ -23,7 +23,7 @@ EXA_OK = 0
 PDE_EULER, PDE_SWE, PDE_ACOUSTIC, PDE_ELASTIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 BC_PERIODIC, BC_WALL = 0, 1
-ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT = 1, 2, 4, 8
+ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT, ST_TIMEOUT = 1, 2, 4, 8, 16
 NVAR = {PDE_EULER: 5, PDE_SWE: 4, PDE_ACOUSTIC: 4, PDE_ELASTIC: 9}
 NPAR = {PDE_EULER: 0, PDE_SWE: 0, PDE_ACOUSTIC: 2, PDE_ELASTIC: 3}
 
@@ -95,6 +95,8 @@ def load_library(path=None):
         "exa_solver_create": [ctypes.POINTER(_Config), ctypes.POINTER(vp)],
         "exa_solver_destroy": [vp],
         "exa_solver_sizes": [vp, ctypes.POINTER(_Sizes)],
+        "exa_solver_set_predictor_variant": [vp, i],
+        "exa_solver_predictor_variant": [vp, ctypes.POINTER(i)],
         "exa_solver_status": [vp, ctypes.POINTER(ctypes.c_uint)],
         "exa_fused_predictor_volume_integral": [vp, i, vp, vp, vp, vp, vp, dp, d, d, vp],
         "exa_riemann_solver_nonlinear": [vp, i, vp, vp, vp, vp, vp, vp],
@@ -213,6 +215,18 @@ class Solver:
         bits = ctypes.c_uint(0)
         _check(self.lib.exa_solver_status(self.h, ctypes.byref(bits)), "exa_solver_status")
         return bits.value
+
+    @property
+    def predictor_variant(self):
+        """0: one cell group per CTA, 1: persistent CTAs with a prefetched next group."""
+        v = ctypes.c_int(0)
+        _check(self.lib.exa_solver_predictor_variant(self.h, ctypes.byref(v)), "exa_solver_predictor_variant")
+        return v.value
+
+    @predictor_variant.setter
+    def predictor_variant(self, v):
+        """-1 selects the variant measured as faster on this device."""
+        _check(self.lib.exa_solver_set_predictor_variant(self.h, int(v)), "exa_solver_set_predictor_variant")
 
     # ---- batched, device tensors -------------------------------------------------------
     def fused_predictor_volume_integral(self, luh, lduh, lQhbnd, lFhbnd, dx, dt, t=0.0, picard=None, stream=None):

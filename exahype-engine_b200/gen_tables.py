@@ -109,9 +109,10 @@ def main():
         for k in ("Kxi", "iK1", "dudx"):
             rows = ["{%s}" % ", ".join(fmt(v) for v in r) for r in t[k]]
             out.append("static __constant__ double c_%s_%d[%d][%d] = {%s};" % (k, o, n, n, ", ".join(rows)))
-        rows = ["{%s}" % ", ".join(fmt(v) + "f" if "e" in fmt(v) or "." in fmt(v) else fmt(v) for v in
-                              (float(x) for x in r)) for r in t["Kxi"]]
-        out.append("static __constant__ float c_Kxif_%d[%d][%d] = {%s};" % (o, n, n, ", ".join(rows)))
+        for k in ("Kxi", "iK1"):
+            rows = ["{%s}" % ", ".join(fmt(v) + "f" if "e" in fmt(v) or "." in fmt(v) else fmt(v) for v in
+                                  (float(x) for x in r)) for r in t[k]]
+            out.append("static __constant__ float c_%sf_%d[%d][%d] = {%s};" % (k, o, n, n, ", ".join(rows)))
         out.append("template <> struct GL<%d> {" % o)
         out.append("  static constexpr int n = %d;" % n)
         for k in ("nodes", "weights", "F0", "F1"):
@@ -119,6 +120,7 @@ def main():
         for k in ("Kxi", "iK1", "dudx"):
             out.append("  static __device__ __forceinline__ double %s(int i, int j) { return c_%s_%d[i][j]; }" % (k, k, o))
         out.append("  static __device__ __forceinline__ float Kxif(int i, int j) { return c_Kxif_%d[i][j]; }" % o)
+        out.append("  static __device__ __forceinline__ float iK1f(int i, int j) { return c_iK1f_%d[i][j]; }" % o)
         out.append("};")
     out.append("}  // namespace exa")
     path = os.path.join(HERE, "csrc", "exa_tables.cuh")

@@ -44,7 +44,8 @@ typedef enum {
   EXA_ST_NONFINITE_PREDICTOR = 1,
   EXA_ST_PICARD_CAP = 2,      /* some cell used all 2(N+1) Picard sweeps without converging */
   EXA_ST_NONFINITE_UPDATE = 4,
-  EXA_ST_BAD_DT = 8
+  EXA_ST_BAD_DT = 8,
+  EXA_ST_TIMEOUT = 16         /* a bounded device-side wait ran out; the launch's results are not valid */
 } exa_status_bits;
 
 /* PDE systems compiled as device functors (the user hooks flux / eigenvalues /
@@ -56,6 +57,17 @@ typedef enum {
   EXA_PDE_ELASTIC = 3   /* linear elasticity v,sigma (V=9) with per-node rho,cp,cs (nPar=3), flux form; new */
 } exa_pde;
 
+/* Application PDE systems: ids from EXA_PDE_USER_BASE up. An application compiles its functor into
+ * its own shared library with include/exa_aderdg_user.cuh (EXA_REGISTER_PDE); loading that library
+ * registers every (dim, order, npar) it instantiates, after which exa_solver_create accepts the id
+ * like a built-in one. Replaces the toolkit-generated Abstract<App>Solver_ADERDG binding of the
+ * user's solver class (AbstractGenericADERDGSolverHeader.template:34-68, 220-338). */
+#define EXA_PDE_USER_BASE 64
+/* called by EXA_REGISTER_PDE at load time: ops is the instantiation's launcher object (an
+ * exa::Ops*, see exahype-engine_b200/csrc/exa_ops.cuh). Ids below EXA_PDE_USER_BASE, a mismatch
+ * between the arguments and the object, or a second registration of the same key are refused. */
+int exa_register_pde(int pde, int dim, int order, int npar, void* ops);
+
 typedef enum {
   EXA_PREC_FP64 = 0,  /* every sweep in FP64 (generic-kernel semantics, parity 1e-12) */
   EXA_PREC_MIXED = 1  /* early Picard sweeps in FP32, final sweep + residual test + update in FP64 */
@@ -66,7 +78,10 @@ typedef enum {
  * exa_patch_halo_pack / exa_patch_halo_unpack). */
 /* EXA_BC_OUTFLOW: the ghost state is the inner state (boundaryValues copying stateIn), which
  * lets waves leave the domain (the absorbing boundary of the elastic configuration). */
-typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1, EXA_BC_HALO = 2, EXA_BC_OUTFLOW = 3 } exa_bc;
+/* EXA_BC_USER: the PDE functor's boundary_values hook gives the outer state and its normal flux
+ * at every face node (the user's boundaryValues, 3d/boundaryConditions.cpph:29-122); only for
+ * functors that define it (include/exa_aderdg_user.cuh). */
+typedef enum { EXA_BC_PERIODIC = 0, EXA_BC_WALL = 1, EXA_BC_HALO = 2, EXA_BC_OUTFLOW = 3, EXA_BC_USER = 4 } exa_bc;
 
 /* Compile-time constants of the reference's generated solver (AbstractGenericADERDGSolverHeader
  * .template:34-68), here runtime fields of a solver handle. */
@@ -102,6 +117,14 @@ int exa_solver_destroy(exa_solver* s);
 int exa_solver_sizes(const exa_solver* s, exa_sizes* out);
 /* reads and clears the device status word (synchronises the device) */
 int exa_solver_status(exa_solver* s, unsigned* bits);
+/* Launch form of the predictor (no reference counterpart: a tuning knob of this implementation).
+ * 0: one group of cells per CTA; 1: persistent CTAs, each fetching its next group's luh by bulk
+ * copy while it computes the current one; -1 (the default): the form measured as faster for this
+ * instantiation on this device. The measurement runs once per (instantiation, precision, device),
+ * in the first exa_patch_set_solution, on (up to 65,536 cells of) the state it was given. */
+int exa_solver_set_predictor_variant(exa_solver* s, int variant);
+/* the form the solver's next predictor launch uses on the current device */
+int exa_solver_predictor_variant(exa_solver* s, int* variant);
 
 /* ---- batched kernels on caller-owned device memory ------------------------------------
  * `dx` is the cell size (DIM doubles, host memory) shared by all `ncells` cells; `dt` a host
@@ -257,6 +280,12 @@ typedef struct {
   int variable;
 } exa_point_source;
 int exa_patch_set_point_source(exa_patch* p, const exa_point_source* src);
+
+/* adjustPointSolution (3d/solutionAdjustment.cpph:17-58) on the device: the functor's
+ * adjust_point_solution hook at every node x of every cell (x = cell centre + dx (node - 0.5)),
+ * with each grid's current time and step, in place; then every grid's CFL step is recomputed.
+ * EXA_ERR_UNSUPPORTED for functors without the hook. Synchronises the patch stream. */
+int exa_patch_adjust_solution(exa_patch* p);
 
 /* ---- one step in phases, for subdomains that exchange face traces ---------------------------
  * The reference exchanges the face data of cells next to a remote rank by MPI

@@ -286,11 +286,14 @@ def test_patch_many_grids_independent(exa):
         off += ref.size
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("dim,order,ncell,steps", [(3, 5, (4, 3, 3), 3), (2, 3, (27, 27), 10)])
-def test_mixed_precision_patch_vs_fp64_oracle(exa, dim, order, ncell, steps):
-    """Mixed mode: FP32 contractions of the flux corrections F(q) - F(luh) inside FP64 sweeps.
-    The iterate, the residual test, the time solve, the update and the CFL stay FP64, so the state
-    stays within 1e-9 (relative) of the FP64 oracle and the Picard counts are unchanged."""
+def test_mixed_precision_patch_vs_fp64_oracle(exa, dim, order, ncell, steps, variant):
+    """Mixed mode: the sweeps after sweep 0 as FP32 corrections to sweep 0's FP64 closed form
+    (FP32 flux corrections F(luh + dq) - F(luh), contractions and time solve), with the iterate
+    update, the residual test, the time averages, the faces, the volume integral, the update and the
+    CFL in FP64. The state stays within 1e-9 (relative) of the FP64 oracle and the Picard counts
+    are unchanged; both launch forms (2 and 3 CTAs per SM) agree."""
     import exa_scenarios as sc
     if dim == 2:
         luh0, _ = sc.euler_entropy_wave(ncell, order, seed=0)
@@ -301,14 +304,75 @@ def test_mixed_precision_patch_vs_fp64_oracle(exa, dim, order, ncell, steps):
     ref = luh0.copy()
     t_ref, _, pic = Oracle(dim, order).run(ref, ncell, size, steps, want_picard=True)
     s = exa.Solver(exa.PDE_EULER, dim, order, precision=exa.PREC_MIXED)
+    s.predictor_variant = variant
     p = exa.Patch(s, [dict(ncell=ncell, size=size)])
     p.set_solution(luh0)
     p.step(steps)
     got = p.get_solution()
+    assert s.predictor_variant == variant
     assert rel(got, ref) < 1e-9
     assert abs(p.time()[0][0] - t_ref) <= 1e-9 * t_ref
     assert p.stats()["picard_mean"] == pytest.approx(pic[-1].mean())
     assert p.status() == 0
+
+
+@pytest.mark.parametrize("name,order,var", [("acoustic", 4, 0), ("elastic", 3, 3)])
+def test_mixed_precision_linear_waves_source_vs_fp64_oracle(exa, name, order, var):
+    """The mixed form on the linear systems with the point source (the source enters sweep 0's
+    closed form) and outflow faces, both launch forms."""
+    import exa_scenarios as sc
+    from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC
+    pde = {"acoustic": PDE_ACOUSTIC, "elastic": PDE_ELASTIC}[name]
+    ncell, size = (5, 4, 6), [1.0, 0.8, 1.2]
+    src = sc.ricker_source(3, size, f0=4.0, variable=var, width=0.1)
+    src = src[:4] + (0.05,) + src[5:]
+    rng = np.random.default_rng(6)
+    luh0 = sc.layered_medium(name, ncell, size, order, seed=2)
+    D = exa.NVAR[pde] + exa.NPAR[pde]
+    lv = luh0.reshape(-1, D)
+    lv[:, :exa.NVAR[pde]] += 0.01 * rng.normal(size=(lv.shape[0], exa.NVAR[pde]))  # every cell iterates
+    o = Oracle(3, order, pde, source=src)
+    ref = luh0.copy()
+    t_ref, _, pic = o.run(ref, ncell, size, 3, walls=3, want_picard=True)
+    for variant in (0, 1):
+        s = exa.Solver(pde, 3, order, npar=exa.NPAR[pde], precision=exa.PREC_MIXED)
+        s.predictor_variant = variant
+        p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=3)])
+        p.set_point_source(src[:3], src[3], src[4], src[5], src[6], int(src[7]))
+        p.set_solution(luh0)
+        p.step(3)
+        got = p.get_solution()
+        assert rel(got, ref) < 1e-9, (variant, rel(got, ref))
+        assert abs(p.time()[0][0] - t_ref) <= 1e-9 * t_ref
+        assert p.stats()["picard_mean"] == pytest.approx(pic[-1].mean())
+        assert pic[-1].mean() > 1.5
+        assert p.status() == 0
+        p.close()
+
+
+@pytest.mark.parametrize("dim,order,ncell", [(3, 5, (5, 4, 3)), (2, 3, (9, 7)), (3, 3, (6, 5, 4))])
+def test_fp64_predictor_launch_forms_agree(exa, dim, order, ncell):
+    """The FP64 predictor's two launch forms (one cell group per CTA; persistent CTAs with a
+    bulk-copy prefetch of the next group) give bit-identical steps, equal to the oracle; the
+    measured default is one of them."""
+    rng = np.random.default_rng(21)
+    luh0 = euler_cells(rng, int(np.prod(ncell)), (order + 1) ** dim, amp=0.04, dim=dim).reshape(-1)
+    size = [1.0] * dim
+    ref = luh0.copy()
+    Oracle(dim, order).run(ref, ncell, size, 2)
+    outs = []
+    for variant in (0, 1, -1):
+        s = exa.Solver(exa.PDE_EULER, dim, order)
+        s.predictor_variant = variant
+        p = exa.Patch(s, [dict(ncell=ncell, size=size)])
+        p.set_solution(luh0)
+        p.step(2)
+        outs.append(p.get_solution())
+        assert p.status() == 0
+        assert s.predictor_variant in (0, 1)
+        p.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    assert rel(outs[0], ref) < TOL
 
 
 def test_mixed_precision_rejected_for_ncp(exa):
