@@ -30,12 +30,33 @@ def sources():
                   [os.path.join(REPO, "include", "exa_aderdg.h")])
 
 
+def build_user_pde(src, out, force=False, verbose=False):
+    """Compile an application's PDE functor (a .cu file using include/exa_aderdg_user.cuh) into a
+    shared library linked against libexa_aderdg.so (built first); loading it registers the
+    functor's instantiations with the library."""
+    lib = build(verbose=verbose)
+    deps = [src] + sources() + [os.path.join(REPO, "include", "exa_aderdg_user.cuh")]
+    if not force and os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(s) for s in deps):
+        return out
+    cmd = [_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + \
+        ["-I", os.path.join(REPO, "include"), "-o", out + ".tmp", src, "-L", HERE, "-lexa_aderdg",
+         "-Xlinker", "-rpath=$ORIGIN/" + os.path.relpath(HERE, os.path.dirname(os.path.abspath(out)))]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed on %s" % src)
+    os.replace(out + ".tmp", out)
+    assert os.path.exists(lib)
+    return out
+
+
 def build(force=False, verbose=False):
     srcs = sources()
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(s) for s in srcs):
         return LIB
+    # the soname lets an application's PDE library (build_user_pde) bind to the copy already loaded
     cmd = [_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + \
-        ["-o", LIB + ".tmp", os.path.join(HERE, "csrc", "exa_aderdg.cu")]
+        ["-Xlinker", "-soname=libexa_aderdg.so", "-o", LIB + ".tmp", os.path.join(HERE, "csrc", "exa_aderdg.cu")]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)

@@ -127,6 +127,10 @@ extern "C" {
 
 const char* exa_last_error(void) { return g_err.c_str(); }
 
+int exa_pde_available(int pde, int dim, int order, int npar) {
+  return exa::find_ops(pde, dim, order, npar) != nullptr ? 1 : 0;
+}
+
 int exa_register_pde(int pde, int dim, int order, int npar, void* ops) {
   exa::Ops* o = static_cast<exa::Ops*>(ops);
   if (!o || pde < EXA_PDE_USER_BASE) return fail(EXA_ERR_INVALID, "user PDE ids start at EXA_PDE_USER_BASE");

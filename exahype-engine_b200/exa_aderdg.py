@@ -57,7 +57,8 @@ class FaceLists(ctypes.Structure):
 
 
 PHASE_PREDICTOR, PHASE_FACES, PHASE_UPDATE, PHASE_ADVANCE = 0, 1, 2, 3
-BC_HALO, BC_OUTFLOW = 2, 3
+BC_HALO, BC_OUTFLOW, BC_USER = 2, 3, 4
+PDE_USER_BASE = 64
 
 
 class PointSource(ctypes.Structure):
@@ -128,6 +129,9 @@ def load_library(path=None):
         "exa_patch_step_host": [vp, vp, vp, d],
         "exa_patch_run_host": [vp, vp, vp, i, d],
         "exa_patch_adjoint_step": [vp, vp, d],
+        "exa_patch_adjust_solution": [vp],
+        "exa_register_pde": [i, i, i, i, vp],
+        "exa_pde_available": [i, i, i, i],
         "exa_checkpoint_schedule": [i, i, ctypes.POINTER(CkAction), i, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong)],
     }
@@ -145,6 +149,19 @@ def load_library(path=None):
     lib.exa_patch_halo_doubles.restype = ctypes.c_longlong
     _lib = lib
     return lib
+
+
+def load_user_pde(path):
+    """Load an application's PDE library (compiled with include/exa_aderdg_user.cuh, e.g. by
+    build.build_user_pde); loading it registers its instantiations with libexa_aderdg.so."""
+    load_library()
+    if not os.path.exists(path):
+        raise ExaError("%s is missing" % path)
+    return ctypes.CDLL(path)
+
+
+def pde_available(pde, dim, order, npar=0):
+    return bool(load_library().exa_pde_available(int(pde), int(dim), int(order), int(npar)))
 
 
 def _check(rc, what):
@@ -379,6 +396,10 @@ class Patch:
 
     def dt_next_copy(self, buf, to_patch):
         _check(self.lib.exa_patch_dt_next_copy(self.h, _ptr(buf), int(to_patch)), "exa_patch_dt_next_copy")
+
+    def adjust_solution(self):
+        """The functor's adjust_point_solution at every node (device initial conditions)."""
+        _check(self.lib.exa_patch_adjust_solution(self.h), "exa_patch_adjust_solution")
 
     def set_point_source(self, x, f0=0.0, t0=0.0, amplitude=0.0, width=1.0, variable=0):
         """Ricker point source on `variable` (acoustic / elastic solvers); x=None removes it."""

@@ -67,6 +67,8 @@ typedef enum {
  * exa::Ops*, see exahype-engine_b200/csrc/exa_ops.cuh). Ids below EXA_PDE_USER_BASE, a mismatch
  * between the arguments and the object, or a second registration of the same key are refused. */
 int exa_register_pde(int pde, int dim, int order, int npar, void* ops);
+/* 1 if kernels for (pde, dim, order, npar) are available (built in or registered), else 0 */
+int exa_pde_available(int pde, int dim, int order, int npar);
 
 typedef enum {
   EXA_PREC_FP64 = 0,  /* every sweep in FP64 (generic-kernel semantics, parity 1e-12) */

@@ -1,0 +1,91 @@
+"""Application PDE functors compiled against include/exa_aderdg_user.cuh (the drop-in for the
+reference's user solver class and its hooks flux / eigenvalues / boundaryValues /
+adjustPointSolution, AbstractGenericADERDGSolverHeader.template:34-68, 220-338).
+
+tests/user_pde/user_euler.cu is such an application: Euler written from the reference's Euler app,
+with its own boundary_values (a reflective wall) and adjust_point_solution (a density wave), built
+into tests/user_pde/libuser_euler.so by the build step. Loading it registers pde EXA_PDE_USER_BASE
+for 3D and 2D order 3; the GPU tests run it through the unchanged C ABI against the oracle.
+"""
+import ctypes
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+USER_LIB = os.path.join(REPO, "tests", "user_pde", "libuser_euler.so")
+TOL = 1e-12
+
+
+def _load():
+    import exa_aderdg as exa
+    if not os.path.exists(USER_LIB):
+        pytest.skip("the application library was not built")
+    exa.load_user_pde(USER_LIB)
+    return exa
+
+
+def test_user_pde_registers_its_instantiations():
+    exa = _load()
+    base = exa.PDE_USER_BASE
+    assert exa.pde_available(base, 3, 3, 0) and exa.pde_available(base, 2, 3, 0)
+    assert not exa.pde_available(base, 3, 5, 0) and not exa.pde_available(base + 1, 3, 3, 0)
+    assert exa.pde_available(exa.PDE_EULER, 3, 5, 0)
+    lib = exa.load_library()
+    # ids below the user range and null launchers are refused
+    assert lib.exa_register_pde(3, 3, 3, 0, None) == 1
+
+
+def density_wave(x, dim):
+    """The application's adjust_point_solution at t = 0, restated in numpy."""
+    z = x[..., 2] if dim == 3 else 0.0
+    rho = 1.0 + 0.1 * np.sin(2.0 * np.pi * (x[..., 0] + 2.0 * x[..., 1] + 3.0 * z))
+    u = np.array([0.3, 0.2, 0.1 if dim == 3 else 0.0])
+    Q = np.zeros(x.shape[:-1] + (5,))
+    Q[..., 0] = rho
+    Q[..., 1:4] = rho[..., None] * u
+    Q[..., 4] = 1.0 / 0.4 + 0.5 * rho * (u ** 2).sum()
+    return Q.reshape(-1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,ncell,bc", [(3, (4, 3, 5), 4), (3, (3, 4, 3), 0), (2, (9, 7), 4), (2, (8, 6), 0)])
+def test_user_pde_adjust_and_steps_vs_oracle(dim, ncell, bc):
+    """adjust_point_solution sets the initial state on the device (checked against the numpy
+    restatement at the nodal positions); then 3 steps with the application's boundary_values on
+    every domain face (EXA_BC_USER) or periodic, against the oracle's Euler system with reflective
+    walls or periodic faces, at 1e-12 relative, with equal time steps."""
+    import exa_scenarios as sc
+    from pyoracle import Oracle
+    exa = _load()
+    order = 3
+    size = [1.0, 0.8, 1.2][:dim]
+    s = exa.Solver(exa.PDE_USER_BASE, dim, order)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    p.adjust_solution()
+    luh0 = p.get_solution()
+    want = density_wave(sc.nodal_positions(ncell, size, order), dim)
+    assert np.max(np.abs(luh0 - want)) <= 1e-14 * np.max(np.abs(want))
+    ref = luh0.copy()
+    t_ref, _, _ = Oracle(dim, order).run(ref, ncell, size, 3, walls=bc == 4)
+    p.step(3)
+    got = p.get_solution()
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))) < TOL
+    assert np.abs(got - luh0).max() > 1e-4
+    assert p.status() == 0
+    p.close()
+    s.close()
+
+
+@pytest.mark.gpu
+def test_builtin_functor_without_hooks_refuses_them():
+    exa = _load()
+    s = exa.Solver(exa.PDE_EULER, 3, 3)
+    with pytest.raises(exa.ExaError):
+        exa.Patch(s, [dict(ncell=(2, 2, 2), size=[1.0] * 3, bc=exa.BC_USER)])
+    p = exa.Patch(s, [dict(ncell=(2, 2, 2), size=[1.0] * 3)])
+    with pytest.raises(exa.ExaError):
+        p.adjust_solution()
