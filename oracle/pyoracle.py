@@ -225,3 +225,29 @@ class RefKernels:
                        int(walls), _p(luh), int(nsteps), ctypes.c_double(t0), ctypes.c_double(fixed_dt),
                        ctypes.byref(t), _p(dts), _p(pic) if pic is not None else None, int(nthreads))
         return t.value, dts, (pic.reshape(nsteps, nc) if pic is not None else None)
+
+
+class KGKernels:
+    """The reference's generated optimised kernels (KernelGenerator, plain-loop mode) for the Euler
+    application, 3D, order 3 or 5 (oracle/_ref/libkg_euler_o{3,5}.so, built by ``make -C oracle kg``)
+    behind a uniform-patch driver with the generic glue's step order. Cubic cells only."""
+
+    def __init__(self, order):
+        path = os.path.join(HERE, "_ref", "libkg_euler_o%d.so" % order)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.lib.kgref_run.restype = ctypes.c_int
+        self.order = order
+
+    def run(self, luh, ncell, size, nsteps, walls=False, fixed_dt=0.0, nthreads=0, want_picard=False):
+        luh = np.ascontiguousarray(luh, dtype=np.float64)
+        nc = int(np.prod(ncell))
+        dts = np.zeros(nsteps)
+        pic = np.zeros(nsteps * nc, dtype=np.int32) if want_picard else None
+        t = ctypes.c_double(0.0)
+        nce = np.array(list(ncell), dtype=np.int32)
+        sz = np.array(list(size), dtype=np.float64)
+        self.lib.kgref_run(_p(nce), _p(sz), int(walls), _p(luh), int(nsteps), ctypes.c_double(fixed_dt),
+                           ctypes.byref(t), _p(dts), _p(pic) if pic is not None else None, int(nthreads))
+        return t.value, dts, (pic.reshape(nsteps, nc) if pic is not None else None)

@@ -468,3 +468,28 @@ def test_swe_wall_patch_run_vs_ref(order, ncell):
     assert pb.min() >= 2 and pb.max() <= 2 * n
     assert relerr(lb, la) < 1e-12
     assert np.abs(lb - luh0).max() > 1e-3  # the bumps moved
+
+
+# ---------------------------------------------------------------------------------------------
+# The reference's generated optimised kernels (KernelGenerator, plain-loop mode; oracle/_ref/
+# libkg_euler_o{3,5}.so): the second CPU baseline, cross-checked against the generic kernels.
+# ---------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("order,walls", [(3, 0), (3, 3), (5, 0), (5, 3)])
+def test_kernelgenerator_kernels_vs_generic_reference(order, walls):
+    import exa_scenarios as sc
+    from pyoracle import KGKernels
+    try:
+        kg = KGKernels(order)
+        ref = RefKernels(3, order)
+    except (FileNotFoundError, AttributeError, OSError) as e:
+        pytest.skip("reference kernels not built: %s" % e)
+    ncell = (4, 3, 5)
+    luh, _ = sc.euler_entropy_wave(ncell, order)
+    a, b = luh.copy(), luh.copy()
+    size = [n / 5.0 for n in ncell]  # cubic cells, as the generated kernels assume
+    _, dta, pa = ref.run(a, ncell, size, 3, walls=walls, want_picard=True)
+    _, dtb, pb = kg.run(b, ncell, size, 3, walls=walls, want_picard=True)
+    assert np.max(np.abs(dta - dtb) / dta) < 1e-13
+    assert np.array_equal(pa + 1, pb)  # generic: break index; generated: sweeps
+    assert relerr(b, a) < 1e-13
