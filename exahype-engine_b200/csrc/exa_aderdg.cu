@@ -111,6 +111,7 @@ struct exa_solver {
   size_t scratch_doubles = 0;
   int* d_iscratch = nullptr;
   int pred_variant = -1;  // predictor launch variant (-1: the measured one)
+  int upd_variant = -1;   // update launch variant (-1: bulk-copy form where possible)
 };
 
 static exa::CellArgs base_args(exa_solver* s, int ncells) {
@@ -126,6 +127,15 @@ static exa::CellArgs base_args(exa_solver* s, int ncells) {
 extern "C" {
 
 const char* exa_last_error(void) { return g_err.c_str(); }
+
+int exa_quadrature(int order, double* nodes, double* weights) {
+  if (order < 1 || order > 9 || !nodes || !weights) return fail(EXA_ERR_INVALID, "order must be in 1..9");
+  for (int i = 0; i <= order; i++) {
+    nodes[i] = exa::h_nodes[order - 1][i];
+    weights[i] = exa::h_weights[order - 1][i];
+  }
+  return EXA_OK;
+}
 
 int exa_pde_available(int pde, int dim, int order, int npar) {
   return exa::find_ops(pde, dim, order, npar) != nullptr ? 1 : 0;
@@ -183,6 +193,13 @@ int exa_solver_destroy(exa_solver* s) {
 int exa_solver_set_predictor_variant(exa_solver* s, int variant) {
   if (!s || variant < -1 || variant > 1) return fail(EXA_ERR_INVALID, "variant must be -1, 0 or 1");
   s->pred_variant = variant;
+  return EXA_OK;
+}
+
+int exa_solver_set_update_variant(exa_solver* s, int variant) {
+  if (!s || variant < -1 || variant > 1) return fail(EXA_ERR_INVALID, "variant must be -1, 0 or 1");
+  s->upd_variant = variant;
+  s->ops->riemann_variant = variant;
   return EXA_OK;
 }
 
@@ -287,7 +304,7 @@ int exa_surface_integral_and_update(exa_solver* s, int ncells, double* luh, cons
   a.lduh = const_cast<double*>(lduh);
   a.lFhbnd = const_cast<double*>(lFhbnd);
   set_uniform(a, s, dx, dt);
-  EXA_CUDA(s->ops->update(a, true, true, (cudaStream_t)stream));
+  EXA_CUDA(s->ops->update(a, true, true, (cudaStream_t)stream, s->upd_variant));
   return EXA_OK;
 }
 
@@ -395,9 +412,34 @@ int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbn
   return converged ? sweeps - 1 : maxIter;
 }
 
+// one cell's volume / surface / face integral on the device (cell_integral_kernel)
+static int shim_cell_integral(exa_solver* s, int mode, double* lduh, const double* in, size_t in_doubles,
+                              int direction, int orientation, const double* dx) {
+  std::lock_guard<std::mutex> lk(s->mu);
+  const exa::Ops& o = *s->ops;
+  if (int e = shim_scratch(s, o.sz_lduh + in_doubles)) return e;
+  double* d_du = s->d_scratch;
+  double* d_in = d_du + o.sz_lduh;
+  if (mode != 0) EXA_CUDA(cudaMemcpy(d_du, lduh, o.sz_lduh * sizeof(double), cudaMemcpyHostToDevice));
+  EXA_CUDA(cudaMemcpy(d_in, in, in_doubles * sizeof(double), cudaMemcpyHostToDevice));
+  double d3[3] = {1.0, 1.0, 1.0};
+  for (int d = 0; d < o.dim; d++) d3[d] = dx[d];
+  EXA_CUDA(s->ops->cell_integral(mode, d_du, d_in, direction, orientation, d3, 0));
+  EXA_CUDA(cudaMemcpy(lduh, d_du, o.sz_lduh * sizeof(double), cudaMemcpyDeviceToHost));
+  return EXA_OK;
+}
+
 int exa_volumeIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhi, const double* dx) {
-  (void)s; (void)lduh; (void)lFhi; (void)dx;
-  return fail(EXA_ERR_UNSUPPORTED, "volumeIntegralNonlinear is fused into exa_fused_predictor_volume_integral");
+  if (!s || !lduh || !lFhi || !dx) return fail(EXA_ERR_INVALID, "null argument");
+  return shim_cell_integral(s, 0, lduh, lFhi, s->ops->sz_lFhi, 0, 0, dx);
+}
+
+int exa_faceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, int direction, int orientation,
+                              const double* dx) {
+  if (!s || !lduh || !lFhbnd || !dx) return fail(EXA_ERR_INVALID, "null argument");
+  if (direction < 0 || direction >= s->ops->dim || (orientation != 0 && orientation != 1))
+    return fail(EXA_ERR_INVALID, "bad face");
+  return shim_cell_integral(s, 2, lduh, lFhbnd, (size_t)s->ops->nf * s->ops->nvar, direction, orientation, dx);
 }
 
 int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const double* QL, const double* QR, double t,
@@ -437,8 +479,8 @@ int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const doub
 }
 
 int exa_surfaceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, const double* dx) {
-  (void)s; (void)lduh; (void)lFhbnd; (void)dx;
-  return fail(EXA_ERR_UNSUPPORTED, "surfaceIntegralNonlinear is fused into exa_surface_integral_and_update");
+  if (!s || !lduh || !lFhbnd || !dx) return fail(EXA_ERR_INVALID, "null argument");
+  return shim_cell_integral(s, 1, lduh, lFhbnd, s->ops->sz_fhb, 0, 0, dx);
 }
 
 int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const double* lduh, double dt) {
@@ -506,6 +548,7 @@ struct exa_patch {
   int *fL = nullptr, *fR = nullptr;
   int8_t* fdir = nullptr;
   int nfaces = 0;
+  int nhalo_faces = 0;  // the last nhalo_faces of the face list touch a ghost cell
   int* bcell = nullptr;
   int8_t* bface = nullptr;
   int nbfaces = 0;
@@ -579,6 +622,7 @@ static exa::FaceArgs patch_faces(exa_patch* p) {
   f.bcell = p->bcell;
   f.bface = p->bface;
   f.btype = p->btype;
+  f.status = p->status;
   f.cell_grid = p->grids.size() > 1 ? p->cell_grid : nullptr;
   f.grid_dx = p->grid_dx;
   f.grid_geo = p->grid_geo;
@@ -601,7 +645,7 @@ static int patch_enqueue_step(exa_patch* p, bool cfl) {
   }
   exa::CellArgs u = patch_args(p);
   if (cfl) u.grid_dt_next = p->grid_dt_next;
-  EXA_CUDA(p->s->ops->update(u, true, true, p->stream));
+  EXA_CUDA(p->s->ops->update(u, true, true, p->stream, p->s->upd_variant));
   const int ng = (int)p->grids.size();
   if (cfl) {
     exa::advance_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_t, p->grid_dt, p->grid_dt_next, p->steps);
@@ -634,6 +678,7 @@ namespace {
 struct FaceBuild {
   long long ncells = 0, nghost = 0, layer = 0;
   int halo_axis = -1;
+  int nhalo_faces = 0;  // faces that touch a ghost cell, at the end of fL / fR / fd
   std::vector<int> cell_grid, fL, fR, bc;
   std::vector<int8_t> fd, bf, bt;
   std::vector<double> dx;
@@ -716,6 +761,24 @@ int build_faces(int dim, int ngrids, const exa_grid_desc* grids, FaceBuild& fb) 
           }
     if (ngrids > 1) fb.cell_grid.insert(fb.cell_grid.end(), (size_t)(nc[0] * (long long)nc[1] * nc[2]), g);
   }
+  // faces that touch a ghost cell go last (stable), so that the faces between real cells can run
+  // while the ghosts' traces are still being exchanged
+  if (fb.nghost > 0) {
+    std::vector<int> L, R;
+    std::vector<int8_t> Dd;
+    for (int pass = 0; pass < 2; pass++)
+      for (size_t k = 0; k < fb.fL.size(); k++) {
+        const bool ghost = fb.fL[k] >= fb.ncells || fb.fR[k] >= fb.ncells;
+        if (ghost != (pass == 1)) continue;
+        L.push_back(fb.fL[k]);
+        R.push_back(fb.fR[k]);
+        Dd.push_back(fb.fd[k]);
+        if (ghost) fb.nhalo_faces++;
+      }
+    fb.fL.swap(L);
+    fb.fR.swap(R);
+    fb.fd.swap(Dd);
+  }
   return EXA_OK;
 }
 }  // namespace
@@ -772,6 +835,7 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
     p->halo_hi_first = fb.ncells - fb.layer;
   }
   p->nfaces = (int)fL.size();
+  p->nhalo_faces = fb.nhalo_faces;
   p->nbfaces = (int)bc.size();
   exa::Ops& o = *s->ops;
   const long long nc = p->ncells;
@@ -990,11 +1054,21 @@ int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt) {
       EXA_CUDA(p->s->ops->predictor(a, p->stream, p->s->cfg.precision == EXA_PREC_MIXED, p->s->pred_variant));
       return EXA_OK;
     }
-    case EXA_PHASE_FACES: {
+    case EXA_PHASE_FACES:
+    case EXA_PHASE_FACES_INTERIOR:
+    case EXA_PHASE_FACES_HALO: {
       exa::FaceArgs f = patch_faces(p);
+      const int ninner = p->nfaces - p->nhalo_faces;
+      if (phase == EXA_PHASE_FACES_INTERIOR) f.nfaces = ninner;
+      if (phase == EXA_PHASE_FACES_HALO) {
+        f.nfaces = p->nhalo_faces;
+        f.left += ninner;
+        f.right += ninner;
+        f.dir += ninner;
+      }
       EXA_CUDA(p->s->ops->riemann(f, p->stream));
-      if (p->nbfaces > 0) {
-        exa::FaceArgs b = f;
+      if (p->nbfaces > 0 && phase != EXA_PHASE_FACES_HALO) {
+        exa::FaceArgs b = patch_faces(p);
         b.nfaces = p->nbfaces;
         EXA_CUDA(p->s->ops->boundary(b, p->stream));
       }
@@ -1003,7 +1077,7 @@ int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt) {
     case EXA_PHASE_UPDATE: {
       exa::CellArgs u = patch_args(p);
       if (cfl) u.grid_dt_next = p->grid_dt_next;
-      EXA_CUDA(p->s->ops->update(u, true, true, p->stream));
+      EXA_CUDA(p->s->ops->update(u, true, true, p->stream, p->s->upd_variant));
       return EXA_OK;
     }
     case EXA_PHASE_ADVANCE: {
@@ -1356,7 +1430,7 @@ int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int 
       u.cell_begin = (int)c0;
       u.ncells = (int)c1;
       if (cfl) u.grid_dt_next = p->grid_dt_next;
-      EXA_CUDA(o.update(u, true, true, p->stream));
+      EXA_CUDA(o.update(u, true, true, p->stream, p->s->upd_variant));
       EXA_CUDA(cudaEventRecord(p->ev_upd[j], p->stream));
       EXA_CUDA(cudaStreamWaitEvent(p->d2h_stream, p->ev_upd[j], 0));
       EXA_CUDA(cudaMemcpyAsync(luh_out + c0 * per, p->luh + c0 * per, (size_t)(c1 - c0) * per * sizeof(double),

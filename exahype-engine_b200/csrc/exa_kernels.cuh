@@ -196,6 +196,7 @@ struct FaceArgs {
   const int* bcell;         // cell owning the boundary face
   const int8_t* bface;      // face index 2*dir + orientation
   const int8_t* btype;      // boundary type (EXA_BC_WALL, EXA_BC_OUTFLOW, EXA_BC_USER)
+  unsigned* status;         // error bits (nullable): bounded waits that ran out
   // geometry and time of the boundary faces' cells (EXA_BC_USER: the functor's boundary_values
   // is evaluated at the face nodes' coordinates); nullable grid arrays as in CellArgs
   const int* cell_grid;
@@ -474,6 +475,82 @@ __global__ void __launch_bounds__(256) riemann_kernel(FaceArgs f) {
   rusanov_face<PDE, DIM, N, P>(QL, QR, FL, FR, d, lane, false, false, BuiltinGhost<PDE, DIM, N, P>{d, d});
 }
 
+// Rusanov on interior faces with bulk copies: persistent warps (8 per CTA), each walking faces
+// w, w + W, ... (W warps in the grid); a face's four trace blocks (QL, QR: nf*D doubles; FL, FR: nf*V)
+// arrive in the warp's own shared-memory buffer by bulk copy -- the next face's while the current
+// one is solved, two buffers per warp -- and FL, FR leave by bulk store. For trace blocks whose
+// sizes are multiples of 16 bytes (RiemannBulk::ok) and 16-byte aligned arrays.
+template <class PDE, int DIM, int N, int P>
+struct RiemannBulk {
+  using S = Shape<PDE, DIM, N, P>;
+  static constexpr int nQ = S::nf * S::D, nF = S::nf * S::V;
+  static constexpr int face = 2 * nQ + 2 * nF;                    // doubles of one face
+  static constexpr int WPB = 8;                                   // warps per CTA
+  static constexpr size_t smem = sizeof(double) * (size_t)(2 * WPB * face);
+  static constexpr bool ok = nQ % 2 == 0 && nF % 2 == 0 && smem <= 200 * 1024;
+};
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) riemann_bulk_kernel(FaceArgs f) {
+  using S = Shape<PDE, DIM, N, P>;
+  using R = RiemannBulk<PDE, DIM, N, P>;
+  extern __shared__ __align__(128) double smem[];
+  __shared__ __align__(8) uint64_t s_bar[R::WPB][2];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int warps = gridDim.x * R::WPB;
+  double* base = smem + (size_t)wl * 2 * R::face;
+  auto issue = [&](int fc, int b) {  // lane 0: the face's four blocks into buffer b
+    const int d = f.dir[fc];
+    const long cl = f.left[fc], cr = f.right[fc];
+    double* st = base + (size_t)b * R::face;
+    mbar_arrive_expect_tx(&s_bar[wl][b], (2 * R::nQ + 2 * R::nF) * 8);
+    bulk_g2s(st, f.lQhbnd + cl * S::sizeQhb + (2 * d + 1) * R::nQ, R::nQ * 8, &s_bar[wl][b]);
+    bulk_g2s(st + R::nQ, f.lQhbnd + cr * S::sizeQhb + (2 * d) * R::nQ, R::nQ * 8, &s_bar[wl][b]);
+    bulk_g2s(st + 2 * R::nQ, f.lFhbnd + cl * S::sizeFhb + (2 * d + 1) * R::nF, R::nF * 8, &s_bar[wl][b]);
+    bulk_g2s(st + 2 * R::nQ + R::nF, f.lFhbnd + cr * S::sizeFhb + (2 * d) * R::nF, R::nF * 8, &s_bar[wl][b]);
+  };
+  const int w0 = blockIdx.x * R::WPB + wl;
+  if (lane == 0) {
+    mbar_init(&s_bar[wl][0], 1);
+    mbar_init(&s_bar[wl][1], 1);
+    fence_mbar_init();
+    if (w0 < f.nfaces) issue(w0, 0);
+  }
+  __syncwarp();
+  int stall = -1;
+  for (int it = 0;; it++) {
+    const int fc = w0 + it * warps;
+    if (fc >= f.nfaces) break;
+    const int b = it & 1;
+    const bool to = !mbar_wait_bounded(&s_bar[wl][b], (it >> 1) & 1, kBulkWaitLimitNs);
+    if (__any_sync(0xffffffffu, to)) {
+      if (lane == 0 && f.status) atomicOr(f.status, ST_TIMEOUT);
+      stall = b | (((it >> 1) & 1) << 1);
+      break;
+    }
+    if (lane == 0 && fc + warps < f.nfaces) {
+      bulk_wait_read_all();  // the other buffer's bulk stores have read it
+      issue(fc + warps, b ^ 1);
+    }
+    double* st = base + (size_t)b * R::face;
+    const int d = f.dir[fc];
+    rusanov_face<PDE, DIM, N, P>(st, st + R::nQ, st + 2 * R::nQ, st + 2 * R::nQ + R::nF, d, lane, false, false,
+                                 BuiltinGhost<PDE, DIM, N, P>{d, d});
+    fence_proxy_async_smem();
+    __syncwarp();
+    if (lane == 0) {
+      const long cl = f.left[fc], cr = f.right[fc];
+      bulk_s2g(f.lFhbnd + cl * S::sizeFhb + (2 * d + 1) * R::nF, st + 2 * R::nQ, R::nF * 8);
+      bulk_s2g(f.lFhbnd + cr * S::sizeFhb + (2 * d) * R::nF, st + 2 * R::nQ + R::nF, R::nF * 8);
+      bulk_commit();
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (stall >= 0) (void)mbar_wait_bounded(&s_bar[wl][stall & 1], (uint32_t)(stall >> 1), kBulkWaitLimitNs);
+    bulk_wait_all();
+  }
+}
+
 // Domain-boundary faces with a reflective wall: the ghost state is the mirrored inner state,
 // its flux the flux of the ghost state; the Riemann solver sees it on the outer side.
 template <class PDE, int DIM, int N, int P>
@@ -676,6 +753,228 @@ update_kernel(CellArgs a) {
   if (p == 0 && live) {
     if (a.cell_dt) a.cell_dt[cell] = s_min[lc];
     if (a.grid_dt_next) atomic_min_pos(&a.grid_dt_next[g], s_min[lc]);
+  }
+}
+
+// Per-cell integrals of the generic-kernel interface on one cell, thread per node, in the
+// reference's operation order:
+//   mode 0  volumeIntegralNonlinear (3d/volumeIntegralNonlinear.cpph:133-223): lduh = sum over the
+//           directions of Kxi[k][m] lFhi_d[line][m] w_a w_b / dx_d (+ w_xyz lShi with a source or
+//           NCP) from the reference lFhi blocks x [z][y][x], y [z][x][y], z [y][x][z], source;
+//   mode 1  surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90): lduh -= the six
+//           faces' terms from lFhbnd [2*DIM][face node][V];
+//   mode 2  faceIntegralNonlinear (3d/faceIntegralNonlinear.cpph:21-103): lduh -= w_a w_b
+//           (2 orientation - 1) / dx_d FCoeff[orientation][k] F of one face block.
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) cell_integral_kernel(int mode, double* lduh, const double* in, int direction,
+                                                            int orientation, double dx0, double dx1, double dx2) {
+  using S = Shape<PDE, DIM, N, P>;
+  using G = GL<N>;
+  constexpr int n = S::n, V = S::V, nd = S::nd, nf = S::nf;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nd) return;
+  const double dxv[3] = {dx0, dx1, dx2};
+  int co[3];
+  node_coords<DIM, n>(p, co);
+  double* du = lduh + (size_t)p * V;
+  if (mode == 0) {
+    double acc[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) acc[m] = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const int L = node_line<DIM, n>(p, d);
+      const double wt = DIM == 3 ? G::weights(L / n) * G::weights(L % n) : G::weights(L);
+      const double us = wt * (1.0 / dxv[d]);
+      const double* F = in + (size_t)d * nd * V + (size_t)L * n * V;
+#pragma unroll
+      for (int m = 0; m < V; m++)
+#pragma unroll
+        for (int mm = 0; mm < n; mm++) acc[m] += G::Kxi(co[d], mm) * F[mm * V + m] * us;
+    }
+    if (PDE::kNCP || PDE::kSource) {
+      const double w = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
+                                : G::weights(co[1]) * G::weights(co[0]);
+#pragma unroll
+      for (int m = 0; m < V; m++) acc[m] += w * in[(size_t)DIM * nd * V + (size_t)p * V + m];
+    }
+#pragma unroll
+    for (int m = 0; m < V; m++) du[m] = acc[m];
+  } else if (mode == 1) {
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+      const int fn = node_line<DIM, n>(p, d);
+      const double wt = DIM == 3 ? G::weights(fn / n) * G::weights(fn % n) : G::weights(fn);
+      const double us = wt * (1.0 / dxv[d]);
+      const int k = co[d];
+#pragma unroll
+      for (int m = 0; m < V; m++)
+        du[m] -= (in[((2 * d + 1) * nf + fn) * V + m] * G::F1(k) - in[((2 * d) * nf + fn) * V + m] * G::F0(k)) * us;
+    }
+  } else {
+    const int d = direction;
+    const int fn = node_line<DIM, n>(p, d);
+    const double scaling = 1.0 / dxv[d] * (2.0 * orientation - 1.0);
+    const double sw = (DIM == 3 ? G::weights(fn / n) * G::weights(fn % n) : G::weights(fn)) * scaling;
+    const double fc = orientation ? G::F1(co[d]) : G::F0(co[d]);
+#pragma unroll
+    for (int m = 0; m < V; m++) du[m] -= sw * fc * in[fn * V + m];
+  }
+}
+
+// Surface integral + solution update + CFL (update_kernel<..., true, true>) as a persistent kernel
+// over cell groups: each group's luh, lduh and lFhbnd blocks (contiguous per group) arrive in shared
+// memory by bulk copy -- the next group's while the current one is computed, two buffers -- and the
+// new luh block leaves by one bulk store. For blocks whose sizes are multiples of 16 bytes
+// (UpdateBulk::ok) and 16-byte aligned arrays; the launcher falls back to update_kernel otherwise.
+template <class PDE, int DIM, int N, int P>
+struct UpdateBulk {
+  using S = Shape<PDE, DIM, N, P>;
+  static constexpr int nL = S::CPB * S::nd * S::D, nU = S::CPB * S::nd * S::V, nF = S::CPB * S::sizeFhb;
+  static constexpr int stage = nL + nU + nF;                         // doubles of one buffer
+  static constexpr size_t smem = 2 * sizeof(double) * (size_t)stage;
+  static constexpr bool ok =
+      (S::nd * S::D) % 2 == 0 && (S::nd * S::V) % 2 == 0 && S::sizeFhb % 2 == 0 && smem <= 200 * 1024;
+};
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_bulk_kernel(CellArgs a) {
+  using S = Shape<PDE, DIM, N, P>;
+  using B = UpdateBulk<PDE, DIM, N, P>;
+  using G = GL<N>;
+  constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf, CPB = S::CPB;
+  extern __shared__ __align__(128) double smem[];
+  __shared__ __align__(8) uint64_t s_bar[2];
+  __shared__ double s_min[CPB];
+  const int tid = threadIdx.x;
+  const bool inr = tid < CPB * nd;
+  const int lc = inr ? tid / nd : 0, p = inr ? tid % nd : 0;
+  const int ngroups = (a.ncells - a.cell_begin + CPB - 1) / CPB;
+  auto live_cells = [&](int g) { return min(CPB, a.ncells - (a.cell_begin + g * CPB)); };
+  auto issue = [&](int g, int b) {  // thread 0: the group's three blocks into buffer b
+    const size_t c0 = (size_t)a.cell_begin + (size_t)g * CPB;
+    const int nl = live_cells(g);
+    double* st = smem + (size_t)b * B::stage;
+    const uint32_t bl = nl * nd * D * 8, bu = nl * nd * V * 8, bf = nl * S::sizeFhb * 8;
+    mbar_arrive_expect_tx(&s_bar[b], bl + bu + bf);
+    bulk_g2s(st, a.luh + c0 * nd * D, bl, &s_bar[b]);
+    bulk_g2s(st + B::nL, a.lduh + c0 * nd * V, bu, &s_bar[b]);
+    bulk_g2s(st + B::nL + B::nU, a.lFhbnd + c0 * S::sizeFhb, bf, &s_bar[b]);
+  };
+  if (tid == 0) {
+    mbar_init(&s_bar[0], 1);
+    mbar_init(&s_bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < ngroups) issue(blockIdx.x, 0);
+  int co[3];
+  node_coords<DIM, n>(p, co);
+  const double w_sp = DIM == 3 ? G::weights(co[2]) * G::weights(co[1]) * G::weights(co[0])
+                               : G::weights(co[1]) * G::weights(co[0]);
+  int stall = -1;
+  for (int it = 0;; it++) {
+    const int grp = blockIdx.x + it * gridDim.x;
+    if (grp >= ngroups) break;
+    const int b = it & 1;
+    const bool to = !mbar_wait_bounded(&s_bar[b], (it >> 1) & 1, kBulkWaitLimitNs);
+    if (__syncthreads_or(to)) {
+      if (tid == 0 && a.status) atomicOr(a.status, ST_TIMEOUT);
+      stall = b | (((it >> 1) & 1) << 1);
+      break;
+    }
+    if (tid == 0 && grp + (int)gridDim.x < ngroups) {
+      // the other buffer's last bulk store (group it - 1) must have read it before it is refilled
+      bulk_wait_read_all();
+      issue(grp + gridDim.x, b ^ 1);
+    }
+    double* st = smem + (size_t)b * B::stage;
+    const int cell = a.cell_begin + grp * CPB + lc;
+    const bool live = inr && cell < a.ncells;
+    if (tid < CPB) s_min[tid] = __longlong_as_double(0x7ff0000000000000ll);
+    const int g = (live && a.cell_grid) ? a.cell_grid[cell] : 0;
+    double invDx[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) invDx[d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
+    double* q = st + ((size_t)lc * nd + p) * D;
+    double qv[D];
+    bool ok = true;
+    if (live) {
+      const double* du = st + B::nL + ((size_t)lc * nd + p) * V;
+      const double* Fb = st + B::nL + B::nU + (size_t)lc * S::sizeFhb;
+      double dv[V];
+#pragma unroll
+      for (int m = 0; m < V; m++) dv[m] = du[m];
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        const int fn = node_line<DIM, n>(p, d);
+        const double wt = DIM == 3 ? G::weights(fn / n) * G::weights(fn % n) : G::weights(fn);
+        const double us = wt * invDx[d];
+        const int k = co[d];
+#pragma unroll
+        for (int m = 0; m < V; m++)
+          dv[m] -= (Fb[((2 * d + 1) * nf + fn) * V + m] * G::F1(k) - Fb[((2 * d) * nf + fn) * V + m] * G::F0(k)) * us;
+      }
+      const double updateSize = (a.grid_dt ? a.grid_dt[g] : a.u_dt) / w_sp;
+#pragma unroll
+      for (int m = 0; m < D; m++) qv[m] = q[m];
+#pragma unroll
+      for (int m = 0; m < V; m++) {
+        qv[m] = qv[m] + dv[m] * updateSize;
+        ok &= finite(qv[m]);
+        q[m] = qv[m];
+      }
+    }
+    // CFL of the new state (stableTimeStepSize :14-62)
+    double dtp = __longlong_as_double(0x7ff0000000000000ll);
+    if (live && (a.grid_dt_next || a.cell_dt)) {
+      double den = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; d++) {
+        double lam[V];
+        PDE::template eigenvalues<DIM>(qv, d, lam);
+        double mx = 0.0;
+#pragma unroll
+        for (int m = 0; m < V; m++) mx = fmax(fabs(lam[m]), mx);
+        den += mx * invDx[d];
+      }
+      dtp = a.cfl_pnpm / den;
+      bool qok = true;
+#pragma unroll
+      for (int m = 0; m < D; m++) qok &= finite(qv[m]);
+      if (!(dtp > 0.0) || !qok) {
+        if (a.status) atomicOr(a.status, ST_BAD_DT);
+        dtp = __longlong_as_double(0x7ff0000000000000ll);
+      }
+    }
+    if (live && !ok && a.status) atomicOr(a.status, ST_NONFINITE_UPDATE);
+    {
+      const int lane = tid & 31;
+      const int seg_end = (lc + 1) * nd - 1;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_down_sync(0xffffffffu, dtp, off);
+        if (lane + off < 32 && tid + off <= seg_end) dtp = fmin(dtp, o);
+      }
+      if ((p == 0 || lane == 0) && live) atomic_min_pos(&s_min[lc], dtp);
+    }
+    // the new luh block is complete in shared memory: one bulk store (thread 0)
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      const size_t c0 = (size_t)a.cell_begin + (size_t)grp * CPB;
+      bulk_s2g(a.luh_out + c0 * nd * D, st, live_cells(grp) * nd * D * 8);
+      bulk_commit();
+    }
+    if (p == 0 && live) {
+      if (a.cell_dt) a.cell_dt[cell] = s_min[lc];
+      if (a.grid_dt_next) atomic_min_pos(&a.grid_dt_next[g], s_min[lc]);
+    }
+    // s_min and this buffer are reused two groups on
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (stall >= 0) (void)mbar_wait_bounded(&s_bar[stall & 1], (uint32_t)(stall >> 1), kBulkWaitLimitNs);
+    bulk_wait_all();
   }
 }
 

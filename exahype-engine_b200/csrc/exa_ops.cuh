@@ -21,6 +21,9 @@ struct Ops {
   bool ncp;
   virtual ~Ops() {}
   bool mixed_ok = false;  // mixed-precision predictor instantiated
+  // Riemann launch form for all solvers of this instantiation: 0 riemann_kernel, otherwise
+  // riemann_bulk_kernel where the trace blocks allow it (exa_solver_set_update_variant sets it)
+  int riemann_variant = -1;
   // variant: 0 one cell group per CTA, 1 persistent CTAs with a prefetched next group, -1 the
   // variant tune() measured as faster on this device (0 until tuned)
   virtual cudaError_t predictor(const CellArgs& a, cudaStream_t st, bool mixed, int variant) = 0;
@@ -30,7 +33,9 @@ struct Ops {
   virtual int tuned_variant(bool mixed) = 0;
   // device scratch the predictor needs for a launch over ncells (outside stream capture)
   virtual cudaError_t reserve(long long ncells) = 0;
-  virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) = 0;
+  // variant (surface + update only): 0 update_kernel; 1 update_bulk_kernel (persistent, bulk copies),
+  // where the block sizes and the arrays' alignment allow it; -1 the latter where possible
+  virtual cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st, int variant = -1) = 0;
   virtual cudaError_t riemann(const FaceArgs& f, cudaStream_t st) = 0;
   virtual cudaError_t boundary(const FaceArgs& f, cudaStream_t st) = 0;
   // discrete adjoint of one step (linear systems only)
@@ -40,6 +45,9 @@ struct Ops {
   // (faces of type EXA_BC_USER)
   bool adjust_ok = false, user_bc_ok = false;
   virtual cudaError_t adjust(const CellArgs& a, cudaStream_t st) = 0;
+  // per-cell volume (mode 0), surface (1) and face (2) integrals of one cell (cell_integral_kernel)
+  virtual cudaError_t cell_integral(int mode, double* lduh, const double* in, int direction, int orientation,
+                                    const double* dx, cudaStream_t st) = 0;
 };
 
 template <class PDE, int DIM, int N, int P>
@@ -237,6 +245,12 @@ struct OpsImpl final : Ops {
       return cudaErrorNotSupported;
     }
   }
+  cudaError_t cell_integral(int mode, double* lduh, const double* in, int direction, int orientation,
+                            const double* dx, cudaStream_t st) override {
+    cell_integral_kernel<PDE, DIM, N, P><<<(S::nd + 255) / 256, 256, 0, st>>>(
+        mode, lduh, in, direction, orientation, dx[0], DIM > 1 ? dx[1] : 1.0, DIM > 2 ? dx[2] : 1.0);
+    return cudaGetLastError();
+  }
   cudaError_t adjust(const CellArgs& a, cudaStream_t st) override {
     if constexpr (has_adjust_point_solution<PDE, DIM>::value) {
       const long long nodes = (long long)a.ncells * S::nd;
@@ -296,8 +310,36 @@ struct OpsImpl final : Ops {
     if constexpr (!kStreamed) return launch_variant<false>(a, st, v);
     return cudaErrorNotSupported;
   }
-  cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st) override {
+  int upd_grid[64] = {};
+  bool upd_bulk_attr = false;
+  cudaError_t update(const CellArgs& a, bool surface, bool upd, cudaStream_t st, int variant) override {
     if (a.ncells <= a.cell_begin) return cudaSuccess;
+    using UB = UpdateBulk<PDE, DIM, N, P>;
+    auto al = [](const void* q) { return reinterpret_cast<uintptr_t>(q) % 16 == 0; };
+    if constexpr (UB::ok) {
+      if (surface && upd && variant != 0 && al(a.luh) && al(a.luh_out) && al(a.lduh) && al(a.lFhbnd)) {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        auto kern = update_bulk_kernel<PDE, DIM, N, P>;
+        if (!upd_bulk_attr) {
+          if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)UB::smem)) !=
+              cudaSuccess)
+            return e;
+          upd_bulk_attr = true;
+        }
+        if (upd_grid[dev] == 0) {
+          int sms = 0, occ = 0;
+          if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+          if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::TPB, UB::smem)) != cudaSuccess) return e;
+          upd_grid[dev] = sms * std::max(occ, 1);
+        }
+        const long long groups = ((long long)a.ncells - a.cell_begin + S::CPB - 1) / S::CPB;
+        kern<<<(unsigned)std::min<long long>(groups, upd_grid[dev]), S::TPB, UB::smem, st>>>(a);
+        return cudaGetLastError();
+      }
+    }
     const unsigned blocks = (unsigned)((a.ncells - a.cell_begin + S::CPB - 1) / S::CPB);
     if (surface && upd)
       update_kernel<PDE, DIM, N, P, true, true><<<blocks, S::TPB, 0, st>>>(a);
@@ -307,8 +349,37 @@ struct OpsImpl final : Ops {
       update_kernel<PDE, DIM, N, P, false, false><<<blocks, S::TPB, 0, st>>>(a);
     return cudaGetLastError();
   }
+  int rie_grid[64] = {};
+  bool rie_bulk_attr = false;
   cudaError_t riemann(const FaceArgs& f, cudaStream_t st) override {
     if (f.nfaces <= 0) return cudaSuccess;
+    using RB = RiemannBulk<PDE, DIM, N, P>;
+    auto al = [](const void* q) { return reinterpret_cast<uintptr_t>(q) % 16 == 0; };
+    if constexpr (RB::ok) {
+      if (riemann_variant != 0 && al(f.lQhbnd) && al(f.lFhbnd)) {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+        auto kern = riemann_bulk_kernel<PDE, DIM, N, P>;
+        if (!rie_bulk_attr) {
+          if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RB::smem)) !=
+              cudaSuccess)
+            return e;
+          rie_bulk_attr = true;
+        }
+        if (rie_grid[dev] == 0) {
+          int sms = 0, occ = 0;
+          if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+          if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 32 * RB::WPB, RB::smem)) != cudaSuccess)
+            return e;
+          rie_grid[dev] = sms * std::max(occ, 1);
+        }
+        const long long ctas = ((long long)f.nfaces + RB::WPB - 1) / RB::WPB;
+        kern<<<(unsigned)std::min<long long>(ctas, rie_grid[dev]), 32 * RB::WPB, RB::smem, st>>>(f);
+        return cudaGetLastError();
+      }
+    }
     const unsigned blocks = (unsigned)((f.nfaces + 7) / 8);
     riemann_kernel<PDE, DIM, N, P><<<blocks, 256, 0, st>>>(f);
     return cudaGetLastError();

@@ -57,6 +57,7 @@ class FaceLists(ctypes.Structure):
 
 
 PHASE_PREDICTOR, PHASE_FACES, PHASE_UPDATE, PHASE_ADVANCE = 0, 1, 2, 3
+PHASE_FACES_INTERIOR, PHASE_FACES_HALO = 4, 5
 BC_HALO, BC_OUTFLOW, BC_USER = 2, 3, 4
 PDE_USER_BASE = 64
 
@@ -98,6 +99,7 @@ def load_library(path=None):
         "exa_solver_sizes": [vp, ctypes.POINTER(_Sizes)],
         "exa_solver_set_predictor_variant": [vp, i],
         "exa_solver_predictor_variant": [vp, ctypes.POINTER(i)],
+        "exa_solver_set_update_variant": [vp, i],
         "exa_solver_status": [vp, ctypes.POINTER(ctypes.c_uint)],
         "exa_fused_predictor_volume_integral": [vp, i, vp, vp, vp, vp, vp, dp, d, d, vp],
         "exa_riemann_solver_nonlinear": [vp, i, vp, vp, vp, vp, vp, vp],
@@ -108,6 +110,9 @@ def load_library(path=None):
         "exa_spaceTimePredictorNonlinear": [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, d, d],
         "exa_riemannSolverNonlinear": [vp, vp, vp, vp, vp, d, d, dp, i],
         "exa_solutionUpdate": [vp, vp, vp, vp, d],
+        "exa_volumeIntegralNonlinear": [vp, vp, vp, dp],
+        "exa_surfaceIntegralNonlinear": [vp, vp, vp, dp],
+        "exa_faceIntegralNonlinear": [vp, vp, vp, i, i, dp],
         "exa_stableTimeStepSize": [vp, vp, dp, dp],
         "exa_patch_create": [vp, i, ctypes.POINTER(GridDesc), ctypes.POINTER(vp)],
         "exa_patch_destroy": [vp],
@@ -240,6 +245,10 @@ class Solver:
         _check(self.lib.exa_solver_predictor_variant(self.h, ctypes.byref(v)), "exa_solver_predictor_variant")
         return v.value
 
+    def set_update_variant(self, v):
+        """0: update kernel with per-thread loads; 1 / -1: bulk-copy form where possible."""
+        _check(self.lib.exa_solver_set_update_variant(self.h, int(v)), "exa_solver_set_update_variant")
+
     @predictor_variant.setter
     def predictor_variant(self, v):
         """-1 selects the variant measured as faster on this device."""
@@ -310,6 +319,27 @@ class Solver:
         _check(self.lib.exa_solutionUpdate(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(luh, dtype=float)),
                                            _np_ptr(np.ascontiguousarray(lduh, dtype=float)), float(dt)),
                "exa_solutionUpdate")
+        return out
+
+    def volume_integral_cell(self, lFhi, dx):
+        """volumeIntegralNonlinear of one cell from its reference lFhi blocks (host arrays)."""
+        out = np.zeros(self.sizes["lduh"])
+        _check(self.lib.exa_volumeIntegralNonlinear(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(lFhi, dtype=float)),
+                                                    _dx3(dx, self.dim)), "exa_volumeIntegralNonlinear")
+        return out
+
+    def surface_integral_cell(self, lduh, lFhbnd, dx):
+        out = np.ascontiguousarray(lduh, dtype=float).copy()
+        _check(self.lib.exa_surfaceIntegralNonlinear(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(lFhbnd, dtype=float)),
+                                                     _dx3(dx, self.dim)), "exa_surfaceIntegralNonlinear")
+        return out
+
+    def face_integral_cell(self, lduh, lFhbnd_face, direction, orientation, dx):
+        out = np.ascontiguousarray(lduh, dtype=float).copy()
+        _check(self.lib.exa_faceIntegralNonlinear(self.h, _np_ptr(out),
+                                                  _np_ptr(np.ascontiguousarray(lFhbnd_face, dtype=float)),
+                                                  int(direction), int(orientation), _dx3(dx, self.dim)),
+               "exa_faceIntegralNonlinear")
         return out
 
     def stable_time_step_size_cell(self, luh, dx):

@@ -7,8 +7,9 @@ and the admissible time step is reduced over all ranks before the next step
 per rank (one rank per GPU). A rank's patch carries EXA_BC_HALO on that axis. Every step:
 
     predictor + volume integral          (local)
-    pack the two boundary layers' face traces -> exchange with the lower / upper rank
-    unpack into the ghost cells            -> Rusanov on every face, ghosts included
+    pack the two boundary layers' face traces -> start the exchange with the lower / upper rank
+    Rusanov on the faces between own cells (overlaps the exchange)
+    finish the exchange, unpack into the ghost cells -> Rusanov on the ghost cells' faces
     surface integral + update + local CFL  -> all-reduce(min) of the time step
     advance t and dt
 
@@ -35,16 +36,29 @@ def slab_partition(n, world, rank):
     return first, count
 
 
-def halo_exchange(send_lo, send_hi, recv_lo, recv_hi, rank, world, group=None):
-    """recv_lo <- lower rank's send_hi; recv_hi <- upper rank's send_lo (periodic ring)."""
+def start_halo_exchange(send_lo, send_hi, recv_lo, recv_hi, rank, world, group=None):
+    """Starts recv_lo <- lower rank's send_hi and recv_hi <- upper rank's send_lo (periodic ring);
+    returns the requests. With NCCL the transfers are ordered after the current stream's work and
+    run on NCCL's stream, so kernels enqueued afterwards overlap them."""
     up = (rank + 1) % world
     down = (rank - 1) % world
     ops = [dist.P2POp(dist.isend, send_hi, up, group, 1),
            dist.P2POp(dist.isend, send_lo, down, group, 2),
            dist.P2POp(dist.irecv, recv_lo, down, group, 1),
            dist.P2POp(dist.irecv, recv_hi, up, group, 2)]
-    for req in dist.batch_isend_irecv(ops):
+    return dist.batch_isend_irecv(ops)
+
+
+def finish_halo_exchange(reqs):
+    """With NCCL, Work.wait() makes the current stream wait for the transfers (no host wait); with
+    gloo it waits on the host."""
+    for req in reqs:
         req.wait()
+
+
+def halo_exchange(send_lo, send_hi, recv_lo, recv_hi, rank, world, group=None):
+    """recv_lo <- lower rank's send_hi; recv_hi <- upper rank's send_lo (periodic ring)."""
+    finish_halo_exchange(start_halo_exchange(send_lo, send_hi, recv_lo, recv_hi, rank, world, group))
 
 
 def min_all_reduce(buf, group=None):
@@ -111,10 +125,13 @@ class SlabPatch:
             with torch.cuda.stream(self.stream):
                 p.step_phase(exa.PHASE_PREDICTOR, fixed_dt)
                 p.halo_pack(self.send_lo, self.send_hi)
-                halo_exchange(self.send_lo, self.send_hi, self.recv_lo, self.recv_hi, self.rank, self.world,
-                              self.group)
+                reqs = start_halo_exchange(self.send_lo, self.send_hi, self.recv_lo, self.recv_hi, self.rank,
+                                           self.world, self.group)
+                # the faces between this rank's own cells while the traces are in flight
+                p.step_phase(exa.PHASE_FACES_INTERIOR, fixed_dt)
+                finish_halo_exchange(reqs)
                 p.halo_unpack(self.recv_lo, self.recv_hi)
-                p.step_phase(exa.PHASE_FACES, fixed_dt)
+                p.step_phase(exa.PHASE_FACES_HALO, fixed_dt)
                 p.step_phase(exa.PHASE_UPDATE, fixed_dt)
                 if not fixed_dt > 0:
                     p.dt_next_copy(self.dtbuf, 0)

@@ -122,6 +122,16 @@ def main():
         out.append("  static __device__ __forceinline__ float Kxif(int i, int j) { return c_Kxif_%d[i][j]; }" % o)
         out.append("  static __device__ __forceinline__ float iK1f(int i, int j) { return c_iK1f_%d[i][j]; }" % o)
         out.append("};")
+    # host copies of the quadrature (exa_quadrature), for glue code that evaluates user hooks
+    out.append("// host-side quadrature nodes and weights, [order][node] (zero-padded to 10 entries)")
+    rows_n, rows_w = [], []
+    for o in range(1, MAX_ORDER + 1):
+        t = operators(o)
+        pad = [0.0] * (MAX_ORDER + 1 - (o + 1))
+        rows_n.append("{%s}" % ", ".join(fmt(v) for v in list(t["nodes"]) + pad))
+        rows_w.append("{%s}" % ", ".join(fmt(v) for v in list(t["weights"]) + pad))
+    out.append("static const double h_nodes[%d][%d] = {%s};" % (MAX_ORDER, MAX_ORDER + 1, ", ".join(rows_n)))
+    out.append("static const double h_weights[%d][%d] = {%s};" % (MAX_ORDER, MAX_ORDER + 1, ", ".join(rows_w)))
     out.append("}  // namespace exa")
     path = os.path.join(HERE, "csrc", "exa_tables.cuh")
     with open(path, "w") as f:

@@ -112,6 +112,10 @@ typedef struct {
 
 const char* exa_last_error(void);
 const char* exa_version(void);
+/* Gauss-Legendre nodes and weights on [0,1] of the given order (order+1 values each; the
+ * kernels::legendre tables of GaussLegendreBasis.csnippet), for host glue that evaluates user hooks
+ * at node positions. Host only. */
+int exa_quadrature(int order, double* nodes, double* weights);
 
 /* ---- solver handle -------------------------------------------------------------------- */
 int exa_solver_create(const exa_solver_config* cfg, exa_solver** out);
@@ -127,6 +131,13 @@ int exa_solver_status(exa_solver* s, unsigned* bits);
 int exa_solver_set_predictor_variant(exa_solver* s, int variant);
 /* the form the solver's next predictor launch uses on the current device */
 int exa_solver_predictor_variant(exa_solver* s, int* variant);
+/* Launch form of the HBM-bound kernels of a step, the surface integral + update + CFL kernel and
+ * the Rusanov kernel: 0 one cell group per CTA / one face per warp with per-thread loads; 1 or -1
+ * (the default) persistent CTAs / warps that move whole cell and face blocks by bulk copy
+ * (cp.async.bulk), double-buffered, where the block sizes are multiples of 16 bytes and the arrays
+ * 16-byte aligned (otherwise the first form runs). The Rusanov form is a setting of the
+ * instantiation, shared by its solvers. */
+int exa_solver_set_update_variant(exa_solver* s, int variant);
 
 /* ---- batched kernels on caller-owned device memory ------------------------------------
  * `dx` is the cell size (DIM doubles, host memory) shared by all `ncells` cells; `dt` a host
@@ -228,6 +239,11 @@ int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const doub
                                double t, double dt, const double* dx, int direction);
 /* surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90). */
 int exa_surfaceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, const double* dx);
+/* faceIntegralNonlinear (3d/faceIntegralNonlinear.cpph:21-103): one face block lFhbnd ([a][b][V])
+ * of face 2*direction+orientation, the per-face form the engine's glue calls (...Implementation
+ * .template:247-285). */
+int exa_faceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd, int direction, int orientation,
+                              const double* dx);
 /* solutionUpdate (3d/solutionUpdate.cpph:28-67). */
 int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const double* lduh, double dt);
 /* stableTimeStepSize (3d/stableTimeStepSize.cpph:14-62); returns the value in *dt. */
@@ -296,8 +312,20 @@ int exa_patch_adjust_solution(exa_patch* p);
  * axis; one step is
  *   PREDICTOR -> halo_pack -> (exchange with the two neighbours) -> halo_unpack -> FACES ->
  *   UPDATE -> (all-reduce min of dt_next, exa_patch_dt_next_copy) -> ADVANCE.
+ * FACES splits into FACES_INTERIOR (faces between real cells and domain faces, which do not need
+ * the neighbours' traces and can run while the exchange is in flight) and FACES_HALO (the faces
+ * of the ghost cells, after halo_unpack):
+ *   PREDICTOR -> halo_pack -> (start the exchange) -> FACES_INTERIOR -> (finish the exchange) ->
+ *   halo_unpack -> FACES_HALO -> UPDATE -> ...
  * exa_patch_step refuses halo patches. All calls enqueue on the patch stream. */
-enum { EXA_PHASE_PREDICTOR = 0, EXA_PHASE_FACES = 1, EXA_PHASE_UPDATE = 2, EXA_PHASE_ADVANCE = 3 };
+enum {
+  EXA_PHASE_PREDICTOR = 0,
+  EXA_PHASE_FACES = 1,
+  EXA_PHASE_UPDATE = 2,
+  EXA_PHASE_ADVANCE = 3,
+  EXA_PHASE_FACES_INTERIOR = 4,
+  EXA_PHASE_FACES_HALO = 5
+};
 int exa_patch_step_phase(exa_patch* p, int phase, double fixed_dt);
 /* doubles in one side's exchange buffer: [lQhbnd face blocks of the layer][lFhbnd face blocks] */
 long long exa_patch_halo_doubles(const exa_patch* p);

@@ -89,6 +89,41 @@ def test_golden3d_predictor_riemann_update(exa):
     assert s.status() == 0
 
 
+def test_cell_integrals_vs_golden_and_reference(exa):
+    """The per-cell volume, surface and face integrals (the generic signatures on host pointers):
+    the reference's surface-integral known answers (GenericEulerKernelTest3D.cpp:277-319), and the
+    compiled reference kernels on random blocks, 3D N=3 and 5 and 2D N=3."""
+    g = np.load(os.path.join(GOLD, "generic_euler_3d.npz"))
+    s = exa.Solver(exa.PDE_EULER, 3, 3, npar=1)
+    lF = np.zeros(480)
+    for i in range(0, 80, 5):
+        lF[0 + i + 1] = lF[80 + i + 1] = 1.0
+        lF[160 + i + 2] = lF[240 + i + 2] = 1.0
+        lF[320 + i + 3] = lF[400 + i + 3] = 1.0
+    out = s.surface_integral_cell(np.arange(320) / 10.0, lF, 0.1)
+    assert np.max(np.abs(out - g["testSurfaceIntegralNonlinear.lduh"])) < EPS_REF
+    from pyoracle import RefKernels
+    rng = np.random.default_rng(31)
+    for dim, order in ((3, 3), (3, 5), (2, 3)):
+        try:
+            ref = RefKernels(dim, order)
+        except (FileNotFoundError, AttributeError, OSError) as e:
+            pytest.skip("reference kernels not built: %s" % e)
+        s = exa.Solver(exa.PDE_EULER, dim, order)
+        n = order + 1
+        nd, nf = n ** dim, n ** (dim - 1)
+        dx = np.array([0.031, 0.027, 0.022])[:dim]
+        lFhi = rng.normal(size=(dim + 1) * nd * 5)
+        assert rel(s.volume_integral_cell(lFhi, dx), ref.volume(lFhi, dx)) < 1e-14
+        lduh = rng.normal(size=nd * 5)
+        lFhbnd = rng.normal(size=2 * dim * nf * 5)
+        assert rel(s.surface_integral_cell(lduh, lFhbnd, dx), ref.surface(lduh, lFhbnd, dx)) < 1e-14
+        for d in range(dim):
+            for ori in (0, 1):
+                face = lFhbnd[(2 * d + ori) * nf * 5:(2 * d + ori + 1) * nf * 5]
+                assert rel(s.face_integral_cell(lduh, face, d, ori, dx), ref.face(lduh, face, d, ori, dx)) < 1e-14
+
+
 def test_golden2d_predictor_riemann_update(exa):
     g = np.load(os.path.join(GOLD, "generic_euler_2d.npz"))
     s = exa.Solver(exa.PDE_EULER, 2, 3, npar=1)
@@ -350,6 +385,53 @@ def test_mixed_precision_linear_waves_source_vs_fp64_oracle(exa, name, order, va
         p.close()
 
 
+@pytest.mark.parametrize("case", ["euler3d_n5", "euler2d_n3", "swe_grids", "acoustic_outflow"])
+def test_update_launch_forms_agree(exa, case):
+    """The update kernel's two launch forms (per-thread loads; persistent CTAs moving whole cell
+    blocks by bulk copy) give bit-identical steps, equal to the oracle."""
+    import exa_scenarios as sc
+    from pyoracle import PDE_ACOUSTIC
+    rng = np.random.default_rng(5)
+    if case == "euler3d_n5":
+        mk = lambda: exa.Solver(exa.PDE_EULER, 3, 5)
+        specs = [dict(ncell=(4, 3, 5), size=[1.0, 0.8, 1.1])]
+        luh0 = euler_cells(rng, 60, 216, amp=0.04).reshape(-1)
+        ref = luh0.copy()
+        Oracle(3, 5).run(ref, (4, 3, 5), [1.0, 0.8, 1.1], 3)
+    elif case == "euler2d_n3":
+        mk = lambda: exa.Solver(exa.PDE_EULER, 2, 3)
+        specs = [dict(ncell=(11, 9), size=[1.0, 0.9], bc=exa.BC_WALL)]
+        luh0 = euler_cells(rng, 99, 16, amp=0.04, dim=2).reshape(-1)
+        ref = luh0.copy()
+        Oracle(2, 3).run(ref, (11, 9), [1.0, 0.9], 3, walls=True)
+    elif case == "swe_grids":
+        mk = lambda: exa.Solver(exa.PDE_SWE, 2, 4)
+        specs, states = sc.swe_batched(ngrids=3, order=4, seed=9, nmin=5, nmax=9)
+        luh0 = np.concatenate(states)
+        ref = None
+    else:
+        mk = lambda: exa.Solver(PDE_ACOUSTIC, 3, 4, npar=2)
+        specs = [dict(ncell=(4, 3, 3), size=[1.0, 0.75, 0.75], bc=exa.BC_OUTFLOW)]
+        luh0 = sc.layered_medium("acoustic", (4, 3, 3), [1.0, 0.75, 0.75], 4, seed=1)
+        lv = luh0.reshape(-1, 6)
+        lv[:, :4] += 0.01 * rng.normal(size=(lv.shape[0], 4))
+        ref = luh0.copy()
+        Oracle(3, 4, PDE_ACOUSTIC).run(ref, (4, 3, 3), [1.0, 0.75, 0.75], 3, walls=3)
+    outs = []
+    for variant in (0, 1):
+        s = mk()
+        s.set_update_variant(variant)
+        p = exa.Patch(s, specs)
+        p.set_solution(luh0)
+        p.step(3)
+        outs.append(p.get_solution())
+        assert p.status() == 0
+        p.close()
+    assert np.array_equal(outs[0], outs[1])
+    if ref is not None:
+        assert rel(outs[1], ref) < TOL
+
+
 @pytest.mark.parametrize("dim,order,ncell", [(3, 5, (5, 4, 3)), (2, 3, (9, 7)), (3, 3, (6, 5, 4))])
 def test_fp64_predictor_launch_forms_agree(exa, dim, order, ncell):
     """The FP64 predictor's two launch forms (one cell group per CTA; persistent CTAs with a
@@ -498,6 +580,67 @@ def test_two_slabs_with_halo_match_whole_grid(exa, torch, nz, split):
     got = np.concatenate([p.get_solution() for p, _ in slabs])
     assert rel(got, ref) < TOL
     assert slabs[0][0].time()[0][0] == whole.time()[0][0]
+
+
+@pytest.mark.parametrize("nz,split", [(6, 3), (7, 4)])
+def test_two_slabs_interior_faces_during_exchange_vs_oracle(exa, torch, nz, split):
+    """The multi-GPU step order, emulated with two slabs on one GPU: the faces between each slab's
+    own cells run before the exchange buffers are delivered (FACES_INTERIOR), the ghost cells'
+    faces after the unpack (FACES_HALO). The joined slabs match the oracle's whole periodic grid at
+    1e-12 after 3 CFL steps, with the oracle's time."""
+    rng = np.random.default_rng(12)
+    order, nx, ny = 3, 4, 3
+    nd = (order + 1) ** 3
+    size = [1.0, 0.8, 1.3]
+    hz = size[2] / nz
+    luh0 = euler_cells(rng, nx * ny * nz, nd, amp=0.05).reshape(-1)
+    ref = luh0.copy()
+    t_ref, _, _ = Oracle(3, order).run(ref, (nx, ny, nz), size, 3)
+    s = exa.Solver(exa.PDE_EULER, 3, order)
+    layer = nx * ny * nd * 5
+    slabs = []
+    for first, count in ((0, split), (split, nz - split)):
+        p = exa.Patch(s, [dict(ncell=(nx, ny, count), size=[size[0], size[1], count * hz],
+                               offset=[0, 0, first * hz], bc=[exa.BC_PERIODIC, exa.BC_PERIODIC, exa.BC_HALO])])
+        p.set_solution(luh0[first * layer:(first + count) * layer])
+        nh = p.halo_doubles()
+        slabs.append((p, {k: torch.zeros(nh, dtype=torch.float64, device="cuda") for k in ("slo", "shi", "rlo", "rhi")}))
+    dtb = [torch.zeros(1, dtype=torch.float64, device="cuda") for _ in slabs]
+    for (p, _), b in zip(slabs, dtb):
+        p.dt_copy(b, 0)
+    torch.cuda.synchronize()
+    m = torch.minimum(dtb[0], dtb[1])
+    for (p, _), b in zip(slabs, dtb):
+        b.copy_(m)
+        p.dt_copy(b, 1)
+    for _ in range(3):
+        for p, bf in slabs:
+            p.step_phase(exa.PHASE_PREDICTOR)
+            p.halo_pack(bf["slo"], bf["shi"])
+            p.step_phase(exa.PHASE_FACES_INTERIOR)  # before the neighbours' traces exist
+        torch.cuda.synchronize()
+        (pa, a), (pb, b) = slabs
+        a["rlo"].copy_(b["shi"]); a["rhi"].copy_(b["slo"])
+        b["rlo"].copy_(a["shi"]); b["rhi"].copy_(a["slo"])
+        torch.cuda.synchronize()
+        for p, bf in slabs:
+            p.halo_unpack(bf["rlo"], bf["rhi"])
+            p.step_phase(exa.PHASE_FACES_HALO)
+            p.step_phase(exa.PHASE_UPDATE)
+        for (p, _), bb in zip(slabs, dtb):
+            p.dt_next_copy(bb, 0)
+        torch.cuda.synchronize()
+        m = torch.minimum(dtb[0], dtb[1])
+        for (p, _), bb in zip(slabs, dtb):
+            bb.copy_(m)
+            p.dt_next_copy(bb, 1)
+            p.step_phase(exa.PHASE_ADVANCE)
+    got = np.concatenate([p.get_solution() for p, _ in slabs])
+    assert rel(got, ref) < TOL
+    assert abs(slabs[1][0].time()[0][0] - t_ref) <= 1e-13 * t_ref
+    for p, _ in slabs:
+        assert p.status() == 0
+        p.close()
 
 
 # ------------------------------------------------------------------------------------------
