@@ -60,6 +60,11 @@ def parse():
     ap.add_argument("--elastic-active", action="store_true",
                     help="elastic3d: start from a smooth random velocity field so that every cell iterates")
     ap.add_argument("--fd-directions", type=int, default=16, help="acoustic_adjoint: finite-difference checks")
+    ap.add_argument("--predictor-variant", type=int, default=-1, choices=[-1, 0, 1],
+                    help="predictor launch form: -1 the one measured as faster on the first state (default), "
+                         "0 one cell group per CTA, 1 persistent (mixed: 2 or 3 CTAs per SM)")
+    ap.add_argument("--update-variant", type=int, default=-1, choices=[-1, 0, 1],
+                    help="launch form of the Rusanov and update kernels: 0 per-thread loads, 1/-1 bulk copies")
     ap.add_argument("--no-workloads", action="store_true",
                     help="euler3d at N=1: skip the short runs of the other configurations (the workloads record)")
     return ap.parse_args()
@@ -607,6 +612,8 @@ def main():
 
     precision = exa.PREC_MIXED if args.precision == "mixed" else exa.PREC_FP64
     solver = exa.Solver(exa.PDE_EULER, 3, ORDER, precision=precision)
+    solver.set_update_variant(args.update_variant)
+    solver.predictor_variant = args.predictor_variant
     # every rank owns one 81^3 slab of an 81 x 81 x (81 N) periodic grid (dx = 1/81 everywhere)
     from exa_distributed import SlabPatch
     slab = SlabPatch(solver, (ncell[0], ncell[1], ncell[2] * world), [1.0, 1.0, float(world)], rank=rank,
@@ -703,6 +710,24 @@ def main():
     e1.synchronize()
     pred_ms = e0.elapsed_time(e1) / reps
     mean_sweeps = float(pic.double().mean().item())
+    # the HBM-bound kernels alone on the patch (Rusanov on every face; surface integral + update +
+    # CFL), events on the patch stream; the state advances, nothing reads it afterwards
+    phase_ms = {}
+    for name, ph in (("riemann", exa.PHASE_FACES), ("update", exa.PHASE_UPDATE)):
+        e0.record(stream)
+        for _ in range(reps):
+            patch.step_phase(ph, 0.0)
+        e1.record(stream)
+        e1.synchronize()
+        phase_ms[name] = e0.elapsed_time(e1) / reps
+    nface = 3 * cells
+    hbm_peak = peaks()[0].get("hbm_gbs")
+    hbm = {"riemann": {"ms": phase_ms["riemann"], "algorithmic_bytes": nface * 8640.0,
+                       "gbs": nface * 8640.0 / (phase_ms["riemann"] * 1e-3) / 1e9},
+           "update": {"ms": phase_ms["update"], "algorithmic_bytes": cells * 34560.0,
+                      "gbs": cells * 34560.0 / (phase_ms["update"] * 1e-3) / 1e9}}
+    for v in hbm.values():
+        v["frac_of_measured_hbm"] = v["gbs"] / hbm_peak if hbm_peak else None
     fp64_peak = fp64_peak_tflops()
     flops_launch = cells * (395280.0 * mean_sweeps + 116640.0)
     achieved = flops_launch / (pred_ms * 1e-3) / 1e12
@@ -772,6 +797,10 @@ def main():
                      "hbm_gbs_of_launch": cells * PRED_BYTES_PER_CELL / (pred_ms * 1e-3) / 1e9,
                      "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},
         "gpu_launches": K * 4,
+        "predictor_launch_form": solver.predictor_variant,
+        "hbm_kernels": dict(hbm, launch_form="bulk copies" if args.update_variant != 0 else "per-thread loads",
+                            bytes="Rusanov 8,640 B per face (2 x (Q + F) in, 2 x F out); update 34,560 B per "
+                                  "cell (luh, lduh, lFhbnd in; luh out)"),
         "clocks": clocks.summary(),
     }
     if e2e:

@@ -144,6 +144,9 @@ int exa_pde_available(int pde, int dim, int order, int npar) {
 int exa_register_pde(int pde, int dim, int order, int npar, void* ops) {
   exa::Ops* o = static_cast<exa::Ops*>(ops);
   if (!o || pde < EXA_PDE_USER_BASE) return fail(EXA_ERR_INVALID, "user PDE ids start at EXA_PDE_USER_BASE");
+  if (o->abi != exa::Ops::kAbi)
+    return fail(EXA_ERR_INVALID, "the application library was compiled against another version of "
+                                 "exa_ops.cuh: rebuild it");
   if (o->dim != dim || o->order != order || o->npar != npar)
     return fail(EXA_ERR_INVALID, "registration arguments do not match the instantiation");
   std::lock_guard<std::mutex> lk(exa::user_mu());
