@@ -77,6 +77,28 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
   return true;
 }
 
+// L2 eviction priorities for plain global loads and stores (createpolicy + .L2::cache_hint): a
+// CTA's scratch that is re-read every sweep is kept (evict_last), data read once is let go first
+__device__ __forceinline__ uint64_t l2_policy_evict_last() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint64_t l2_policy_evict_first() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// volatile: kept in program order with the other hinted accesses (the scratch is updated in place)
+__device__ __forceinline__ double ld_hint(const double* a, uint64_t pol) {
+  double v;
+  asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_hint(double* a, double v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f64 [%0], %1, %2;" ::"l"(a), "d"(v), "l"(pol) : "memory");
+}
+
 // a bulk copy that has not completed after this long is reported (EXA_ST_TIMEOUT), never waited
 // for indefinitely
 constexpr uint64_t kBulkWaitLimitNs = 2000000000ull;

@@ -103,8 +103,9 @@ predictor_streamed_kernel(CellArgs a) {
     const double& iweight = u[D + 1];  // 1 / w_p
     {
       const double* luh = a.luh + (size_t)cell * nd * D + (size_t)(live_node ? p : 0) * D;
+      const uint64_t once = l2_policy_evict_first();  // luh is read once per step
 #pragma unroll
-      for (int m = 0; m < D; m++) u[m] = live_node ? luh[m] : 1.0;
+      for (int m = 0; m < D; m++) u[m] = live_node ? ld_hint(luh + m, once) : 1.0;
     }
     // point source (algebraicSource at x_p, t + node_i dt)
     bool srcOn = false;
@@ -171,6 +172,8 @@ predictor_streamed_kernel(CellArgs a) {
     double* qn = slot + slab;      // rhs slices (scaled by 1/w_p), then the new iterate
     // entry (t, m) of this thread's node in a slab
     auto at = [&](int t, int m) -> size_t { return ((size_t)t * V + m) * nd + p; };
+    // the slot is re-read every sweep: ask L2 to keep it over the streamed luh and outputs
+    const uint64_t keep = l2_policy_evict_last();
     const int maxIter = a.max_picard > 0 ? a.max_picard : S::maxSweeps;
     int sweeps = 0;
     bool last_old_is_luh = true;   // the last sweep started from lQi = luh
@@ -207,7 +210,7 @@ predictor_streamed_kernel(CellArgs a) {
               if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
               const double dl = q1 - um;
               res = fma(dl, dl, res);
-              qn[at(t, m)] = q1;
+              st_hint(qn + at(t, m), q1, keep);
             }
           }
         }
@@ -216,7 +219,7 @@ predictor_streamed_kernel(CellArgs a) {
         for (int i = 0; i < n; i++) {
           double q[D];
 #pragma unroll
-          for (int m = 0; m < D; m++) q[m] = (m < V && live_node) ? qo[at(i, m)] : u[m];
+          for (int m = 0; m < D; m++) q[m] = (m < V && live_node) ? ld_hint(qo + at(i, m), keep) : u[m];
           store_flux(q);
           __syncthreads();
           contract(G::weights(i));
@@ -230,7 +233,7 @@ predictor_streamed_kernel(CellArgs a) {
 #pragma unroll
               for (int d = 0; d < DIM; d++) rhs -= sF[(d * V + m) * BS + off[d]];
               if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * s_cd[0] * si;
-              R[at(i, m)] = iweight * rhs;
+              st_hint(R + at(i, m), iweight * rhs, keep);
             }
           }
           // no barrier: the next phase 1 rewrites only this thread's own flux slots, which this
@@ -247,8 +250,8 @@ predictor_streamed_kernel(CellArgs a) {
           double r[n], ol[n];
 #pragma unroll
           for (int i = 0; i < n; i++) {
-            r[i] = qn[at(i, m)];
-            ol[i] = qo[at(i, m)];
+            r[i] = ld_hint(qn + at(i, m), keep);
+            ol[i] = ld_hint(qo + at(i, m), keep);
           }
 #pragma unroll
           for (int t = 0; t < n; t++) {
@@ -257,7 +260,7 @@ predictor_streamed_kernel(CellArgs a) {
             for (int i = 0; i < n; i++) q = fma(r[i], G::iK1(t, i), q);
             const double dl = q - ol[t];
             res = fma(dl, dl, res);
-            qn[at(t, m)] = q;
+            st_hint(qn + at(t, m), q, keep);
           }
         }
       }
@@ -297,13 +300,13 @@ predictor_streamed_kernel(CellArgs a) {
       for (int m = 0; m < D; m++) {
         double acc = 0.0;
 #pragma unroll
-        for (int t = 0; t < n; t++) acc = fma(m < V ? qn[at(t, m)] : u[m], G::weights(t), acc);
+        for (int t = 0; t < n; t++) acc = fma(m < V ? ld_hint(qn + at(t, m), keep) : u[m], G::weights(t), acc);
         qh[m] = acc;
       }
       if (a.ex_lQi) {
         double* e = a.ex_lQi + (size_t)cell * nd * n * D + (size_t)p * n * D;
         for (int t = 0; t < n; t++)
-          for (int m = 0; m < D; m++) e[t * D + m] = m < V ? qn[at(t, m)] : u[m];
+          for (int m = 0; m < D; m++) e[t * D + m] = m < V ? ld_hint(qn + at(t, m), keep) : u[m];
       }
       if (a.ex_lQhi)
         for (int m = 0; m < D; m++) a.ex_lQhi[(size_t)cell * nd * D + p * D + m] = qh[m];
@@ -315,7 +318,7 @@ predictor_streamed_kernel(CellArgs a) {
       for (int i = 0; i < n; i++) {
         double q[D], F[DIM * V];
 #pragma unroll
-        for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? qo[at(i, m)] : u[m];
+        for (int m = 0; m < D; m++) q[m] = (m < V && !last_old_is_luh) ? ld_hint(qo + at(i, m), keep) : u[m];
         PDE::template flux<DIM>(q, F);
         const double wi = G::weights(i);
 #pragma unroll
