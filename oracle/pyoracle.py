@@ -227,6 +227,53 @@ class RefKernels:
         return t.value, dts, (pic.reshape(nsteps, nc) if pic is not None else None)
 
 
+class RefLinear:
+    """The reference's linear generic kernels (Cauchy-Kowalewski predictor, linear Riemann solver,
+    delta-distribution point source) with the PDE terms of its own linear applications: "elastic"
+    (ElasticWave3D: v1 v2 v3 s11 s22 s33 s12 s13 s23 + rho cp cs) or "acoustic" (acousticwaveCPP:
+    p, u1, u2, u3 with unit density and speed, u = minus the flux-form velocity). 3D, orders 3, 4."""
+
+    def __init__(self, pde, order, source=None):
+        """source: (x, y, z, f0, t0, amplitude, -, variable): a delta at (x, y, z) with amplitude
+        times the Ricker wavelet of peak frequency f0 delayed by t0 on `variable`, or None."""
+        path = os.path.join(HERE, "_ref", "libexaref3d.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.prefix = "exalin_%s_o%d" % (pde, order)
+        if not hasattr(self.lib, self.prefix + "_run"):
+            raise AttributeError("instantiation %s not built" % self.prefix)
+        self.elastic = pde == "elastic"
+        self.v, self.npar = (9, 3) if self.elastic else (4, 0)
+        self.D, self.n = self.v + self.npar, order + 1
+        src = (ctypes.c_double * 8)(*(list(source) if source is not None else [0, 0, 0, 0, 0, 0, 1, 0]))
+        self.lib.exaref_set_source(src, 1 if source is not None else 0)
+
+    def terms(self, Q, G):
+        """M(Q) (F_d(G_d) + B_d(G)) for d = 0, 1, 2: the d-th term of -dQ/dt for a field with state Q
+        (parameters included) and per-direction gradients G[d] of the variables."""
+        out = np.zeros((3, self.v))
+        fn = self.lib.exalin_elastic_terms if self.elastic else self.lib.exalin_acoustic_terms
+        fn(_p(_f64(Q)), _p(_f64(np.asarray(G).reshape(3, self.v))), _p(out))
+        return out
+
+    def eigenvalues(self, Q):
+        out = np.zeros(self.v)
+        self.lib.exalin_eigenvalues(1 if self.elastic else 0, _p(_f64(Q)), _p(out))
+        return out
+
+    def run(self, luh, ncell, size, nsteps, offset=(0.0, 0.0, 0.0), t0=0.0, fixed_dt=0.0, nthreads=0):
+        """Periodic uniform patch, luh [cells][n^3][D] updated in place; returns (t, dts)."""
+        luh = np.ascontiguousarray(luh, dtype=np.float64)
+        dts = np.zeros(nsteps)
+        t = ctypes.c_double(0.0)
+        nce = np.array(list(ncell), dtype=np.int32)
+        self.lib[self.prefix + "_run"](_p(nce), _p(_f64(offset)), _p(_f64(size)), _p(luh), int(nsteps),
+                                       ctypes.c_double(t0), ctypes.c_double(fixed_dt), ctypes.byref(t), _p(dts),
+                                       int(nthreads))
+        return t.value, dts
+
+
 class KGKernels:
     """The reference's generated optimised kernels (KernelGenerator, plain-loop mode) for the Euler
     application, 3D, order 3 or 5 (oracle/_ref/libkg_euler_o{3,5}.so, built by ``make -C oracle kg``)

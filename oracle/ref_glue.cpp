@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -436,7 +437,294 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
   return 0;
 }
 
+#if DIMENSIONS == 3
+// ---------------------------------------------------------------------------------------------
+// Linear ADER-DG: the reference's linear generic kernels (3d/spaceTimePredictorLinear.cpph:30-647,
+// Cauchy-Kowalewski; 3d/riemannSolverLinear.cpph:22-160; 3d/volumeIntegralLinear.cpph,
+// 3d/surfaceIntegralLinear.cpph; 3d/deltaDistribution.cpph for point sources) with the PDE terms of
+// the reference's own linear applications, in the pointer-array form the linear kernels call
+// (AbstractGenericADERDGSolverImplementation.template:473-480). A second, independent scheme for the
+// acoustic and elastic systems: the nonlinear path here integrates the same physics with a Picard
+// predictor, Rusanov fluxes and flux-form functors.
+//
+// LinElastic: ApplicationExamples/Linear/ElasticWave3D/MyElasticWaveSolver.cpp, eigenvalues
+// :190-208, flux :211-252, nonConservativeProduct :255-297, multiplyMaterialParameterMatrix
+// :331-381 (variables v1 v2 v3 s11 s22 s33 s12 s13 s23, parameters rho cp cs). That file does not
+// compile against its own header (riemannSolver is declared with a lengthScale argument in
+// MyElasticWaveSolver.h and defined without one at :383), so its PDE terms are restated here.
+// LinAcoustic: ApplicationExamples/AcousticWave/acousticwaveCPP/MyAcousticWaveSolver.cpp,
+// eigenvalues :35-44, flux :46-61 (zero), nonConservativeProduct :97-156 (unit density and sound
+// speed, no parameters; its velocity is minus the flux-form velocity).
+struct LinElastic {
+  static constexpr int NumberOfVariables = 9;
+  static constexpr int NumberOfParameters = 3;
+  static constexpr bool kFlux = true, kNCP = true, kMM = true;
+  static void eigenvalues(const double* const Q, const int, double* const l) {
+    const double cp = Q[10], cs = Q[11];
+    const double e[9] = {cp, cs, cs, -cp, -cs, -cs, 0.0, 0.0, 0.0};
+    std::copy_n(e, 9, l);
+  }
+  static void flux(const double* const Q, double** const F) {
+    const double sxx = Q[3], syy = Q[4], szz = Q[5], sxy = Q[6], sxz = Q[7], syz = Q[8];
+    const double f[3][3] = {{-sxx, -sxy, -sxz}, {-sxy, -syy, -syz}, {-sxz, -syz, -szz}};
+    for (int d = 0; d < 3; d++) {
+      std::fill_n(F[d], 9, 0.0);
+      for (int k = 0; k < 3; k++) F[d][k] = f[d][k];
+    }
+  }
+  static void ncp(const double* const, const double* const* const G, double** const B) {
+    const double ux = G[0][0], vx = G[0][1], wx = G[0][2];
+    const double uy = G[1][0], vy = G[1][1], wy = G[1][2];
+    const double uz = G[2][0], vz = G[2][1], wz = G[2][2];
+    for (int d = 0; d < 3; d++) std::fill_n(B[d], 9, 0.0);
+    B[0][3] = -ux; B[0][6] = -vx; B[0][7] = -wx;
+    B[1][4] = -vy; B[1][6] = -uy; B[1][8] = -wy;
+    B[2][5] = -wz; B[2][7] = -uz; B[2][8] = -vz;
+  }
+  static void mm(const double* const Q, double** const rhs) {
+    const double rho = Q[9], cp = Q[10], cs = Q[11];
+    const double mu = rho * cs * cs;
+    const double lambda = rho * cp * cp - 2 * mu;
+    const double rho_inv = 1.0 / rho;
+    for (int d = 0; d < 3; d++) {
+      double* r = rhs[d];
+      r[0] = rho_inv * r[0];
+      r[1] = rho_inv * r[1];
+      r[2] = rho_inv * r[2];
+      const double lam_temp = lambda * (r[3] + r[4] + r[5]);
+      r[3] = (2 * mu) * r[3] + lam_temp;
+      r[4] = (2 * mu) * r[4] + lam_temp;
+      r[5] = (2 * mu) * r[5] + lam_temp;
+      r[6] = mu * r[6];
+      r[7] = mu * r[7];
+      r[8] = mu * r[8];
+    }
+  }
+};
+
+struct LinAcoustic {
+  static constexpr int NumberOfVariables = 4;
+  static constexpr int NumberOfParameters = 0;
+  static constexpr bool kFlux = false, kNCP = true, kMM = false;
+  static void eigenvalues(const double* const, const int, double* const l) {
+    l[0] = 1.0;
+    l[1] = -1.0;
+    l[2] = 0.0;
+    l[3] = 0.0;
+  }
+  static void flux(const double* const, double** const F) {
+    for (int d = 0; d < 3; d++) std::fill_n(F[d], 4, 0.0);
+  }
+  static void ncp(const double* const, const double* const* const G, double** const B) {
+    for (int d = 0; d < 3; d++) std::fill_n(B[d], 4, 0.0);
+    B[0][0] = -G[0][1];
+    B[0][1] = -G[0][0];
+    B[1][0] = -G[1][2];
+    B[1][2] = -G[1][0];
+    B[2][0] = -G[2][3];
+    B[2][3] = -G[2][0];
+  }
+  static void mm(const double* const, double** const) {}
+};
+
+// One point source at (g_src[0..2]) on variable g_src[7]: amplitude g_src[5] times the Ricker
+// wavelet of peak frequency g_src[3] delayed by g_src[4] -- the time function of the
+// regularised source of the nonlinear path, here as an exact delta distribution in space.
+inline double ricker(double t) {
+  const double pi = 3.14159265358979323846;
+  const double a = pi * g_src[3] * (t - g_src[4]);
+  return (1.0 - 2.0 * a * a) * std::exp(-a * a);
+}
+
+template <class PDE, int ORDER>
+struct LinSolver {
+  static constexpr int Order = ORDER;
+  static constexpr int NumberOfVariables = PDE::NumberOfVariables;
+  static constexpr int NumberOfParameters = PDE::NumberOfParameters;
+  static constexpr int NumberOfPointSources = 1;
+  static constexpr bool UseLobattoBasis = false;
+  static constexpr double CFL = 0.9;
+  static constexpr double PNPM = kPNPM[ORDER];
+  static double** weights;
+  static double** nodes;
+  static double*** dudx;
+  static double*** FCoeff;
+  static kernels::UnivariateFunction** basisFunction;
+  double pointSourceLocation[1][3];
+
+  LinSolver() {
+    for (int d = 0; d < 3; d++) pointSourceLocation[0][d] = g_src[d];
+  }
+  void eigenvalues(const double* const Q, const int d, double* const l) { PDE::eigenvalues(Q, d, l); }
+  void viscousEigenvalues(const double* const, const int, double* const l) { std::fill_n(l, NumberOfVariables, 0.0); }
+  void flux(const double* const Q, double** const F) { PDE::flux(Q, F); }
+  void nonConservativeProduct(const double* const Q, const double* const* const G, double** const B) {
+    PDE::ncp(Q, G, B);
+  }
+  void multiplyMaterialParameterMatrix(const double* const Q, double** const rhs) { PDE::mm(Q, rhs); }
+  void algebraicSource(const tarch::la::Vector<DIMENSIONS, double>&, double, const double* const, double* S) {
+    std::fill_n(S, NumberOfVariables, 0.0);
+  }
+  void pointSource(const double* const, const double* const, const double t, const double, double* const f, int) {
+    std::fill_n(f, NumberOfVariables, 0.0);
+    f[(int)g_src[7]] = g_src[5] * ricker(t);
+  }
+};
+template <class P, int O> double** LinSolver<P, O>::weights = kernels::legendre::weights;
+template <class P, int O> double** LinSolver<P, O>::nodes = kernels::legendre::nodes;
+template <class P, int O> double*** LinSolver<P, O>::dudx = kernels::legendre::dudx;
+template <class P, int O> double*** LinSolver<P, O>::FCoeff = kernels::legendre::FCoeff;
+template <class P, int O> kernels::UnivariateFunction** LinSolver<P, O>::basisFunction = kernels::legendre::basisFunction;
+
+// Periodic uniform patch in the order of the generated glue for linear solvers
+// (AbstractGenericADERDGSolverImplementation.template:114-165 and :296-297): dt = min over cells
+// of stableTimeStepSize (or fixed) -> per cell getPointSources / deltaDistribution, the
+// Cauchy-Kowalewski predictor and the volume integral -> linear Riemann solver on every face ->
+// surface integral + solution update. Cell c = (iz*ny + iy)*nx + ix; an OpenMP loop over cells
+// stands in for the absent Peano scheduler.
+template <class S>
+int run_patch_linear(const int* ncell, const double* offset, const double* size, double* luh_all, int nsteps,
+                     double t0, double fixed_dt, double* t_out, double* dts, int nthreads) {
+  using PDE = typename std::conditional<S::NumberOfVariables == 9, LinElastic, LinAcoustic>::type;
+  constexpr int n = S::Order + 1, v = S::NumberOfVariables, D = v + S::NumberOfParameters;
+  constexpr int nd = n * n * n, nf = n * n;
+  constexpr int sLQi = D * nd * (n + 1), sLFi = 4 * v * nd * n, sGradQ = 3 * v * nd;
+  constexpr int sPSi = v * nd * (n + 1), sPSd = v * nd * n, sLQhi = D * nd, sLFhi = 4 * v * nd;
+  constexpr int sLuh = D * nd, sLduh = v * nd, sQb = 6 * nf * D, sFb = 6 * nf * v;
+  const int nx = ncell[0], ny = ncell[1], nz = ncell[2];
+  const long nc = (long)nx * ny * nz;
+  const double dx[3] = {size[0] / nx, size[1] / ny, size[2] / nz};
+  std::vector<double> lduh(nc * sLduh), lQhbnd(nc * sQb), lFhbnd(nc * sFb);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  auto cellIndex = [&](int ix, int iy, int iz) -> long { return ((long)iz * ny + iy) * nx + ix; };
+  double t = t0;
+  for (int step = 0; step < nsteps; step++) {
+    double dt = std::numeric_limits<double>::max();
+    if (fixed_dt > 0) {
+      dt = fixed_dt;
+    } else {
+#pragma omp parallel for reduction(min : dt) schedule(static)
+      for (long c = 0; c < nc; c++) {
+        S s;
+        dt = std::min(dt, kernels::aderdg::generic::c::stableTimeStepSize<S, false>(s, luh_all + c * sLuh, vec(dx)));
+      }
+    }
+#pragma omp parallel
+    {
+      std::vector<double> lQi(sLQi), lFi(sLFi), gradQ(sGradQ), PSi(sPSi), PSd(sPSd), tmpPSd(sPSd), lQhi(sLQhi),
+          lFhi(sLFhi);
+      S s;
+#pragma omp for schedule(static)
+      for (long c = 0; c < nc; c++) {
+        const int ix = c % nx, iy = (c / nx) % ny, iz = (int)(c / ((long)nx * ny));
+        const double centre[3] = {offset[0] + (ix + 0.5) * dx[0], offset[1] + (iy + 0.5) * dx[1],
+                                  offset[2] + (iz + 0.5) * dx[2]};
+        const double* luh = luh_all + c * sLuh;
+        const auto ctr = vec(centre), cdx = vec(dx);
+        const auto invDx = tarch::la::invertEntries(cdx);
+        std::vector<int>* ps = g_src_active ? kernels::aderdg::generic::c::getPointSources<S>(s, ctr, cdx) : nullptr;
+        if (ps != nullptr) {
+          kernels::aderdg::generic::c::deltaDistribution<S>(s, luh, t, dt, ctr, cdx, ps, PSi.data());
+          kernels::aderdg::generic::c::spaceTimePredictorLinear<true, false, PDE::kFlux, PDE::kNCP, PDE::kMM, S>(
+              s, lQhbnd.data() + c * sQb, lFhbnd.data() + c * sFb, lQi.data(), lFi.data(), gradQ.data(), PSi.data(),
+              PSd.data(), tmpPSd.data(), lQhi.data(), lFhi.data(), luh, ctr, invDx, t, dt);
+        } else {
+          kernels::aderdg::generic::c::spaceTimePredictorLinear<false, false, PDE::kFlux, PDE::kNCP, PDE::kMM, S>(
+              s, lQhbnd.data() + c * sQb, lFhbnd.data() + c * sFb, lQi.data(), lFi.data(), gradQ.data(), PSi.data(),
+              PSd.data(), tmpPSd.data(), lQhi.data(), lFhi.data(), luh, ctr, invDx, t, dt);
+        }
+        kernels::aderdg::generic::c::volumeIntegralLinear<S, false, PDE::kFlux, v, n>(lduh.data() + c * sLduh,
+                                                                                      lFhi.data(), cdx);
+      }
+    }
+    // one direction at a time, so that no two faces write the same cell face
+    for (int d = 0; d < 3; d++) {
+#pragma omp parallel for schedule(static)
+      for (long c = 0; c < nc; c++) {
+        S s;
+        const int ix = c % nx, iy = (c / nx) % ny, iz = (int)(c / ((long)nx * ny));
+        int j[3] = {ix, iy, iz};
+        const int lim = d == 0 ? nx : (d == 1 ? ny : nz);
+        j[d] = (j[d] + 1) % lim;
+        const long c2 = cellIndex(j[0], j[1], j[2]);
+        kernels::aderdg::generic::c::riemannSolverLinear<PDE::kFlux, PDE::kNCP, PDE::kMM, S>(
+            s, lFhbnd.data() + c * sFb + (2 * d + 1) * nf * v, lFhbnd.data() + c2 * sFb + (2 * d) * nf * v,
+            lQhbnd.data() + c * sQb + (2 * d + 1) * nf * D, lQhbnd.data() + c2 * sQb + (2 * d) * nf * D, t, dt, d);
+      }
+    }
+#pragma omp parallel for schedule(static)
+    for (long c = 0; c < nc; c++) {
+      S s;
+      kernels::aderdg::generic::c::surfaceIntegralLinear<S, v, n>(lduh.data() + c * sLduh, lFhbnd.data() + c * sFb,
+                                                                  vec(dx));
+      kernels::aderdg::generic::c::solutionUpdate<S>(s, luh_all + c * sLuh, luh_all + c * sLuh,
+                                                     lduh.data() + c * sLduh, dt);
+    }
+    if (dts) dts[step] = dt;
+    t += dt;
+  }
+  if (t_out) *t_out = t;
+  return 0;
+}
+#endif
+
 }  // namespace exaref
+
+#if DIMENSIONS == 3
+// The reference applications' PDE terms applied to a linear field (state Q with its material
+// parameters, per-direction gradients G[d][0..v)): out[d] = M(Q) (F_d(G_d) + B_d(G)), the d-th
+// term of -dQ/dt in the linear kernels' convention (3d/spaceTimePredictorLinear.cpph:183-345).
+#define EXALIN_DEFINE(NAME, PDE, O)                                                                          \
+  extern "C" int NAME##_run(const int* ncell, const double* offset, const double* size, double* luh,       \
+                            int nsteps, double t0, double fixed_dt, double* t_out, double* dts, int nthreads) { \
+    return exaref::run_patch_linear<exaref::LinSolver<exaref::PDE, O>>(ncell, offset, size, luh, nsteps, t0,  \
+                                                                       fixed_dt, t_out, dts, nthreads);     \
+  }
+EXALIN_DEFINE(exalin_elastic_o3, LinElastic, 3)
+EXALIN_DEFINE(exalin_elastic_o4, LinElastic, 4)
+EXALIN_DEFINE(exalin_acoustic_o3, LinAcoustic, 3)
+EXALIN_DEFINE(exalin_acoustic_o4, LinAcoustic, 4)
+
+template <class PDE>
+static void exalin_terms_impl(const double* Q, const double* G, double* out) {
+  constexpr int v = PDE::NumberOfVariables;
+  double fbuf[3][v], nbuf[3][v];
+  double* F[3] = {fbuf[0], fbuf[1], fbuf[2]};
+  double* B[3] = {nbuf[0], nbuf[1], nbuf[2]};
+  const double* Gp[3] = {G, G + v, G + 2 * v};
+  for (int d = 0; d < 3; d++) {
+    // the flux of the d-th gradient (the flux terms are linear in the variables)
+    double q[v + PDE::NumberOfParameters + 1];
+    for (int m = 0; m < v; m++) q[m] = G[d * v + m];
+    for (int m = v; m < v + PDE::NumberOfParameters; m++) q[m] = Q[m];
+    double tb[3][v];
+    double* T[3] = {tb[0], tb[1], tb[2]};
+    PDE::flux(q, T);
+    std::copy_n(tb[d], v, fbuf[d]);
+  }
+  PDE::ncp(Q, Gp, B);
+  double rbuf[3][v];
+  double* R[3] = {rbuf[0], rbuf[1], rbuf[2]};
+  for (int d = 0; d < 3; d++)
+    for (int m = 0; m < v; m++) rbuf[d][m] = (PDE::kFlux ? fbuf[d][m] : 0.0) + (PDE::kNCP ? nbuf[d][m] : 0.0);
+  if (PDE::kMM) PDE::mm(Q, R);
+  for (int d = 0; d < 3; d++) std::copy_n(rbuf[d], v, out + d * v);
+}
+extern "C" void exalin_elastic_terms(const double* Q, const double* G, double* out) {
+  exalin_terms_impl<exaref::LinElastic>(Q, G, out);
+}
+extern "C" void exalin_acoustic_terms(const double* Q, const double* G, double* out) {
+  exalin_terms_impl<exaref::LinAcoustic>(Q, G, out);
+}
+extern "C" void exalin_eigenvalues(int elastic, const double* Q, double* l) {
+  if (elastic)
+    exaref::LinElastic::eigenvalues(Q, 0, l);
+  else
+    exaref::LinAcoustic::eigenvalues(Q, 0, l);
+}
+#endif
 
 #define EXAREF_S(PDE, O, P, X) exaref::RefSolver<exaref::PDE, O, P, X>
 #define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false, false)
