@@ -70,6 +70,73 @@ def parse():
     return ap.parse_args()
 
 
+def amr_limiter_record(exa, solver, torch, stream, luh_dev, cells, nd, hbm_peak, fp64_peak, reps=5):
+    """The mesh-level and limiter kernels on the benchmark state (CUDA events on `stream`):
+    the discrete maximum principle over every cell, the DG -> FV -> DG projections (P = 11
+    subcells, 2 ghost layers) over a block of cells, and the prolongation of 27 children per coarse
+    cell and their grouped restriction. Algorithmic bytes count every block read or written once."""
+    V = solver.nvar
+    blk = nd * V * 8.0
+    out = {}
+
+    def timed(fn):
+        fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def rec(ms, nbytes, what):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        return {"ms": ms, "algorithmic_bytes": nbytes, "gbs": gbs,
+                "frac_of_measured_hbm": gbs / hbm_peak if hbm_peak else None, "work": what}
+
+    with torch.cuda.stream(stream):
+        nobs = V
+        bmin = torch.full((cells * 6 * nobs,), -1e30, dtype=torch.float64, device="cuda")
+        bmax = torch.full((cells * 6 * nobs,), 1e30, dtype=torch.float64, device="cuda")
+        ok = torch.zeros(cells, dtype=torch.uint8, device="cuda")
+        ms = timed(lambda: solver.limiter_dmp(luh_dev, nobs, 1e-4, 1e-3, bmin, bmax, ok))
+        out["dmp"] = rec(ms, cells * (blk + 2 * 6 * nobs * 8 + 2 * 2 * nobs * 8 + 1),
+                         "%d cells, %d observables (nodes, Lobatto nodes, 11^3 subcell means)" % (cells, nobs))
+        # the projections onto the Gauss-Lobatto nodes (3 n^4 multiply-adds per observable) and
+        # the subcell means (n^3 P + n^2 P^2 + n P^3) bound it, not memory
+        n_, P_ = solver.order + 1, 2 * solver.order + 1
+        fma_cell = nobs * (3 * n_ ** 4 + n_ ** 3 * P_ + n_ ** 2 * P_ ** 2 + n_ * P_ ** 3)
+        tf = 2.0 * fma_cell * cells / (ms * 1e-3) / 1e12
+        out["dmp"].update({"fp64_tflops": tf, "algorithmic_flops": 2.0 * fma_cell * cells,
+                           "frac_of_measured_fp64": tf / fp64_peak if fp64_peak else None})
+        del bmin, bmax, ok
+        nl = min(cells, 32768)
+        ghost = 2
+        lim = torch.zeros(nl * solver.limiter_patch_size(ghost), dtype=torch.float64, device="cuda")
+        part = luh_dev[: nl * nd * V]
+        back = torch.empty_like(part)
+        sub = (2 * solver.order + 1) ** 3 * V * 8.0
+        ms = timed(lambda: solver.limiter_project_on_fv(part, lim, ghost))
+        out["project_on_fv"] = rec(ms, nl * (blk + sub), "%d cells -> 11^3 subcells + 2 ghost layers" % nl)
+        ms = timed(lambda: solver.limiter_project_on_dg(lim, back, ghost))
+        out["project_on_dg"] = rec(ms, nl * (blk + sub), "%d cells" % nl)
+        del lim, back
+        nc = min(cells, 4096)
+        kids = [(i1, i2, i3) for i3 in range(3) for i2 in range(3) for i1 in range(3)]
+        jobs = torch.tensor([[27 * c + k, c, 1, *kids[k]] for c in range(nc) for k in range(27)], dtype=torch.int32,
+                            device="cuda")
+        coarse = luh_dev[: nc * nd * V].clone()
+        fine = torch.empty(27 * nc * nd * V, dtype=torch.float64, device="cuda")
+        ptr = torch.arange(0, 27 * nc + 1, 27, dtype=torch.int32, device="cuda")
+        ms = timed(lambda: solver.amr_volume(exa.AMR_PROLONGATE, fine, coarse, jobs))
+        out["volume_prolongation"] = rec(ms, nc * 28 * blk, "%d coarse cells x 27 children" % nc)
+        ms = timed(lambda: solver.amr_volume(exa.AMR_RESTRICT, fine, coarse, jobs, group_ptr=ptr))
+        out["volume_restriction"] = rec(ms, nc * 29 * blk, "%d coarse cells <- 27 children each" % nc)
+        del coarse, fine, jobs, ptr
+    out["status_bits"] = solver.status()
+    return out
+
+
 def peaks():
     path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -729,6 +796,8 @@ def main():
     for v in hbm.values():
         v["frac_of_measured_hbm"] = v["gbs"] / hbm_peak if hbm_peak else None
     fp64_peak = fp64_peak_tflops()
+    amr_lim = (amr_limiter_record(exa, solver, torch, stream, luh_dev, cells, nd, hbm_peak, fp64_peak)
+               if world == 1 else None)
     flops_launch = cells * (395280.0 * mean_sweeps + 116640.0)
     achieved = flops_launch / (pred_ms * 1e-3) / 1e12
 
@@ -798,6 +867,7 @@ def main():
                      "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},
         "gpu_launches": K * 4,
         "predictor_launch_form": solver.predictor_variant,
+        "amr_limiter_kernels": amr_lim,
         "hbm_kernels": dict(hbm, launch_form="bulk copies" if args.update_variant != 0 else "per-thread loads",
                             bytes="Rusanov 8,640 B per face (2 x (Q + F) in, 2 x F out); update 34,560 B per "
                                   "cell (luh, lduh, lFhbnd in; luh out)"),

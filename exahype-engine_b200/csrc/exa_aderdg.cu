@@ -533,6 +533,277 @@ int exa_stableTimeStepSize(exa_solver* s, const double* luh, const double* dx, d
   return r;
 }
 
+// ---- mesh levels and the limiter ------------------------------------------------------------
+static int amr_call(exa_solver* s, bool face, int mode, double* fQ, double* fF, double* cQ, double* cF, long long nfine,
+                    long long ncoarse, int njobs, const int* jobs, int ngroups, const int* group_ptr, cudaStream_t st) {
+  if (!s) return fail(EXA_ERR_INVALID, "null solver");
+  if (mode < EXA_AMR_PROLONGATE || mode > EXA_AMR_RESTRICT_FLUX || (mode == EXA_AMR_RESTRICT_FLUX && !face))
+    return fail(EXA_ERR_INVALID, "bad mode");
+  if (face && s->cfg.dim < 2) return fail(EXA_ERR_UNSUPPORTED, "faces of a 1D cell");
+  if (njobs < 0 || nfine < 0 || ncoarse < 0 || ngroups < 0) return fail(EXA_ERR_INVALID, "negative size");
+  if (mode != EXA_AMR_RESTRICT || !group_ptr) {
+    group_ptr = nullptr;
+    ngroups = njobs;
+  }
+  if (ngroups == 0) return EXA_OK;
+  if (!jobs) return fail(EXA_ERR_INVALID, "null jobs");
+  const bool needQ = mode != EXA_AMR_RESTRICT_FLUX;
+  if ((needQ && (!fQ || !cQ)) || (face && (!fF || !cF))) return fail(EXA_ERR_INVALID, "null block array");
+  exa::AmrArgs a;
+  memset(&a, 0, sizeof(a));
+  a.mode = mode;
+  if (mode == EXA_AMR_PROLONGATE) {
+    a.outQ = fQ, a.inQ = cQ, a.outF = fF, a.inF = cF;
+  } else {
+    a.outQ = cQ, a.inQ = fQ, a.outF = cF, a.inF = fF;
+  }
+  a.nfine = nfine;
+  a.ncoarse = ncoarse;
+  a.ngroups = ngroups;
+  a.ptr = group_ptr;
+  a.njobs = njobs;
+  a.jobs = jobs;
+  a.status = s->d_status;
+  EXA_CUDA(s->ops->amr(a, face, st));
+  return EXA_OK;
+}
+
+int exa_amr_volume_unknowns(exa_solver* s, int mode, double* luhFine, double* luhCoarse, long long nfine,
+                            long long ncoarse, int njobs, const int* jobs, int ngroups, const int* group_ptr,
+                            void* stream) {
+  return amr_call(s, false, mode, luhFine, nullptr, luhCoarse, nullptr, nfine, ncoarse, njobs, jobs, ngroups,
+                  group_ptr, (cudaStream_t)stream);
+}
+
+int exa_amr_face_unknowns(exa_solver* s, int mode, double* lQhbndFine, double* lFhbndFine, double* lQhbndCoarse,
+                          double* lFhbndCoarse, long long nfine, long long ncoarse, int njobs, const int* jobs,
+                          int ngroups, const int* group_ptr, void* stream) {
+  return amr_call(s, true, mode, lQhbndFine, lFhbndFine, lQhbndCoarse, lFhbndCoarse, nfine, ncoarse, njobs, jobs,
+                  ngroups, group_ptr, (cudaStream_t)stream);
+}
+
+// one job on host arrays: the blocks are copied to the shim scratch, the job checked on the host
+static int amr_shim(exa_solver* s, bool face, int mode, double* fQ, double* fF, double* cQ, double* cF, int levelDelta,
+                    const int* index) {
+  if (!s || !index) return fail(EXA_ERR_INVALID, "null argument");
+  const int axes = face ? s->cfg.dim - 1 : s->cfg.dim;
+  if (levelDelta < 1 || levelDelta > exa::kAmrMaxLevelDelta) return fail(EXA_ERR_INVALID, "level difference out of range");
+  long long span = 1;
+  for (int l = 0; l < levelDelta; l++) span *= 3;
+  int job[6] = {0, 0, levelDelta, 0, 0, 0};
+  for (int r = 0; r < axes; r++) {
+    if (index[r] < 0 || index[r] >= span) return fail(EXA_ERR_INVALID, "subcell index out of range");
+    job[3 + r] = index[r];
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  const exa::Ops& o = *s->ops;
+  const size_t nq = face ? o.sz_qhb / (2 * o.dim) : o.sz_luh, nf = face ? o.sz_fhb / (2 * o.dim) : 0;
+  if (int e = shim_scratch(s, 2 * (nq + nf))) return e;
+  double *dfQ = s->d_scratch, *dcQ = dfQ + nq, *dfF = dcQ + nq, *dcF = dfF + nf;
+  const bool needQ = mode != EXA_AMR_RESTRICT_FLUX;
+  auto up = [&](double* d, const double* h, size_t k) { return cudaMemcpy(d, h, k * sizeof(double), cudaMemcpyHostToDevice); };
+  auto down = [&](double* h, const double* d, size_t k) { return cudaMemcpy(h, d, k * sizeof(double), cudaMemcpyDeviceToHost); };
+  if (needQ && (!fQ || !cQ)) return fail(EXA_ERR_INVALID, "null argument");
+  if (face && (!fF || !cF)) return fail(EXA_ERR_INVALID, "null argument");
+  if (mode == EXA_AMR_PROLONGATE) {
+    EXA_CUDA(up(dcQ, cQ, nq));
+    if (face) EXA_CUDA(up(dcF, cF, nf));
+  } else {
+    if (needQ) EXA_CUDA(up(dfQ, fQ, nq));
+    if (needQ) EXA_CUDA(up(dcQ, cQ, nq));
+    if (face) EXA_CUDA(up(dfF, fF, nf));
+    if (face && mode == EXA_AMR_RESTRICT) EXA_CUDA(up(dcF, cF, nf));
+  }
+  EXA_CUDA(cudaMemcpy(s->d_iscratch, job, sizeof(job), cudaMemcpyHostToDevice));
+  if (int e = amr_call(s, face, mode, needQ ? dfQ : nullptr, face ? dfF : nullptr, needQ ? dcQ : nullptr,
+                       face ? dcF : nullptr, 1, 1, 1, s->d_iscratch, 1, nullptr, 0))
+    return e;
+  if (mode == EXA_AMR_PROLONGATE) {
+    EXA_CUDA(down(fQ, dfQ, nq));
+    if (face) EXA_CUDA(down(fF, dfF, nf));
+  } else {
+    if (needQ) EXA_CUDA(down(cQ, dcQ, nq));
+    if (face) EXA_CUDA(down(cF, dcF, nf));
+  }
+  return EXA_OK;
+}
+
+int exa_volumeUnknownsProlongation(exa_solver* s, double* luhFine, const double* luhCoarse, int coarseGridLevel,
+                                   int fineGridLevel, const int* subcellIndex) {
+  return amr_shim(s, false, EXA_AMR_PROLONGATE, luhFine, nullptr, const_cast<double*>(luhCoarse), nullptr,
+                  fineGridLevel - coarseGridLevel, subcellIndex);
+}
+int exa_volumeUnknownsRestriction(exa_solver* s, double* luhCoarse, const double* luhFine, int coarseGridLevel,
+                                  int fineGridLevel, const int* subcellIndex) {
+  return amr_shim(s, false, EXA_AMR_RESTRICT, const_cast<double*>(luhFine), nullptr, luhCoarse, nullptr,
+                  fineGridLevel - coarseGridLevel, subcellIndex);
+}
+int exa_faceUnknownsProlongation(exa_solver* s, double* lQhbndFine, double* lFhbndFine, const double* lQhbndCoarse,
+                                 const double* lFhbndCoarse, int coarseGridLevel, int fineGridLevel,
+                                 const int* subfaceIndex) {
+  return amr_shim(s, true, EXA_AMR_PROLONGATE, lQhbndFine, lFhbndFine, const_cast<double*>(lQhbndCoarse),
+                  const_cast<double*>(lFhbndCoarse), fineGridLevel - coarseGridLevel, subfaceIndex);
+}
+int exa_faceUnknownsRestriction(exa_solver* s, double* lQhbndCoarse, double* lFhbndCoarse, const double* lQhbndFine,
+                                const double* lFhbndFine, int coarseGridLevel, int fineGridLevel,
+                                const int* subfaceIndex) {
+  return amr_shim(s, true, EXA_AMR_RESTRICT, const_cast<double*>(lQhbndFine), const_cast<double*>(lFhbndFine),
+                  lQhbndCoarse, lFhbndCoarse, fineGridLevel - coarseGridLevel, subfaceIndex);
+}
+int exa_faceFluxRestriction(exa_solver* s, double* lFhbndCoarse, const double* lFhbndFine, const int* subfaceIndex,
+                            int levelDelta) {
+  return amr_shim(s, true, EXA_AMR_RESTRICT_FLUX, nullptr, const_cast<double*>(lFhbndFine), nullptr, lFhbndCoarse,
+                  levelDelta, subfaceIndex);
+}
+
+static int lim_patch(const exa_solver* s, int ghost) {
+  const int E = 2 * s->cfg.order + 1 + 2 * ghost;
+  return s->cfg.dim == 3 ? E * E * E : E * E;
+}
+static int lim_call(exa_solver* s, exa::LimArgs& a, cudaStream_t st) {
+  if (!s) return fail(EXA_ERR_INVALID, "null solver");
+  const int D = s->ops->nvar + s->ops->npar;
+  if (a.ncells < 0) return fail(EXA_ERR_INVALID, "ncells < 0");
+  if (a.ghost < 0 || a.ghost > 4) return fail(EXA_ERR_INVALID, "ghost layer width out of range");
+  if (a.nobs < 0 || a.nobs > std::min(32, D)) return fail(EXA_ERR_INVALID, "observables out of range");
+  if (a.ncells == 0) return EXA_OK;
+  EXA_CUDA(s->ops->limiter(a, st));
+  return EXA_OK;
+}
+static exa::LimArgs lim_args(int op, int ncells, int ghost, int nobs) {
+  exa::LimArgs a;
+  memset(&a, 0, sizeof(a));
+  a.op = op;
+  a.ncells = ncells;
+  a.ghost = ghost;
+  a.nobs = nobs;
+  return a;
+}
+
+int exa_limiter_project_on_fv(exa_solver* s, int ncells, const double* luh, double* lim, int ghost, void* stream) {
+  if (ncells > 0 && (!luh || !lim)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::LimArgs a = lim_args(0, ncells, ghost, 0);
+  a.luh = luh;
+  a.lim_out = lim;
+  return lim_call(s, a, (cudaStream_t)stream);
+}
+int exa_limiter_project_on_dg(exa_solver* s, int ncells, const double* lim, double* luh, int ghost, void* stream) {
+  if (ncells > 0 && (!luh || !lim)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::LimArgs a = lim_args(1, ncells, ghost, 0);
+  a.lim = lim;
+  a.luh_out = luh;
+  return lim_call(s, a, (cudaStream_t)stream);
+}
+int exa_limiter_local_min_max(exa_solver* s, int ncells, const double* luh, int nobs, double* mn, double* mx,
+                              void* stream) {
+  if (ncells > 0 && nobs > 0 && (!luh || !mn || !mx)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::LimArgs a = lim_args(2, ncells, 0, nobs);
+  a.luh = luh;
+  a.mn = mn;
+  a.mx = mx;
+  return lim_call(s, a, (cudaStream_t)stream);
+}
+int exa_limiter_fv_min_max(exa_solver* s, int ncells, const double* lim, int ghost, int nobs, double* mn, double* mx,
+                           void* stream) {
+  if (ncells > 0 && nobs > 0 && (!lim || !mn || !mx)) return fail(EXA_ERR_INVALID, "null argument");
+  exa::LimArgs a = lim_args(3, ncells, ghost, nobs);
+  a.lim = lim;
+  a.mn = mn;
+  a.mx = mx;
+  return lim_call(s, a, (cudaStream_t)stream);
+}
+int exa_limiter_dmp(exa_solver* s, int ncells, const double* luh, int nobs, double relax, double scale, double* bmin,
+                    double* bmax, unsigned char* ok, void* stream) {
+  if (ncells > 0 && (!luh || !ok || (nobs > 0 && (!bmin || !bmax)))) return fail(EXA_ERR_INVALID, "null argument");
+  exa::LimArgs a = lim_args(4, ncells, 0, nobs);
+  a.luh = luh;
+  a.mn = bmin;
+  a.mx = bmax;
+  a.ok = ok;
+  a.relax = relax;
+  a.scale = scale;
+  return lim_call(s, a, (cudaStream_t)stream);
+}
+
+// one cell on host arrays through the shim scratch: [luh][lim][mn][mx][ok]
+static int lim_shim(exa_solver* s, int op, const double* luh_in, double* luh_out, const double* lim_in, double* lim_out,
+                    int ghost, int nobs, double* mn, double* mx, double relax, double scale, int* ok) {
+  if (!s) return fail(EXA_ERR_INVALID, "null solver");
+  if (ghost < 0 || ghost > 4) return fail(EXA_ERR_INVALID, "ghost layer width out of range");
+  const int D = s->ops->nvar + s->ops->npar;
+  if (nobs < 0 || nobs > std::min(32, D)) return fail(EXA_ERR_INVALID, "observables out of range");
+  std::lock_guard<std::mutex> lk(s->mu);
+  const size_t nl = (size_t)s->ops->sz_luh, nm = (size_t)lim_patch(s, ghost) * D;
+  const size_t nb = op == 4 ? (size_t)2 * s->cfg.dim * nobs : (size_t)nobs;
+  if (int e = shim_scratch(s, nl + nm + 2 * nb + 1)) return e;
+  double *d_luh = s->d_scratch, *d_lim = d_luh + nl, *d_mn = d_lim + nm, *d_mx = d_mn + nb;
+  unsigned char* d_ok = reinterpret_cast<unsigned char*>(d_mx + nb);
+  if (luh_in) EXA_CUDA(cudaMemcpy(d_luh, luh_in, nl * sizeof(double), cudaMemcpyHostToDevice));
+  if (lim_in) EXA_CUDA(cudaMemcpy(d_lim, lim_in, nm * sizeof(double), cudaMemcpyHostToDevice));
+  if (lim_out) EXA_CUDA(cudaMemcpy(d_lim, lim_out, nm * sizeof(double), cudaMemcpyHostToDevice));  // ghosts kept
+  if (op == 4 && nb) {
+    EXA_CUDA(cudaMemcpy(d_mn, mn, nb * sizeof(double), cudaMemcpyHostToDevice));
+    EXA_CUDA(cudaMemcpy(d_mx, mx, nb * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  exa::LimArgs a = lim_args(op, 1, ghost, nobs);
+  a.luh = d_luh;
+  a.luh_out = d_luh;
+  a.lim = d_lim;
+  a.lim_out = d_lim;
+  a.mn = d_mn;
+  a.mx = d_mx;
+  a.ok = d_ok;
+  a.relax = relax;
+  a.scale = scale;
+  if (int e = lim_call(s, a, 0)) return e;
+  if (luh_out) EXA_CUDA(cudaMemcpy(luh_out, d_luh, nl * sizeof(double), cudaMemcpyDeviceToHost));
+  if (lim_out) EXA_CUDA(cudaMemcpy(lim_out, d_lim, nm * sizeof(double), cudaMemcpyDeviceToHost));
+  if (mn && nb) EXA_CUDA(cudaMemcpy(mn, d_mn, nb * sizeof(double), cudaMemcpyDeviceToHost));
+  if (mx && nb) EXA_CUDA(cudaMemcpy(mx, d_mx, nb * sizeof(double), cudaMemcpyDeviceToHost));
+  if (ok) {
+    unsigned char v = 1;
+    EXA_CUDA(cudaMemcpy(&v, d_ok, 1, cudaMemcpyDeviceToHost));
+    *ok = v;
+  }
+  return EXA_OK;
+}
+
+int exa_projectOnFVLimiterSpace(exa_solver* s, const double* luh, double* lim, int ghost) {
+  if (!luh || !lim) return fail(EXA_ERR_INVALID, "null argument");
+  return lim_shim(s, 0, luh, nullptr, nullptr, lim, ghost, 0, nullptr, nullptr, 0.0, 0.0, nullptr);
+}
+int exa_projectOnDGSpace(exa_solver* s, const double* lim, double* luh, int ghost) {
+  if (!luh || !lim) return fail(EXA_ERR_INVALID, "null argument");
+  return lim_shim(s, 1, nullptr, luh, lim, nullptr, ghost, 0, nullptr, nullptr, 0.0, 0.0, nullptr);
+}
+int exa_findCellLocalMinAndMax(exa_solver* s, const double* luh, int nobs, double* mn, double* mx) {
+  if (!luh || (nobs > 0 && (!mn || !mx))) return fail(EXA_ERR_INVALID, "null argument");
+  return lim_shim(s, 2, luh, nullptr, nullptr, nullptr, 0, nobs, mn, mx, 0.0, 0.0, nullptr);
+}
+int exa_findCellLocalLimiterMinAndMax(exa_solver* s, const double* lim, int ghost, int nobs, double* mn, double* mx) {
+  if (!lim || (nobs > 0 && (!mn || !mx))) return fail(EXA_ERR_INVALID, "null argument");
+  return lim_shim(s, 3, nullptr, nullptr, lim, nullptr, ghost, nobs, mn, mx, 0.0, 0.0, nullptr);
+}
+int exa_discreteMaximumPrincipleAndMinAndMaxSearch(exa_solver* s, const double* luh, int nobs, double relax,
+                                                   double scale, double* bmin, double* bmax, int* ok) {
+  if (!luh || !ok || (nobs > 0 && (!bmin || !bmax))) return fail(EXA_ERR_INVALID, "null argument");
+  return lim_shim(s, 4, luh, nullptr, nullptr, nullptr, 0, nobs, bmin, bmax, relax, scale, ok);
+}
+
+int exa_amr_limiter_projectors(int order, double* fine, double* dg2fv, double* fv2dg, double* leg2lob) {
+  if (order < 1 || order > 9) return fail(EXA_ERR_INVALID, "order out of range");
+  const int n = order + 1, P = 2 * order + 1;
+  const double* t = exa::h_amr_lim[order];
+  if (fine) std::copy_n(t, 3 * n * n, fine);
+  t += 3 * n * n;
+  if (dg2fv) std::copy_n(t, n * P, dg2fv);
+  t += n * P;
+  if (fv2dg) std::copy_n(t, P * n, fv2dg);
+  t += P * n;
+  if (leg2lob) std::copy_n(t, n * n, leg2lob);
+  return EXA_OK;
+}
+
 }  // extern "C"
 
 // ------------------------------------------------------------------------------------------

@@ -11,6 +11,7 @@
 
 #include "exa_kernels.cuh"
 #include "exa_adjoint.cuh"
+#include "exa_amr.cuh"
 
 namespace exa {
 
@@ -18,7 +19,7 @@ namespace exa {
 struct Ops {
   // layout version of this interface: an application library compiled against another layout is
   // refused by exa_register_pde (its object would be read with the wrong offsets)
-  static constexpr int kAbi = 3;
+  static constexpr int kAbi = 4;
   int abi = kAbi;
   int dim, order, nvar, npar, nd, nf, cpb;
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
@@ -52,6 +53,11 @@ struct Ops {
   // per-cell volume (mode 0), surface (1) and face (2) integrals of one cell (cell_integral_kernel)
   virtual cudaError_t cell_integral(int mode, double* lduh, const double* in, int direction, int orientation,
                                     const double* dx, cudaStream_t st) = 0;
+  // mesh levels: volume (face = false: luh blocks) or face (lQhbnd and lFhbnd blocks) unknowns,
+  // prolongation / restriction / flux-only restriction (AmrArgs::mode)
+  virtual cudaError_t amr(const AmrArgs& a, bool face, cudaStream_t st) = 0;
+  // limiter cell kernels (LimArgs::op)
+  virtual cudaError_t limiter(const LimArgs& a, cudaStream_t st) = 0;
 };
 
 template <class PDE, int DIM, int N, int P>
@@ -247,6 +253,52 @@ struct OpsImpl final : Ops {
       (void)st;
       return cudaErrorNotSupported;
     }
+  }
+  cudaError_t amr(const AmrArgs& a, bool face, cudaStream_t st) override {
+    if (a.ngroups <= 0) return cudaSuccess;
+    if (face) {
+      if constexpr (DIM > 1) {
+        using Sh = AmrShape<N, DIM - 1, S::D>;
+        amr_kernel<N, DIM - 1, S::D, S::V, true><<<a.ngroups, 256, Sh::smem, st>>>(a);
+      }
+    } else {
+      using Sh = AmrShape<N, DIM, S::D>;
+      static_assert(Sh::smem <= 227 * 1024, "mesh-level kernel shared memory exceeds one CTA");
+      if (!amr_attr) {
+        cudaError_t e = cudaFuncSetAttribute(amr_kernel<N, DIM, S::D, S::V, false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::smem);
+        if (e != cudaSuccess) return e;
+        amr_attr = true;
+      }
+      amr_kernel<N, DIM, S::D, S::V, false><<<a.ngroups, 256, Sh::smem, st>>>(a);
+    }
+    return cudaGetLastError();
+  }
+  bool lim_attr = false, amr_attr = false, lim_mm_attr = false;
+  cudaError_t limiter(const LimArgs& a, cudaStream_t st) override {
+    using L = LimShape<N, DIM, S::D>;
+    static_assert(L::smem <= 227 * 1024, "limiter shared memory exceeds one CTA");
+    if (a.ncells <= 0) return cudaSuccess;
+    if (!lim_attr) {
+      cudaError_t e = cudaFuncSetAttribute(limiter_kernel<N, DIM, S::D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::smem);
+      if (e != cudaSuccess) return e;
+      lim_attr = true;
+    }
+    if (a.op >= 2) {
+      using M = LimMinMaxShape<N, DIM, S::D>;
+      static_assert(M::smem <= 227 * 1024, "limiter min / max shared memory exceeds one CTA");
+      if (!lim_mm_attr) {
+        cudaError_t e = cudaFuncSetAttribute(limiter_minmax_kernel<N, DIM, S::D>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)M::smem);
+        if (e != cudaSuccess) return e;
+        lim_mm_attr = true;
+      }
+      limiter_minmax_kernel<N, DIM, S::D><<<a.ncells, 32 * M::WPC, M::smem, st>>>(a);
+    } else {
+      limiter_kernel<N, DIM, S::D><<<a.ncells, 256, L::smem, st>>>(a);
+    }
+    return cudaGetLastError();
   }
   cudaError_t cell_integral(int mode, double* lduh, const double* in, int direction, int orientation,
                             const double* dx, cudaStream_t st) override {

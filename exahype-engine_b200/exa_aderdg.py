@@ -23,7 +23,9 @@ EXA_OK = 0
 PDE_EULER, PDE_SWE, PDE_ACOUSTIC, PDE_ELASTIC = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 BC_PERIODIC, BC_WALL = 0, 1
-ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT, ST_TIMEOUT = 1, 2, 4, 8, 16
+ST_NONFINITE_PREDICTOR, ST_PICARD_CAP, ST_NONFINITE_UPDATE, ST_BAD_DT, ST_TIMEOUT, ST_BAD_JOB = 1, 2, 4, 8, 16, 32
+# mesh-level operations (exa_amr_volume_unknowns / exa_amr_face_unknowns)
+AMR_PROLONGATE, AMR_RESTRICT, AMR_RESTRICT_FLUX = 0, 1, 2
 NVAR = {PDE_EULER: 5, PDE_SWE: 4, PDE_ACOUSTIC: 4, PDE_ELASTIC: 9}
 NPAR = {PDE_EULER: 0, PDE_SWE: 0, PDE_ACOUSTIC: 2, PDE_ELASTIC: 3}
 
@@ -93,6 +95,7 @@ def load_library(path=None):
     lib.exa_last_error.restype = ctypes.c_char_p
     lib.exa_version.restype = ctypes.c_char_p
     vp, i, d, dp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_double)
+    ll = ctypes.c_longlong
     sigs = {
         "exa_solver_create": [ctypes.POINTER(_Config), ctypes.POINTER(vp)],
         "exa_solver_destroy": [vp],
@@ -139,6 +142,24 @@ def load_library(path=None):
         "exa_pde_available": [i, i, i, i],
         "exa_checkpoint_schedule": [i, i, ctypes.POINTER(CkAction), i, ctypes.POINTER(ctypes.c_int),
                                     ctypes.POINTER(ctypes.c_longlong)],
+        "exa_amr_volume_unknowns": [vp, i, vp, vp, ll, ll, i, vp, i, vp, vp],
+        "exa_amr_face_unknowns": [vp, i, vp, vp, vp, vp, ll, ll, i, vp, i, vp, vp],
+        "exa_volumeUnknownsProlongation": [vp, vp, vp, i, i, vp],
+        "exa_volumeUnknownsRestriction": [vp, vp, vp, i, i, vp],
+        "exa_faceUnknownsProlongation": [vp, vp, vp, vp, vp, i, i, vp],
+        "exa_faceUnknownsRestriction": [vp, vp, vp, vp, vp, i, i, vp],
+        "exa_faceFluxRestriction": [vp, vp, vp, vp, i],
+        "exa_limiter_project_on_fv": [vp, i, vp, vp, i, vp],
+        "exa_limiter_project_on_dg": [vp, i, vp, vp, i, vp],
+        "exa_limiter_local_min_max": [vp, i, vp, i, vp, vp, vp],
+        "exa_limiter_fv_min_max": [vp, i, vp, i, i, vp, vp, vp],
+        "exa_limiter_dmp": [vp, i, vp, i, d, d, vp, vp, vp, vp],
+        "exa_projectOnFVLimiterSpace": [vp, vp, vp, i],
+        "exa_projectOnDGSpace": [vp, vp, vp, i],
+        "exa_findCellLocalMinAndMax": [vp, vp, i, vp, vp],
+        "exa_findCellLocalLimiterMinAndMax": [vp, vp, i, i, vp, vp],
+        "exa_discreteMaximumPrincipleAndMinAndMaxSearch": [vp, vp, i, d, d, vp, vp, ctypes.POINTER(i)],
+        "exa_amr_limiter_projectors": [i, vp, vp, vp, vp],
     }
     for name, args in sigs.items():
         f = getattr(lib, name)
@@ -342,11 +363,140 @@ class Solver:
                "exa_faceIntegralNonlinear")
         return out
 
+    # ---- mesh levels and the limiter --------------------------------------------------------
+    def amr_volume(self, mode, luh_fine, luh_coarse, jobs, group_ptr=None, stream=None):
+        """Batched volume prolongation / restriction (AMR_PROLONGATE / AMR_RESTRICT) on device tensors;
+        jobs: int32 [njobs][6] = (fine cell, coarse cell, levelDelta, subcell index x, y, z)."""
+        s = self.sizes["luh"]
+        _check(self.lib.exa_amr_volume_unknowns(
+            self.h, int(mode), _ptr(luh_fine), _ptr(luh_coarse), luh_fine.numel() // s, luh_coarse.numel() // s,
+            jobs.shape[0], _ptr(jobs), 0 if group_ptr is None else group_ptr.numel() - 1, _ptr(group_ptr),
+            _stream(stream)), "exa_amr_volume_unknowns")
+
+    def amr_face(self, mode, qf, ff, qc, fc, jobs, group_ptr=None, stream=None):
+        """Batched face prolongation / restriction on lQhbnd / lFhbnd device tensors (blocks = cell * 2 DIM + face)."""
+        nq = self.sizes["lQhbnd"] // (2 * self.dim)
+        nfine = (qf.numel() // nq) if qf is not None else ff.numel() // (self.sizes["lFhbnd"] // (2 * self.dim))
+        ncoarse = (qc.numel() // nq) if qc is not None else fc.numel() // (self.sizes["lFhbnd"] // (2 * self.dim))
+        _check(self.lib.exa_amr_face_unknowns(
+            self.h, int(mode), _ptr(qf), _ptr(ff), _ptr(qc), _ptr(fc), nfine, ncoarse, jobs.shape[0], _ptr(jobs),
+            0 if group_ptr is None else group_ptr.numel() - 1, _ptr(group_ptr), _stream(stream)),
+            "exa_amr_face_unknowns")
+
+    def volume_prolongation_cell(self, luh_coarse, coarse_level, fine_level, subcell):
+        out = np.zeros(self.sizes["luh"])
+        idx = np.ascontiguousarray(subcell, dtype=np.int32)
+        _check(self.lib.exa_volumeUnknownsProlongation(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(luh_coarse, dtype=float)),
+                                                       int(coarse_level), int(fine_level), _np_ptr(idx)),
+               "exa_volumeUnknownsProlongation")
+        return out
+
+    def volume_restriction_cell(self, luh_coarse, luh_fine, coarse_level, fine_level, subcell):
+        out = np.ascontiguousarray(luh_coarse, dtype=float).copy()
+        idx = np.ascontiguousarray(subcell, dtype=np.int32)
+        _check(self.lib.exa_volumeUnknownsRestriction(self.h, _np_ptr(out), _np_ptr(np.ascontiguousarray(luh_fine, dtype=float)),
+                                                      int(coarse_level), int(fine_level), _np_ptr(idx)),
+               "exa_volumeUnknownsRestriction")
+        return out
+
+    def face_prolongation_cell(self, q_coarse, f_coarse, coarse_level, fine_level, subface):
+        q = np.zeros(self.sizes["lQhbnd"] // (2 * self.dim))
+        f = np.zeros(self.sizes["lFhbnd"] // (2 * self.dim))
+        idx = np.ascontiguousarray(subface, dtype=np.int32)
+        _check(self.lib.exa_faceUnknownsProlongation(self.h, _np_ptr(q), _np_ptr(f),
+                                                     _np_ptr(np.ascontiguousarray(q_coarse, dtype=float)),
+                                                     _np_ptr(np.ascontiguousarray(f_coarse, dtype=float)),
+                                                     int(coarse_level), int(fine_level), _np_ptr(idx)),
+               "exa_faceUnknownsProlongation")
+        return q, f
+
+    def face_restriction_cell(self, q_coarse, f_coarse, q_fine, f_fine, coarse_level, fine_level, subface):
+        q = np.ascontiguousarray(q_coarse, dtype=float).copy()
+        f = np.ascontiguousarray(f_coarse, dtype=float).copy()
+        idx = np.ascontiguousarray(subface, dtype=np.int32)
+        _check(self.lib.exa_faceUnknownsRestriction(self.h, _np_ptr(q), _np_ptr(f),
+                                                    _np_ptr(np.ascontiguousarray(q_fine, dtype=float)),
+                                                    _np_ptr(np.ascontiguousarray(f_fine, dtype=float)),
+                                                    int(coarse_level), int(fine_level), _np_ptr(idx)),
+               "exa_faceUnknownsRestriction")
+        return q, f
+
+    def face_flux_restriction_cell(self, f_fine, subface, level_delta):
+        f = np.zeros(self.sizes["lFhbnd"] // (2 * self.dim))
+        idx = np.ascontiguousarray(subface, dtype=np.int32)
+        _check(self.lib.exa_faceFluxRestriction(self.h, _np_ptr(f), _np_ptr(np.ascontiguousarray(f_fine, dtype=float)),
+                                                _np_ptr(idx), int(level_delta)), "exa_faceFluxRestriction")
+        return f
+
+    def limiter_patch_size(self, ghost):
+        return (2 * self.order + 1 + 2 * ghost) ** self.dim * self.ndata
+
+    def project_on_fv_cell(self, luh, ghost, lim=None):
+        out = np.zeros(self.limiter_patch_size(ghost)) if lim is None else np.ascontiguousarray(lim, dtype=float).copy()
+        _check(self.lib.exa_projectOnFVLimiterSpace(self.h, _np_ptr(np.ascontiguousarray(luh, dtype=float)),
+                                                    _np_ptr(out), int(ghost)), "exa_projectOnFVLimiterSpace")
+        return out
+
+    def project_on_dg_cell(self, lim, ghost):
+        out = np.zeros(self.sizes["luh"])
+        _check(self.lib.exa_projectOnDGSpace(self.h, _np_ptr(np.ascontiguousarray(lim, dtype=float)), _np_ptr(out),
+                                             int(ghost)), "exa_projectOnDGSpace")
+        return out
+
+    def local_min_max_cell(self, luh, nobs):
+        mn, mx = np.zeros(nobs), np.zeros(nobs)
+        _check(self.lib.exa_findCellLocalMinAndMax(self.h, _np_ptr(np.ascontiguousarray(luh, dtype=float)), int(nobs),
+                                                   _np_ptr(mn), _np_ptr(mx)), "exa_findCellLocalMinAndMax")
+        return mn, mx
+
+    def fv_min_max_cell(self, lim, ghost, nobs):
+        mn, mx = np.zeros(nobs), np.zeros(nobs)
+        _check(self.lib.exa_findCellLocalLimiterMinAndMax(self.h, _np_ptr(np.ascontiguousarray(lim, dtype=float)),
+                                                          int(ghost), int(nobs), _np_ptr(mn), _np_ptr(mx)),
+               "exa_findCellLocalLimiterMinAndMax")
+        return mn, mx
+
+    def dmp_cell(self, luh, nobs, relax, scale, bmin, bmax):
+        """discreteMaximumPrincipleAndMinAndMaxSearch: returns (ok, bmin, bmax) with the rewritten blocks."""
+        bmn = np.ascontiguousarray(bmin, dtype=float).copy()
+        bmx = np.ascontiguousarray(bmax, dtype=float).copy()
+        ok = ctypes.c_int(0)
+        _check(self.lib.exa_discreteMaximumPrincipleAndMinAndMaxSearch(
+            self.h, _np_ptr(np.ascontiguousarray(luh, dtype=float)), int(nobs), float(relax), float(scale),
+            _np_ptr(bmn), _np_ptr(bmx), ctypes.byref(ok)), "exa_discreteMaximumPrincipleAndMinAndMaxSearch")
+        return bool(ok.value), bmn, bmx
+
+    def limiter_project_on_fv(self, luh, lim, ghost, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_limiter_project_on_fv(self.h, ncells, _ptr(luh), _ptr(lim), int(ghost), _stream(stream)),
+               "exa_limiter_project_on_fv")
+
+    def limiter_project_on_dg(self, lim, luh, ghost, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_limiter_project_on_dg(self.h, ncells, _ptr(lim), _ptr(luh), int(ghost), _stream(stream)),
+               "exa_limiter_project_on_dg")
+
+    def limiter_dmp(self, luh, nobs, relax, scale, bmin, bmax, ok, stream=None):
+        ncells = luh.numel() // self.sizes["luh"]
+        _check(self.lib.exa_limiter_dmp(self.h, ncells, _ptr(luh), int(nobs), float(relax), float(scale), _ptr(bmin),
+                                        _ptr(bmax), _ptr(ok), _stream(stream)), "exa_limiter_dmp")
+
     def stable_time_step_size_cell(self, luh, dx):
         out = ctypes.c_double(0.0)
         _check(self.lib.exa_stableTimeStepSize(self.h, _np_ptr(np.ascontiguousarray(luh, dtype=float)),
                                                _dx3(dx, self.dim), ctypes.byref(out)), "exa_stableTimeStepSize")
         return out.value
+
+
+def amr_limiter_projectors(order):
+    """The mesh-level and limiter projectors of one order (host tables of the library): fine
+    [3][n][n], dg2fv [n][P], fv2dg [P][n], leg2lob [n][n] with P = 2N+1."""
+    lib = load_library()
+    n, P = order + 1, 2 * order + 1
+    out = dict(fine=np.zeros((3, n, n)), dg2fv=np.zeros((n, P)), fv2dg=np.zeros((P, n)), leg2lob=np.zeros((n, n)))
+    _check(lib.exa_amr_limiter_projectors(int(order), _np_ptr(out["fine"]), _np_ptr(out["dg2fv"]),
+                                          _np_ptr(out["fv2dg"]), _np_ptr(out["leg2lob"])), "exa_amr_limiter_projectors")
+    return out
 
 
 def grid_descs(grids):

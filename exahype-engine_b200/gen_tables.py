@@ -88,6 +88,63 @@ def operators(order):
                 F0=p0, F1=p1)
 
 
+def gauss_lobatto01(n):
+    """Gauss-Lobatto nodes on [0,1] in DEScending order (1 first, 0 last): the order of the
+    reference's lobatto::nodes tables, which its Legendre-to-Lobatto projector follows."""
+    N = n - 1
+    xs = [mp.mpf(1), mp.mpf(-1)]
+    for k in range(1, N):
+        # interior nodes: roots of P'_N, Newton from the Chebyshev-Gauss-Lobatto points
+        x = mp.cos(mp.pi * k / N)
+        for _ in range(100):
+            p0, p1 = mp.mpf(1), x
+            for j in range(2, N + 1):
+                p0, p1 = p1, ((2 * j - 1) * x * p1 - (j - 1) * p0) / j
+            dp = N * (x * p1 - p0) / (x * x - 1)               # P'_N
+            d2p = (2 * x * dp - N * (N + 1) * p1) / (1 - x * x)  # P''_N (Legendre ODE)
+            dx = dp / d2p
+            x -= dx
+            if abs(dx) < mp.mpf(10) ** (-45):
+                break
+        xs.append(x)
+    return sorted(((x + 1) / 2 for x in xs), reverse=True)
+
+
+def amr_limiter_operators(order):
+    """Projectors between mesh levels and onto the limiter's finite-volume subcells:
+
+    * fine[j][k][m] = phi_k((j + x_m) / 3): coarse basis function k at the fine node m of the j-th
+      third of the cell (3:1 refinement), the single-level prolongation (3d/amrRoutines.cpph);
+    * dg2fv[k][i] = sum_j w_j phi_k((i + x_j) / P): the mean of phi_k over subcell i of P = 2N+1;
+    * fv2dg[i][k]: the least-squares DG reconstruction from the P subcell means under the constraint
+      that the DG cell mean equals the subcell mean (Dumbser et al., J. Comput. Phys. 278 (2014));
+      the saddle-point system is set up as LimiterProjectionMatrices.h:216-262 does;
+    * leg2lob[k][i] = phi_k(lobatto node i) (lobatto nodes descending).
+    """
+    n = order + 1
+    P = 2 * order + 1
+    x, w = gauss_legendre01(n)
+    fine = [[[basis(x, (j + x[m]) / 3)[0][k] for m in range(n)] for k in range(n)] for j in range(3)]
+    dg2fv = [[mp.mpf(0)] * P for _ in range(n)]
+    for i in range(P):
+        for j in range(n):
+            phi, _ = basis(x, (i + x[j]) / P)
+            for k in range(n):
+                dg2fv[k][i] += w[j] * phi[k]
+    M = mp.matrix(n + 1, n + 1)
+    for i in range(n):
+        for j in range(n):
+            M[i, j] = sum(2 * dg2fv[i][k] * dg2fv[j][k] for k in range(P))
+        M[i, n] = w[i]
+        M[n, i] = -w[i]
+    iM = M ** -1
+    rhs = [[2 * dg2fv[j][i] for j in range(n)] + [mp.mpf(1) / P] for i in range(P)]
+    fv2dg = [[sum(iM[k, j] * rhs[i][k] for k in range(n + 1)) for j in range(n)] for i in range(P)]
+    lob = gauss_lobatto01(n)
+    leg2lob = [[basis(x, lob[i])[0][k] for i in range(n)] for k in range(n)]
+    return dict(fine=fine, dg2fv=dg2fv, fv2dg=fv2dg, leg2lob=leg2lob, lobatto=lob, P=P)
+
+
 def fmt(v):
     return repr(float(v)) if float(v) != 0.0 else "0.0"
 
@@ -134,6 +191,46 @@ def main():
     out.append("static const double h_weights[%d][%d] = {%s};" % (MAX_ORDER, MAX_ORDER + 1, ", ".join(rows_w)))
     out.append("}  // namespace exa")
     path = os.path.join(HERE, "csrc", "exa_tables.cuh")
+    with open(path, "w") as f:
+        f.write("\n".join(out) + "\n")
+    print("wrote", path)
+    write_amr_limiter_tables()
+
+
+def write_amr_limiter_tables():
+    out = []
+    out.append("// Generated by exahype-engine_b200/gen_tables.py -- do not edit.")
+    out.append("// Mesh-level and limiter projectors on [0,1] (amr_limiter_operators in the generator):")
+    out.append("// fine[j][k][m], dg2fv[k][i], fv2dg[i][k], leg2lob[k][i], per order, with P = 2N+1 subcells.")
+    out.append("#pragma once")
+    out.append("namespace exa {")
+    out.append("template <int N> struct AmrT;")
+    hosts = []
+    for o in range(1, MAX_ORDER + 1):
+        n = o + 1
+        t = amr_limiter_operators(o)
+        P = t["P"]
+        fine = ", ".join("{%s}" % ", ".join("{%s}" % ", ".join(fmt(v) for v in row) for row in blk) for blk in t["fine"])
+        out.append("static __constant__ double c_fine_%d[3][%d][%d] = {%s};" % (o, n, n, fine))
+        for k, (r, c) in (("dg2fv", (n, P)), ("fv2dg", (P, n)), ("leg2lob", (n, n))):
+            rows = ", ".join("{%s}" % ", ".join(fmt(v) for v in row) for row in t[k])
+            out.append("static __constant__ double c_%s_%d[%d][%d] = {%s};" % (k, o, r, c, rows))
+        out.append("template <> struct AmrT<%d> {" % o)
+        out.append("  static constexpr int n = %d, P = %d;" % (n, P))
+        out.append("  static __device__ __forceinline__ double fine(int j, int k, int m) { return c_fine_%d[j][k][m]; }" % o)
+        out.append("  static __device__ __forceinline__ double dg2fv(int k, int i) { return c_dg2fv_%d[k][i]; }" % o)
+        out.append("  static __device__ __forceinline__ double fv2dg(int i, int k) { return c_fv2dg_%d[i][k]; }" % o)
+        out.append("  static __device__ __forceinline__ double leg2lob(int k, int i) { return c_leg2lob_%d[k][i]; }" % o)
+        out.append("};")
+        flat = [v for blk in t["fine"] for row in blk for v in row] + [v for row in t["dg2fv"] for v in row] + \
+            [v for row in t["fv2dg"] for v in row] + [v for row in t["leg2lob"] for v in row]
+        hosts.append("static const double h_amr_lim_%d[%d] = {%s};" % (o, len(flat), ", ".join(fmt(v) for v in flat)))
+    out.append("// host copies, per order: fine (3 n n), dg2fv (n P), fv2dg (P n), leg2lob (n n), concatenated")
+    out.extend(hosts)
+    out.append("static const double* const h_amr_lim[%d] = {nullptr, %s};" % (
+        MAX_ORDER + 1, ", ".join("h_amr_lim_%d" % o for o in range(1, MAX_ORDER + 1))))
+    out.append("}  // namespace exa")
+    path = os.path.join(HERE, "csrc", "exa_amr_tables.cuh")
     with open(path, "w") as f:
         f.write("\n".join(out) + "\n")
     print("wrote", path)

@@ -45,7 +45,8 @@ typedef enum {
   EXA_ST_PICARD_CAP = 2,      /* some cell used all 2(N+1) Picard sweeps without converging */
   EXA_ST_NONFINITE_UPDATE = 4,
   EXA_ST_BAD_DT = 8,
-  EXA_ST_TIMEOUT = 16         /* a bounded device-side wait ran out; the launch's results are not valid */
+  EXA_ST_TIMEOUT = 16,        /* a bounded device-side wait ran out; the launch's results are not valid */
+  EXA_ST_BAD_JOB = 32         /* a mesh-level job named a block, level difference or subcell index out of range */
 } exa_status_bits;
 
 /* PDE systems compiled as device functors (the user hooks flux / eigenvalues /
@@ -248,6 +249,92 @@ int exa_faceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd,
 int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const double* lduh, double dt);
 /* stableTimeStepSize (3d/stableTimeStepSize.cpph:14-62); returns the value in *dt. */
 int exa_stableTimeStepSize(exa_solver* s, const double* luh, const double* dx, double* dt);
+
+/* ---- mesh levels (AMR) ---------------------------------------------------------------------
+ * A fine cell of the 3:1 refined mesh lies levelDelta = fineGridLevel - coarseGridLevel levels
+ * below a coarse cell; its subcell index along each axis runs over 0 .. 3^levelDelta - 1.
+ *
+ * Batched forms, on device arrays and `stream`. jobs: device int[njobs][6] = {fine block, coarse
+ * block, levelDelta (1..12), subcell index along x, y (, z)}; the unused last entries of a face job
+ * are ignored. Volume blocks are cells of luh
+ * (n^DIM nodes x (nVar + nPar)); face blocks are faces of lQhbnd / lFhbnd (block = cell * 2 DIM +
+ * face: n^(DIM-1) nodes x (nVar + nPar) or nVar). nfine / ncoarse: blocks in the fine / coarse arrays.
+ *   EXA_AMR_PROLONGATE: the fine block is the coarse data prolongated (3d/amrRoutines.cpph:48-143
+ *     faceUnknownsProlongation, :369-444 volumeUnknownsProlongation); group_ptr is ignored.
+ *   EXA_AMR_RESTRICT: the restriction of each fine block is added to its coarse block
+ *     (faceUnknownsRestriction :248-334, volumeUnknownsRestriction :484-554). One CTA per group of
+ *     jobs: group g = jobs [group_ptr[g], group_ptr[g+1]) (device int[ngroups + 1]), all naming one
+ *     coarse block, added in job order; with group_ptr NULL every job is its own group (ngroups is
+ *     then ignored), and no two jobs may then name the same coarse block.
+ *   EXA_AMR_RESTRICT_FLUX (faces): the coarse lFhbnd block is replaced by the fine block's
+ *     restriction (faceUnknownsRestriction :186-246); every job is its own group.
+ * A job out of range is skipped and sets EXA_ST_BAD_JOB in the solver's status word. */
+#define EXA_AMR_PROLONGATE 0
+#define EXA_AMR_RESTRICT 1
+#define EXA_AMR_RESTRICT_FLUX 2
+int exa_amr_volume_unknowns(exa_solver* s, int mode, double* luhFine, double* luhCoarse, long long nfine,
+                            long long ncoarse, int njobs, const int* jobs, int ngroups, const int* group_ptr,
+                            void* stream);
+int exa_amr_face_unknowns(exa_solver* s, int mode, double* lQhbndFine, double* lFhbndFine, double* lQhbndCoarse,
+                          double* lFhbndCoarse, long long nfine, long long ncoarse, int njobs, const int* jobs,
+                          int ngroups, const int* group_ptr, void* stream);
+
+/* Per-call shims with the reference's signatures on host arrays of one cell (luh) or one face
+ * (lQhbnd / lFhbnd of one face); subcellIndex: DIM ints, subfaceIndex: DIM - 1 ints. The
+ * restrictions add to the coarse arrays (the reference's accumulate), except
+ * exa_faceFluxRestriction, which overwrites lFhbndCoarse. */
+int exa_volumeUnknownsProlongation(exa_solver* s, double* luhFine, const double* luhCoarse, int coarseGridLevel,
+                                   int fineGridLevel, const int* subcellIndex);
+int exa_volumeUnknownsRestriction(exa_solver* s, double* luhCoarse, const double* luhFine, int coarseGridLevel,
+                                  int fineGridLevel, const int* subcellIndex);
+int exa_faceUnknownsProlongation(exa_solver* s, double* lQhbndFine, double* lFhbndFine, const double* lQhbndCoarse,
+                                 const double* lFhbndCoarse, int coarseGridLevel, int fineGridLevel,
+                                 const int* subfaceIndex);
+int exa_faceUnknownsRestriction(exa_solver* s, double* lQhbndCoarse, double* lFhbndCoarse, const double* lQhbndFine,
+                                const double* lFhbndFine, int coarseGridLevel, int fineGridLevel,
+                                const int* subfaceIndex);
+int exa_faceFluxRestriction(exa_solver* s, double* lFhbndCoarse, const double* lFhbndFine, const int* subfaceIndex,
+                            int levelDelta);
+
+/* ---- a-posteriori subcell limiter (limiter/generic/c/Limiter.cpph) ------------------------------
+ * The finite-volume patch of a cell has P = 2N+1 subcells per axis (the generated limiting
+ * solver's default PatchSize) plus `ghost` layers (0..4; the FV scheme's GhostLayerWidth: 1
+ * Godunov, 2 MUSCL-Hancock): lim is [(P + 2 ghost)^DIM][nVar + nPar] per cell. Only interior
+ * subcells are read or written. DMP observables are the first nobs (0..min(32, nVar + nPar))
+ * variables and the relaxation parameter is `relax` itself (the generated solver's defaults of
+ * mapDiscreteMaximumPrincipleObservables / getDiscreteMaximumPrincipleRelaxationParameter).
+ * Batched over ncells cells of device arrays on `stream`:
+ *   project_on_fv   projectOnFVLimiterSpace (:43-78): the subcell means of the DG polynomial;
+ *   project_on_dg   projectOnDGSpace (:80-116): the constrained least-squares DG reconstruction;
+ *   local_min_max   findCellLocalMinAndMax (:121-164): per observable, over the nodes, the
+ *                   Gauss-Lobatto nodes and the subcell means; mn / mx [cell][nobs];
+ *   fv_min_max      findCellLocalLimiterMinAndMax (:166-199), over the interior subcells;
+ *   dmp             discreteMaximumPrincipleAndMinAndMaxSearch (:201-255): bmin / bmax
+ *                   [cell][2 DIM][nobs] hold the neighbours' min / max on entry; on return face
+ *                   block 0 holds the cell's own min / max and block 1 the neighbours'; ok[cell] = 1
+ *                   where the principle holds (relaxed by max((max - min) * scale, relax)) and
+ *                   every extremum is finite. */
+int exa_limiter_project_on_fv(exa_solver* s, int ncells, const double* luh, double* lim, int ghost, void* stream);
+int exa_limiter_project_on_dg(exa_solver* s, int ncells, const double* lim, double* luh, int ghost, void* stream);
+int exa_limiter_local_min_max(exa_solver* s, int ncells, const double* luh, int nobs, double* mn, double* mx,
+                              void* stream);
+int exa_limiter_fv_min_max(exa_solver* s, int ncells, const double* lim, int ghost, int nobs, double* mn, double* mx,
+                           void* stream);
+int exa_limiter_dmp(exa_solver* s, int ncells, const double* luh, int nobs, double relax, double scale, double* bmin,
+                    double* bmax, unsigned char* ok, void* stream);
+/* the same for one cell on host arrays, as the generated limiting solver calls them
+ * (GenericLimiterSolverImplementation.template:40-62); exa_discreteMaximumPrincipleAndMinAndMaxSearch
+ * sets *ok to the verdict */
+int exa_projectOnFVLimiterSpace(exa_solver* s, const double* luh, double* lim, int ghost);
+int exa_projectOnDGSpace(exa_solver* s, const double* lim, double* luh, int ghost);
+int exa_findCellLocalMinAndMax(exa_solver* s, const double* luh, int nobs, double* mn, double* mx);
+int exa_findCellLocalLimiterMinAndMax(exa_solver* s, const double* lim, int ghost, int nobs, double* mn, double* mx);
+int exa_discreteMaximumPrincipleAndMinAndMaxSearch(exa_solver* s, const double* luh, int nobs, double relax,
+                                                   double scale, double* bmin, double* bmax, int* ok);
+/* The projectors of order `order` (1..9), host arrays: fine [3][n][n] (phi_k((j + x_m)/3)), dg2fv
+ * [n][P], fv2dg [P][n], leg2lob [n][n] (Gauss-Lobatto nodes descending, as the reference's
+ * tables); any pointer may be NULL. */
+int exa_amr_limiter_projectors(int order, double* fine, double* dg2fv, double* fv2dg, double* leg2lob);
 
 /* ---- device-resident patches: the per-step chain as one CUDA graph ------------------------
  * A patch holds one or more uniform grids (all cells of all grids in one batch, cell-major, grid

@@ -274,6 +274,63 @@ class RefLinear:
         return t.value, dts
 
 
+class RefAmrLimiter:
+    """The reference's mesh-level (3d/amrRoutines.cpph) and limiter (limiter/generic/c/Limiter.cpph)
+    kernels, 3D, for (order, nVar, nPar) in (3,5,0), (3,5,1), (5,5,0), (4,4,2), (4,9,3)
+    (oracle/_ref/libexaref_amrlim3d.so). DMP observables: the first nVar variables."""
+
+    def __init__(self, order, nvar, npar):
+        path = os.path.join(HERE, "_ref", "libexaref_amrlim3d.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        self.order, self.nvar, self.npar = order, nvar, npar
+        self.n, self.D, self.P = order + 1, nvar + npar, 2 * order + 1
+
+    def _idx(self, idx):
+        a = np.zeros(3, dtype=np.int32)
+        a[: len(idx)] = idx
+        return a
+
+    def volume(self, mode, out, inp, coarse_level, fine_level, idx):
+        """mode 0: out (fine luh) = prolongation of inp (coarse); 1: out (coarse) += restriction of inp."""
+        out = _f64(out).copy()
+        r = self.lib.exaamr_volume(self.order, self.nvar, self.npar, int(mode), _p(out), _p(_f64(inp)),
+                                   int(coarse_level), int(fine_level), _p(self._idx(idx)))
+        assert r == 0, "configuration not built"
+        return out
+
+    def face(self, mode, outQ, outF, inQ, inF, coarse_level, fine_level, idx):
+        """mode 0 prolongation, 1 restriction (accumulating), 2 flux-only restriction (overwrite)."""
+        outQ, outF = _f64(outQ).copy(), _f64(outF).copy()
+        r = self.lib.exaamr_face(self.order, self.nvar, self.npar, int(mode), _p(outQ), _p(outF), _p(_f64(inQ)),
+                                 _p(_f64(inF)), int(coarse_level), int(fine_level), _p(self._idx(idx)))
+        assert r == 0, "configuration not built"
+        return outQ, outF
+
+    def limiter(self, op, a, ghost=0, out=None, mn=None, mx=None, relax=0.0, scale=0.0):
+        """op 0 luh -> lim, 1 lim -> luh, 2 / 3 min and max (observables = the first nVar variables),
+        4 discrete maximum principle (mn / mx [2 DIM][nVar] in/out); returns (result, out, mn, mx)."""
+        out = None if out is None else _f64(out).copy()
+        mn = None if mn is None else _f64(mn).copy()
+        mx = None if mx is None else _f64(mx).copy()
+        self.lib.exaamr_limiter.restype = ctypes.c_int
+        r = self.lib.exaamr_limiter(self.order, self.nvar, self.npar, int(ghost), int(op), _p(_f64(a)),
+                                    _p(out) if out is not None else None, _p(mn) if mn is not None else None,
+                                    _p(mx) if mx is not None else None, ctypes.c_double(relax), ctypes.c_double(scale))
+        assert r >= 0, "configuration not built"
+        return r, out, mn, mx
+
+    @staticmethod
+    def tables(order):
+        lib = ctypes.CDLL(os.path.join(HERE, "_ref", "libexaref_amrlim3d.so"))
+        n, P = order + 1, 2 * order + 1
+        fine, d, v, l = np.zeros(3 * n * n), np.zeros(n * P), np.zeros(n * P), np.zeros(n * n)
+        lib.exaamr_fine_grid_projector(int(order), _p(fine))
+        lib.exaamr_limiter_projectors(int(order), _p(d), _p(v), _p(l))
+        return dict(fine=fine.reshape(3, n, n), dg2fv=d.reshape(n, P), fv2dg=v.reshape(P, n), leg2lob=l.reshape(n, n))
+
+
 class KGKernels:
     """The reference's generated optimised kernels (KernelGenerator, plain-loop mode) for the Euler
     application, 3D, order 3 or 5 (oracle/_ref/libkg_euler_o{3,5}.so, built by ``make -C oracle kg``)

@@ -14,6 +14,10 @@ generic_euler_{2d,3d}.npz
 gl_tables.npz
     The reference's DG operator tables (weights, nodes, Kxi, iK1, dudx, FCoeff for orders
     0..9) parsed from ExaHyPE/kernels/generated/GaussLegendreBasis.csnippet.
+limiter_{2d,3d}.npz
+    Every array of the reference's limiter known-answer file
+    ExaHyPE/exahype/tests/kernels/testdata/limiter_testdata.cpp (N = 3, nVar = 5, P = 7 subcells:
+    luh -> subcell means, subcell means -> luh, luh -> Gauss-Lobatto values), parsed as text.
 picard_euler3d_o3.npz, picard_euler2d_o3.npz
     Outputs of the reference's generic kernels (through oracle/_ref) on seeded NON-constant
     cells, which exercise the Picard iteration that the known-answer file leaves trivial.
@@ -37,7 +41,8 @@ def _strip_comments(text):
 
 
 def parse_testdata(path):
-    """Return {'2d': {key: array}, '3d': {key: array}} from generic_euler_testdata.cpp."""
+    """Return {'2d': {key: array}, '3d': {key: array}} from a known-answer file of the reference
+    (generic_euler_testdata.cpp, limiter_testdata.cpp)."""
     raw = open(path).read()
     out = {"2d": {}, "3d": {}}
     for dim, tag in (("2d", "Dim2"), ("3d", "Dim3")):
@@ -155,6 +160,10 @@ def main():
     for dim in ("2d", "3d"):
         np.savez_compressed(os.path.join(HERE, "generic_euler_%s.npz" % dim), **td[dim])
         print(dim, len(td[dim]), "arrays")
+    lt = parse_testdata(os.path.join(args.ref, "ExaHyPE/exahype/tests/kernels/testdata/limiter_testdata.cpp"))
+    for dim in ("2d", "3d"):
+        np.savez_compressed(os.path.join(HERE, "limiter_%s.npz" % dim), **lt[dim])
+        print("limiter", dim, len(lt[dim]), "arrays")
     gl = parse_gl_tables(os.path.join(args.ref, "ExaHyPE/kernels/generated/GaussLegendreBasis.csnippet"))
     np.savez_compressed(os.path.join(HERE, "gl_tables.npz"), **gl)
     print("gl tables", len(gl))
