@@ -838,6 +838,7 @@ struct exa_patch {
   // halo (slab decomposition): ghost cells appended after the real cells, face traces only
   long long nghost = 0;      // 2 * layer cells, or 0
   int halo_axis = -1;        // axis with EXA_BC_HALO
+  bool has_user_bc = false;  // some domain face is EXA_BC_USER
   long long layer = 0;       // cells per layer normal to the halo axis
   long long halo_lo_first = 0, halo_hi_first = 0;  // first real cell of the low / high boundary layer
   // discrete adjoint workspace (allocated on the first exa_patch_adjoint_step)
@@ -1089,9 +1090,11 @@ int exa_patch_create(exa_solver* s, int ngrids, const exa_grid_desc* grids, exa_
   p->grids.assign(grids, grids + ngrids);
   FaceBuild fb;
   if (int r = build_faces(dim, ngrids, grids, fb)) return r;
-  for (int8_t t : fb.bt)
+  for (int8_t t : fb.bt) {
     if (t == EXA_BC_USER && !s->ops->user_bc_ok)
       return fail(EXA_ERR_UNSUPPORTED, "EXA_BC_USER needs a PDE functor with boundary_values");
+    if (t == EXA_BC_USER) p->has_user_bc = true;
+  }
   std::vector<int>& hcell_grid = fb.cell_grid;
   std::vector<int>& fL = fb.fL;
   std::vector<int>& fR = fb.fR;
@@ -1566,8 +1569,8 @@ int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
   const int S = p->s->cfg.max_picard;
   if (S <= 0) return fail(EXA_ERR_UNSUPPORTED, "the adjoint needs a fixed Picard sweep count (max_picard > 0)");
   if (p->s->cfg.precision != EXA_PREC_FP64) return fail(EXA_ERR_UNSUPPORTED, "the adjoint runs in FP64");
-  if (p->nbfaces > 0 || p->halo_axis >= 0)
-    return fail(EXA_ERR_UNSUPPORTED, "the adjoint supports periodic grids (no boundary or halo faces)");
+  if (p->halo_axis >= 0) return fail(EXA_ERR_UNSUPPORTED, "the adjoint of a slab with halo faces is not built");
+  if (p->has_user_bc) return fail(EXA_ERR_UNSUPPORTED, "the adjoint supports periodic, wall and outflow faces");
   if (!(dt > 0)) return fail(EXA_ERR_INVALID, "the adjoint needs the fixed time step of the forward step");
   const size_t nc = (size_t)p->ncells;
   if (!p->adjQ) EXA_CUDA(cudaMalloc(&p->adjQ, nc * o.sz_qhb * sizeof(double)));
@@ -1588,6 +1591,8 @@ int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
   exa::AdjArgs a;
   a.c = c;
   a.f = patch_faces(p);
+  a.fb = a.f;
+  a.fb.nfaces = p->nbfaces;
   a.lam = lambda;
   a.adjQ = p->adjQ;
   a.adjF = p->adjF;

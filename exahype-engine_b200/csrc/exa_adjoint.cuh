@@ -18,6 +18,9 @@
 //   adjoint_face_kernel       one warp per interior face: transposed surface integral of both
 //                             cells' lambda, transposed Rusanov -> adjoints of the predictor's
 //                             face traces (adjQ, adjF), both sides;
+//   adjoint_boundary_kernel   one warp per domain face (reflective wall or outflow): the same for
+//                             the cell's side of a boundary Rusanov flux whose outer state is a
+//                             diagonal sign map B of the inner trace (boundary_kernel's ghost);
 //   adjoint_predictor_kernel  one CTA per cell, one thread per node: takes the Picard iterates
 //                             from a global scratch (written there by the forward predictor
 //                             launch when have_iter is set, else recomputed first), then runs
@@ -30,6 +33,7 @@ namespace exa {
 struct AdjArgs {
   CellArgs c;      // the patch's cell arguments at u_k (luh, geometry, grid dt, source)
   FaceArgs f;      // interior faces
+  FaceArgs fb;     // domain faces (walls, outflow): bcell / bface / btype, fb.nfaces of them
   double* lam;     // in: dJ/du_{k+1}; out: dJ/du_k (luh layout, D entries per node)
   double* adjQ;    // [cell][2 DIM][nf][D]: adjoint of the predictor's lQhbnd
   double* adjF;    // [cell][2 DIM][nf][V]: adjoint of the predictor's lFhbnd (before Riemann)
@@ -148,6 +152,125 @@ __global__ void __launch_bounds__(256) adjoint_face_kernel(AdjArgs a) {
     double* aq = leftMax ? aQL : aQR;
 #pragma unroll
     for (int m = 0; m < D; m++) aq[fn * D + m] += lsm * w * (leftMax ? gL[m] : gR[m]);
+  }
+}
+
+// Domain faces (3d/boundaryConditions.cpph:29-122 with the built-in ghosts of boundary_kernel).
+// The cell's trace q meets the ghost qg = B q (B: +-1 per entry; outflow the identity, a wall the
+// functor's mirrored velocity; parameters copied) whose normal flux is F_d(qg). With the cell on
+// side o of the face (o = 1: the cell is left, o = 0: right),
+//   F* = (F_c + F_d(B q)) / 2 - smax (q_R - q_L) / 2,  q_L, q_R = (q, B q) or (B q, q),
+// so lambda_F* reaches F_c with 1/2, q through B^T J_d(B q)^T / 2 and the dissipation term, and the
+// parameters through smax = max|lambda| of the larger side's face average.
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) adjoint_boundary_kernel(AdjArgs a) {
+  using S = Shape<PDE, DIM, N, P>;
+  using G = GL<N>;
+  constexpr int n = S::n, V = S::V, D = S::D, nd = S::nd, nf = S::nf;
+  const int bf = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (bf >= a.fb.nfaces) return;  // uniform per warp
+  const long c = a.fb.bcell[bf];
+  const int face = a.fb.bface[bf];
+  const int d = face >> 1, o = face & 1;
+  const int type = a.fb.btype ? a.fb.btype[bf] : 1;
+  const int normal = type == 3 ? -1 : d;  // boundary_kernel: outflow (3) or the functor's wall
+  const int g = a.c.cell_grid ? a.c.cell_grid[c] : 0;
+  const double dx = a.c.grid_dx ? a.c.grid_dx[g * 3 + d] : a.c.u_dx[d];
+  const double dt = a.c.grid_dt ? a.c.grid_dt[g] : a.c.u_dt;
+  const double cdt = dt / dx;
+  const double* Q = a.c.lQhbnd + (size_t)c * S::sizeQhb + (size_t)face * nf * D;
+  const double* lam = a.lam + (size_t)c * nd * D;
+  const int st = line_stride<n>(d);
+  // diag(B): the ghost map of a vector of ones
+  double b[D];
+  {
+    double one[D];
+#pragma unroll
+    for (int m = 0; m < D; m++) one[m] = 1.0;
+    ghost_state<PDE, DIM, D>(one, normal, b);
+#pragma unroll
+    for (int m = V; m < D; m++) b[m] = 1.0;
+  }
+  // forward: face averages of both sides and the Rusanov max wave speed
+  double aI[D], aG[D];
+#pragma unroll
+  for (int m = 0; m < D; m++) aI[m] = aG[m] = 0.0;
+  for (int fn = lane; fn < nf; fn += 32) {
+    const double w = DIM == 3 ? G::weights(fn / n) * G::weights(fn % n) : G::weights(fn);
+#pragma unroll
+    for (int m = 0; m < D; m++) {
+      aI[m] += w * Q[fn * D + m];
+      aG[m] += w * b[m] * Q[fn * D + m];
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < D; m++) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      aI[m] += __shfl_xor_sync(0xffffffffu, aI[m], off);
+      aG[m] += __shfl_xor_sync(0xffffffffu, aG[m], off);
+    }
+  }
+  double gI[D], gG[D];
+  const double sI = PDE::template max_speed_grad<DIM>(aI, d, gI);
+  const double sG = PDE::template max_speed_grad<DIM>(aG, d, gG);
+  const double sL = o == 0 ? sG : sI, sR = o == 0 ? sI : sG;
+  const bool leftMax = sL >= sR;  // fmax(sL, sR) in the forward kernel
+  const double smax = leftMax ? sL : sR;
+  const bool ghostMax = (o == 0) == leftMax;
+  double* aF = a.adjF + (size_t)c * S::sizeFhb + (size_t)face * nf * V;
+  double* aQ = a.adjQ + (size_t)c * S::sizeQhb + (size_t)face * nf * D;
+  double lsm = 0.0;  // adjoint of smax
+  const double sgn = o == 1 ? 1.0 : -1.0;  // F* = ... - smax sgn (B q - q) / 2
+  for (int fn = lane; fn < nf; fn += 32) {
+    const int base = line_base<DIM, n>(d, fn);
+    double lf[V];
+#pragma unroll
+    for (int m = 0; m < V; m++) lf[m] = 0.0;
+    // the cell's surface integral (o = 1: its right face, F1; o = 0: its left face, F0)
+#pragma unroll
+    for (int k = 0; k < n; k++) {
+      const double ck = o == 1 ? -cdt * G::F1(k) / G::weights(k) : cdt * G::F0(k) / G::weights(k);
+      const double* ll = lam + (size_t)(base + k * st) * D;
+#pragma unroll
+      for (int m = 0; m < V; m++) lf[m] += ck * ll[m];
+    }
+    double q[D], qg[D];
+#pragma unroll
+    for (int m = 0; m < D; m++) {
+      q[m] = Q[fn * D + m];
+      qg[m] = b[m] * q[m];
+    }
+    // the ghost's normal flux F_d(B q)
+    double lF[DIM * V], lqg[D];
+#pragma unroll
+    for (int k = 0; k < DIM * V; k++) lF[k] = 0.0;
+#pragma unroll
+    for (int m = 0; m < V; m++) lF[d * V + m] = 0.5 * lf[m];
+#pragma unroll
+    for (int m = 0; m < D; m++) lqg[m] = 0.0;
+    PDE::template flux_vjp<DIM>(qg, lF, lqg);
+#pragma unroll
+    for (int m = 0; m < V; m++) {
+      lsm -= 0.5 * sgn * lf[m] * (qg[m] - q[m]);
+      aF[fn * V + m] = 0.5 * lf[m];
+    }
+#pragma unroll
+    for (int m = 0; m < D; m++) {
+      // dissipation: d/dq of -smax sgn (b q - q) / 2
+      const double diss = m < V ? -0.5 * smax * sgn * (b[m] - 1.0) * lf[m] : 0.0;
+      aQ[fn * D + m] = b[m] * lqg[m] + diss;
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) lsm += __shfl_xor_sync(0xffffffffu, lsm, off);
+  __syncwarp();
+  // smax = max|lambda| of the larger side's face average (of q, or of B q)
+  for (int fn = lane; fn < nf; fn += 32) {
+    const double w = DIM == 3 ? G::weights(fn / n) * G::weights(fn % n) : G::weights(fn);
+#pragma unroll
+    for (int m = 0; m < D; m++) aQ[fn * D + m] += lsm * w * (ghostMax ? b[m] * gG[m] : gI[m]);
   }
 }
 

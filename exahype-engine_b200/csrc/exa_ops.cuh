@@ -19,7 +19,7 @@ namespace exa {
 struct Ops {
   // layout version of this interface: an application library compiled against another layout is
   // refused by exa_register_pde (its object would be read with the wrong offsets)
-  static constexpr int kAbi = 4;
+  static constexpr int kAbi = 5;
   int abi = kAbi;
   int dim, order, nvar, npar, nd, nf, cpb;
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
@@ -236,6 +236,11 @@ struct OpsImpl final : Ops {
       static_assert(A::smem <= 227 * 1024, "adjoint shared memory exceeds one CTA");
       if (a.f.nfaces > 0) {
         adjoint_face_kernel<PDE, DIM, N, P><<<(unsigned)((a.f.nfaces + 7) / 8), 256, 0, st>>>(a);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+      }
+      if (a.fb.nfaces > 0) {
+        adjoint_boundary_kernel<PDE, DIM, N, P><<<(unsigned)((a.fb.nfaces + 7) / 8), 256, 0, st>>>(a);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
       }

@@ -62,7 +62,9 @@ class WaveInversion:
     """One forward model: grid, order, time step, receivers, checkpoint budget."""
 
     def __init__(self, pde, ncell, size, order, dt, nsteps, receivers, rec_var=0, snaps=20, source=None,
-                 device="cuda"):
+                 device="cuda", bc=0):
+        """bc: domain faces of the grid (exa_aderdg.BC_*, one or per axis): periodic, reflective
+        walls or outflow (absorbing for normal waves)."""
         if pde not in (exa.PDE_ACOUSTIC, exa.PDE_ELASTIC):
             raise ValueError("the adjoint is built for the acoustic and elastic systems")
         self.pde, self.ncell, self.size, self.order = pde, tuple(ncell), list(size), order
@@ -75,7 +77,7 @@ class WaveInversion:
         self.ncells = int(np.prod(ncell))
         # the reference's fixed-count Picard mode: MaxPicardIterations = Order + 1
         self.solver = exa.Solver(pde, len(ncell), order, npar=self.P, max_picard=order + 1)
-        self.patch = exa.Patch(self.solver, [dict(ncell=self.ncell, size=self.size)])
+        self.patch = exa.Patch(self.solver, [dict(ncell=self.ncell, size=self.size, bc=bc)])
         self.source = source
         if source is not None:
             self.patch.set_point_source(source[:3], source[3], source[4], source[5], source[6], int(source[7]))

@@ -458,8 +458,9 @@ int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int 
 /* ---- discrete adjoint (acoustic and elastic systems) -----------------------------------------
  * No reference counterpart: the reference has no adjoint. The forward step differentiated is
  * exa_patch_step(p, 1, dt) with a fixed dt and a solver created with max_picard > 0 (the
- * reference's UseMaxPicardIterations mode: a fixed Picard sweep count, no residual test), on
- * periodic grids, FP64.
+ * reference's UseMaxPicardIterations mode: a fixed Picard sweep count, no residual test), FP64,
+ * on grids whose domain faces are periodic, reflective walls or outflow (EXA_BC_USER faces and
+ * halo slabs are refused with EXA_ERR_UNSUPPORTED).
  *
  * exa_patch_adjoint_step: the patch's current solution is u_k at time t_k (exa_patch_set_time).
  * lambda (device, luh layout: D doubles per node) holds dJ/du_{k+1} on entry and
