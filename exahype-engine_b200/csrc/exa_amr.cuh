@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(kAmrThreads) limiter_kernel(LimArgs a) {
   const double* luh = a.luh ? a.luh + (size_t)c * nb * D : nullptr;
   const double* lim = a.lim ? a.lim + (size_t)c * ext * D : nullptr;
   const int nvar = (a.op <= 1) ? D : a.nobs;
-  const int myv = threadIdx.x < STEP ? threadIdx.x % VC : -1;  // this thread's variable in extrema passes
+  const int myv = (int)threadIdx.x < STEP ? (int)threadIdx.x % VC : -1;  // this thread's variable in extrema passes
   // the projectors as uniform operands of the unrolled sweeps (constant bank)
   auto d2f = [](int k, int m) { return A::dg2fv(k, m); };
   auto f2d = [](int i, int k) { return A::fv2dg(i, k); };
@@ -475,8 +475,15 @@ struct LimMinMaxShape {
   static constexpr int m1 = DIM == 3 ? n * n * P : n * P;
   static constexpr int m2 = DIM == 3 ? n * P * P : 1;
   static constexpr int per_warp = nb + m1 + m2;
-  static constexpr int WPC = D < 8 ? D : 8;
-  static constexpr size_t smem = sizeof(double) * (size_t)WPC * per_warp;
+  // warps per CTA: one per observable up to 8, as many as fit one CTA's shared memory next to the
+  // cell's DG block (staged once with contiguous loads for all warps)
+  static constexpr int fitw = (int)((220 * 1024 - 8 * nb * D) / (8 * per_warp));
+  static constexpr int WPC = (D < 8 ? D : 8) < fitw ? (D < 8 ? D : 8) : (fitw < 1 ? 1 : fitw);
+  static constexpr int smem_words = nb * D + WPC * per_warp;
+  static constexpr size_t smem = sizeof(double) * (size_t)smem_words;
+  // resident CTAs the register budget is sized for (shared memory permitting)
+  static constexpr int MinBlocks = 3 * (8 * smem_words + 2048) <= 220 * 1024 ? 3
+                                   : (2 * (8 * smem_words + 2048) <= 220 * 1024 ? 2 : 1);
 };
 
 // Limiter ops 2 (findCellLocalMinAndMax), 3 (findCellLocalLimiterMinAndMax) and 4
@@ -484,7 +491,8 @@ struct LimMinMaxShape {
 // ...; each warp projects its observable onto the Gauss-Lobatto nodes and the subcell means with
 // warp-synchronous sweeps, reduces its extrema by shuffles, and thread 0 applies the principle.
 template <int N, int DIM, int D>
-__global__ void __launch_bounds__(32 * LimMinMaxShape<N, DIM, D>::WPC) limiter_minmax_kernel(LimArgs a) {
+__global__ void __launch_bounds__(32 * LimMinMaxShape<N, DIM, D>::WPC, LimMinMaxShape<N, DIM, D>::MinBlocks)
+limiter_minmax_kernel(LimArgs a) {
   using A = AmrT<N>;
   using Sh = LimMinMaxShape<N, DIM, D>;
   constexpr int n = Sh::n, P = Sh::P, nb = Sh::nb, WPC = Sh::WPC;
@@ -492,7 +500,8 @@ __global__ void __launch_bounds__(32 * LimMinMaxShape<N, DIM, D>::WPC) limiter_m
   __shared__ double s_lmin[32], s_lmax[32];
   const int c = blockIdx.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* U = sm + (size_t)warp * Sh::per_warp;  // [nb]
+  double* blk = sm;                                          // [nb][D] the cell's DG block
+  double* U = sm + (size_t)nb * D + (size_t)warp * Sh::per_warp;  // [nb]
   double* M1 = U + nb;
   double* M2 = M1 + Sh::m1;
   const int g = a.ghost;
@@ -501,6 +510,11 @@ __global__ void __launch_bounds__(32 * LimMinMaxShape<N, DIM, D>::WPC) limiter_m
   auto d2f = [](int k, int m) { return A::dg2fv(k, m); };
   auto l2b = [](int k, int i) { return A::leg2lob(k, i); };
   if (a.op == 4 && threadIdx.x == 0) a.ok[c] = 1;
+  if (a.op != 3) {
+    const double* src = a.luh + (size_t)c * nb * D;
+    for (int e = threadIdx.x; e < nb * D; e += blockDim.x) blk[e] = src[e];
+    __syncthreads();
+  }
   for (int v = warp; v < a.nobs; v += WPC) {
     double lo = INFINITY, hi = -INFINITY;
     auto take = [&](int, double x) {
@@ -517,9 +531,8 @@ __global__ void __launch_bounds__(32 * LimMinMaxShape<N, DIM, D>::WPC) limiter_m
         take(0, lim[at * D]);
       }
     } else {
-      const double* luh = a.luh + (size_t)c * nb * D + v;
       for (int p = lane; p < nb; p += 32) {
-        U[p] = luh[(size_t)p * D];
+        U[p] = blk[p * D + v];
         take(0, U[p]);
       }
       __syncwarp();
