@@ -1,9 +1,9 @@
-// Checker glue around the reference's OWN mesh-level and limiter kernels (3D).
+// Checker glue around the reference's OWN mesh-level and limiter kernels (2D or 3D).
 //
 // Test infrastructure: compiled by oracle/Makefile, with the unmodified reference sources
-// ExaHyPE/kernels/aderdg/generic/Kernels.h (3d/amrRoutines.cpph), kernels/limiter/generic/Limiter.h
+// ExaHyPE/kernels/aderdg/generic/Kernels.h ({2d,3d}/amrRoutines.cpph), kernels/limiter/generic/Limiter.h
 // (c/Limiter.cpph), kernels/LimiterProjectionMatrices.{h,cpp}, kernels/GaussLegendreBasis.cpp and
-// kernels/GaussLobattoBasis.cpp read in place, into oracle/_ref/libexaref_amrlim3d.so. Only tests load
+// kernels/GaussLobattoBasis.cpp read in place, into oracle/_ref/libexaref_amrlim{2,3}d.so. Only tests load
 // it. The solver type plays the role of the generated glue: the static tables the kernels read
 // (weights, fineGridProjector) and the default DMP hooks of
 // AbstractGenericADERDGSolverHeader.template:176-198 (observables = the first NumberOfDMPObservables
@@ -42,8 +42,8 @@ template <int O, int V, int P, int B> double**** Solver<O, V, P, B>::fineGridPro
 
 template <class S>
 void volume(int mode, double* out, const double* in, int coarseLevel, int fineLevel, const int* idx) {
-  tarch::la::Vector<3, int> sub;
-  for (int d = 0; d < 3; d++) sub[d] = idx[d];
+  tarch::la::Vector<DIMENSIONS, int> sub;
+  for (int d = 0; d < DIMENSIONS; d++) sub[d] = idx[d];
   constexpr int n = S::Order + 1;
   if (mode == 0)
     kernels::aderdg::generic::c::volumeUnknownsProlongation<S, S::NumberOfVariables, S::NumberOfParameters, n>(
@@ -56,9 +56,8 @@ void volume(int mode, double* out, const double* in, int coarseLevel, int fineLe
 template <class S>
 void face(int mode, double* outQ, double* outF, const double* inQ, const double* inF, int coarseLevel,
           int fineLevel, const int* idx) {
-  tarch::la::Vector<2, int> sub;
-  sub[0] = idx[0];
-  sub[1] = idx[1];
+  tarch::la::Vector<DIMENSIONS - 1, int> sub;
+  for (int d = 0; d < DIMENSIONS - 1; d++) sub[d] = idx[d];
   constexpr int n = S::Order + 1;
   if (mode == 0)
     kernels::aderdg::generic::c::faceUnknownsProlongation<S, S::NumberOfVariables, S::NumberOfParameters, n>(
@@ -110,8 +109,10 @@ int limiter(int op, const double* a, double* b, double* mn, double* mx, double r
 
 using exaamr::Solver;
 
-// configurations (order, nVar, nPar) of the GPU library's 3D instantiations: (3, 5, 0), (3, 5, 1),
-// (5, 5, 0) [Euler], (4, 4, 2) [acoustics], (4, 9, 3) [elasticity with material parameters]
+// configurations (order, nVar, nPar) of the GPU library's instantiations: 3D (3, 5, 0), (3, 5, 1),
+// (5, 5, 0) [Euler], (4, 4, 2) [acoustics], (4, 9, 3) [elasticity with material parameters]; 2D
+// (3, 5, 0), (3, 5, 1) [Euler], (4, 4, 0) [shallow water]
+#if DIMENSIONS == 3
 #define EXAAMR_DISPATCH(FN, ...)                                                                   \
   if (order == 3 && nvar == 5 && npar == 0) return FN<Solver<3, 5, 0, 5>>(__VA_ARGS__), 0;           \
   if (order == 3 && nvar == 5 && npar == 1) return FN<Solver<3, 5, 1, 5>>(__VA_ARGS__), 0;           \
@@ -119,6 +120,13 @@ using exaamr::Solver;
   if (order == 5 && nvar == 5 && npar == 0) return FN<Solver<5, 5, 0, 5>>(__VA_ARGS__), 0;           \
   if (order == 4 && nvar == 9 && npar == 3) return FN<Solver<4, 9, 3, 9>>(__VA_ARGS__), 0;           \
   return -1;
+#else
+#define EXAAMR_DISPATCH(FN, ...)                                                                   \
+  if (order == 3 && nvar == 5 && npar == 0) return FN<Solver<3, 5, 0, 5>>(__VA_ARGS__), 0;           \
+  if (order == 3 && nvar == 5 && npar == 1) return FN<Solver<3, 5, 1, 5>>(__VA_ARGS__), 0;           \
+  if (order == 4 && nvar == 4 && npar == 0) return FN<Solver<4, 4, 0, 4>>(__VA_ARGS__), 0;           \
+  return -1;
+#endif
 
 extern "C" int exaamr_volume(int order, int nvar, int npar, int mode, double* out, const double* in,
                              int coarseLevel, int fineLevel, const int* idx) {
@@ -172,8 +180,12 @@ extern "C" int exaamr_limiter(int order, int nvar, int npar, int ghost, int op, 
   }
   EXAAMR_LIM(3, 5, 0)
   EXAAMR_LIM(3, 5, 1)
+#if DIMENSIONS == 3
   EXAAMR_LIM(5, 5, 0)
   EXAAMR_LIM(4, 9, 3)
+#else
+  EXAAMR_LIM(4, 4, 0)
+#endif
 #undef EXAAMR_LIM
   return -1;
 }

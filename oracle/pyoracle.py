@@ -279,12 +279,13 @@ class RefAmrLimiter:
     kernels, 3D, for (order, nVar, nPar) in (3,5,0), (3,5,1), (5,5,0), (4,4,2), (4,9,3)
     (oracle/_ref/libexaref_amrlim3d.so). DMP observables: the first nVar variables."""
 
-    def __init__(self, order, nvar, npar):
-        path = os.path.join(HERE, "_ref", "libexaref_amrlim3d.so")
+    def __init__(self, order, nvar, npar, dim=3):
+        """dim 2: (order, nVar, nPar) in (3,5,0), (3,5,1), (4,4,0) (libexaref_amrlim2d.so)."""
+        path = os.path.join(HERE, "_ref", "libexaref_amrlim%dd.so" % dim)
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = ctypes.CDLL(path)
-        self.order, self.nvar, self.npar = order, nvar, npar
+        self.order, self.nvar, self.npar, self.dim = order, nvar, npar, dim
         self.n, self.D, self.P = order + 1, nvar + npar, 2 * order + 1
 
     def _idx(self, idx):

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from conftest import REPO
-from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC, PDE_EULER, RefAmrLimiter
+from pyoracle import PDE_ACOUSTIC, PDE_ELASTIC, PDE_EULER, PDE_SWE, RefAmrLimiter
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(REPO, "tests", "golden")
@@ -283,4 +283,70 @@ def test_limiter_batched_matches_per_cell(exa, torch):
     # the DG -> FV -> DG round trip is the identity on polynomials of degree N (mass-conserving
     # least squares of exact subcell means)
     assert rel(backh, luh) < 1e-11
+    s.close()
+
+
+# ------------------------------------------------------------------------------------------
+# 2D (the reference's 2d/amrRoutines.cpph and the 2D branches of Limiter.cpph)
+# ------------------------------------------------------------------------------------------
+CONFIGS_2D = [(PDE_EULER, 3, 5, 0), (PDE_EULER, 3, 5, 1), (PDE_SWE, 4, 4, 0)]
+IDS_2D = ["euler2d_n3", "euler2d_n3_p1", "swe2d_n4"]
+
+
+@pytest.mark.parametrize("cfg", CONFIGS_2D, ids=IDS_2D)
+@pytest.mark.parametrize("level_delta", [1, 2])
+def test_2d_volume_and_face_unknowns_vs_reference(exa, cfg, level_delta):
+    pde, order, nvar, npar = cfg
+    rng = np.random.default_rng(31 + order + level_delta + npar)
+    s = exa.Solver(pde, 2, order, npar=npar)
+    ref = RefAmrLimiter(order, nvar, npar, dim=2)
+    nl = s.sizes["luh"]
+    nq, nf = s.sizes["lQhbnd"] // 4, s.sizes["lFhbnd"] // 4
+    for idx in [tuple(int(x) for x in rng.integers(0, 3 ** level_delta, 2)) for _ in range(6)]:
+        coarse = rng.normal(size=nl)
+        assert rel(s.volume_prolongation_cell(coarse, 0, level_delta, idx),
+                   ref.volume(0, np.zeros(nl), coarse, 0, level_delta, idx)) < TOL
+        fine, acc = rng.normal(size=nl), rng.normal(size=nl)
+        assert rel(s.volume_restriction_cell(acc, fine, 0, level_delta, idx),
+                   ref.volume(1, acc, fine, 0, level_delta, idx)) < TOL
+        sub = idx[:1]
+        qc, fc, qf, ff = rng.normal(size=nq), rng.normal(size=nf), rng.normal(size=nq), rng.normal(size=nf)
+        gq, gf = s.face_prolongation_cell(qc, fc, 0, level_delta, sub)
+        wq, wf = ref.face(0, np.zeros(nq), np.zeros(nf), qc, fc, 0, level_delta, sub)
+        assert rel(gq, wq) < TOL and rel(gf, wf) < TOL
+        gq, gf = s.face_restriction_cell(qc, fc, qf, ff, 0, level_delta, sub)
+        wq, wf = ref.face(1, qc, fc, qf, ff, 0, level_delta, sub)
+        assert rel(gq, wq) < TOL and rel(gf, wf) < TOL
+    assert s.status() == 0
+    s.close()
+
+
+@pytest.mark.parametrize("cfg", CONFIGS_2D, ids=IDS_2D)
+@pytest.mark.parametrize("ghost", [1, 2])
+def test_2d_limiter_kernels_vs_reference(exa, cfg, ghost):
+    pde, order, nvar, npar = cfg
+    rng = np.random.default_rng(41 + ghost + order + npar)
+    s = exa.Solver(pde, 2, order, npar=npar)
+    ref = RefAmrLimiter(order, nvar, npar, dim=2)
+    nl, nm = s.sizes["luh"], s.limiter_patch_size(ghost)
+    luh = rng.normal(size=nl)
+    filler = rng.normal(size=nm)
+    _, want, _, _ = ref.limiter(0, luh, ghost, out=filler)
+    assert rel(s.project_on_fv_cell(luh, ghost, lim=filler), want) < TOL
+    lim = rng.normal(size=nm)
+    _, want, _, _ = ref.limiter(1, lim, ghost, out=np.zeros(nl))
+    assert rel(s.project_on_dg_cell(lim, ghost), want) < TOL
+    gmn, gmx = s.local_min_max_cell(luh, nvar)
+    _, _, wmn, wmx = ref.limiter(2, luh, ghost, mn=np.zeros(nvar), mx=np.zeros(nvar))
+    assert rel(gmn, wmn) < TOL and rel(gmx, wmx) < TOL
+    span = gmx - gmn
+    for trial in range(4):
+        bmin = gmn - rng.uniform(0.01, 0.2, (4, nvar)) * span
+        bmax = gmx + rng.uniform(0.01, 0.2, (4, nvar)) * span
+        if trial % 2:
+            bmax[:, trial % nvar] = gmx[trial % nvar] - 0.1 * span[trial % nvar]
+        ok, m0, m1 = s.dmp_cell(luh, nvar, 1e-4, 1e-3, bmin.reshape(-1), bmax.reshape(-1))
+        r, _, w0, w1 = ref.limiter(4, luh, 0, mn=bmin.reshape(-1), mx=bmax.reshape(-1), relax=1e-4, scale=1e-3)
+        assert ok == bool(r) == (trial % 2 == 0)
+        assert rel(m0, w0) < TOL and rel(m1, w1) < TOL
     s.close()
