@@ -115,8 +115,15 @@ struct Shape {
   static constexpr int even(int x) { return (x + 1) / 2 * 2; }  // 16-byte boundary in doubles
   // predictor shared memory for a given per-node stride dq of the iterate slices and the luh
   // block; the staging buffer of the persistent form comes last
+  // per-cell stride of the iterate slices [t][node][dq]: where a warp spans two cells (CPB > 1),
+  // padded to a stride congruent to nd*dq modulo 16 words, so that the next cell's nodes continue
+  // the bank-pair progression of the node stride dq instead of landing on pairs the first cell's
+  // lanes already use (2D N=4: 625 -> 637 words)
+  static constexpr int qcs(int dq) {
+    return CPB > 1 ? n * nd * dq + ((nd * dq - n * nd * dq) % 16 + 16) % 16 : n * nd * dq;
+  }
   static constexpr size_t smem_for(int dq) {
-    return sizeof(double) * (size_t)(even(CPB * n * nd * dq + smemF + CPB * nd * dq) + smemStage);
+    return sizeof(double) * (size_t)(even(CPB * qcs(dq) + smemF + CPB * nd * dq) + smemStage);
   }
   // resident CTAs per SM: two when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
   static constexpr int blocks_for(int dq) { return 2 * (smem_for(dq) + 3 * 1024) <= 228 * 1024 ? 2 : 1; }
@@ -128,7 +135,8 @@ struct Shape {
                                  fits_cta(smem_for(D | 1)) >= fits_cta(smem_for(D));
   static constexpr int DQ = pad_ok ? (D | 1) : D;
   // dynamic shared memory of the predictor: iterate/rhs slices [cell][t][node][DQ] + flux/partials
-  static constexpr int smemQ = CPB * n * nd * DQ;
+  static constexpr int QCS = qcs(DQ);
+  static constexpr int smemQ = CPB * QCS;
   static constexpr int items = CPB * DIM * V * NL;             // line contractions per time node
   static constexpr int rounds = (items + TPB - 1) / TPB;       // per thread
   static constexpr int smemU = CPB * nd * DQ;                  // luh of the CTA's cells

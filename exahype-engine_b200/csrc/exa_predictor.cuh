@@ -142,7 +142,7 @@ predictor_kernel(CellArgs a) {
     // luh of this node, kept in shared memory (read once per phase, not worth 2*D registers);
     // the old iterate starts as lQi[., t] = luh (:71-82)
     double* u = sQ + S::smemQ + S::smemF + ((size_t)lc * nd + p) * DQ;
-    double* q_s = sQ + (size_t)lc * n * nd * DQ;
+    double* q_s = sQ + (size_t)lc * S::QCS;
     double* f_s = sF + (size_t)lc * FCS;
     const int cell0 = a.cell_begin + grp * CPB;
     const int cell = cell0 + lc;
@@ -642,7 +642,7 @@ predictor_kernel(CellArgs a) {
       const int d = rl / NL, L = rl % NL;
       const int st = d == 0 ? 1 : (d == 1 ? n : n * n);
       if (isQ) {
-        const double* src = smem + (size_t)c * n * nd * DQ + (size_t)line_base<DIM, n>(d, L) * DQ;
+        const double* src = smem + (size_t)c * S::QCS + (size_t)line_base<DIM, n>(d, L) * DQ;
         double* o0 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d) * nf + L) * D;
         double* o1 = a.lQhbnd + (size_t)gc * S::sizeQhb + (size_t)((2 * d + 1) * nf + L) * D;
 #pragma unroll
