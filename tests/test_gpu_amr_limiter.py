@@ -350,3 +350,49 @@ def test_2d_limiter_kernels_vs_reference(exa, cfg, ghost):
         assert ok == bool(r) == (trial % 2 == 0)
         assert rel(m0, w0) < TOL and rel(m1, w1) < TOL
     s.close()
+
+
+def test_edge_cases_and_argument_checks(exa, torch):
+    """Empty batches are no-ops; out-of-range arguments are refused on the host (EXA_ERR_INVALID)
+    before any launch; the per-call shims check level differences and subcell indices."""
+    s = exa.Solver(PDE_EULER, 3, 3, npar=0)
+    nl = s.sizes["luh"]
+    dev = torch.device("cuda")
+    luh = torch.zeros(nl, dtype=torch.float64, device=dev)
+    empty_jobs = torch.zeros((0, 6), dtype=torch.int32, device=dev)
+    s.amr_volume(exa.AMR_PROLONGATE, luh, luh, empty_jobs)
+    s.amr_volume(exa.AMR_RESTRICT, luh, luh, empty_jobs)
+    lim0 = torch.zeros(0, dtype=torch.float64, device=dev)
+    luh0 = torch.zeros(0, dtype=torch.float64, device=dev)
+    s.limiter_project_on_fv(luh0, lim0, 1)
+    s.limiter_project_on_dg(lim0, luh0, 1)
+    torch.cuda.synchronize()
+    assert s.status() == 0
+    one = np.ones(nl)
+    with pytest.raises(exa.ExaError):
+        s.volume_prolongation_cell(one, 2, 2, (0, 0, 0))           # level difference 0
+    with pytest.raises(exa.ExaError):
+        s.volume_prolongation_cell(one, 0, 1, (3, 0, 0))           # index beyond 3^1
+    with pytest.raises(exa.ExaError):
+        s.volume_restriction_cell(one, one, 0, 13, (0, 0, 0))      # beyond 12 levels
+    with pytest.raises(exa.ExaError):
+        s.project_on_fv_cell(one, 5)                               # ghost layers 0..4
+    with pytest.raises(exa.ExaError):
+        s.local_min_max_cell(one, 6)                               # more observables than variables
+    with pytest.raises(exa.ExaError):
+        s.dmp_cell(one, -1, 1e-4, 1e-3, np.zeros(0), np.zeros(0))
+    # the flux-only restriction is a face operation
+    jobs = torch.tensor([[0, 0, 1, 0, 0, 0]], dtype=torch.int32, device=dev)
+    with pytest.raises(exa.ExaError):
+        s.amr_volume(exa.AMR_RESTRICT_FLUX, luh, luh, jobs)
+    # a group pointer beyond the job list is flagged and the group skipped
+    ptr = torch.tensor([0, 2], dtype=torch.int32, device=dev)
+    before = luh.clone()
+    s.amr_volume(exa.AMR_RESTRICT, luh, luh, jobs, group_ptr=ptr)
+    torch.cuda.synchronize()
+    assert s.status() & exa.ST_BAD_JOB
+    assert torch.equal(luh, before)
+    # the DMP of a cell with no observables holds
+    ok, _, _ = s.dmp_cell(one, 0, 1e-4, 1e-3, np.zeros(0), np.zeros(0))
+    assert ok
+    s.close()
