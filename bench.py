@@ -451,6 +451,7 @@ def run_acoustic_adjoint(args):
     # finite differences along seeded directions
     rng = np.random.default_rng(1)
     errs, kinks = [], []
+    dirder, cond_ad, cond_fd, err_scaled = [], [], [], []
     cgrid = params0[:, 1].reshape(ncell[2], ncell[1], ncell[0])
 
     def kink_faces(vc, h):
@@ -472,9 +473,16 @@ def run_acoustic_adjoint(args):
     for _ in range(args.fd_directions):
         vp = torch.tensor(rng.normal(size=tuple(params0.shape)), device=dev) * params0
         vf = torch.tensor(rng.normal(size=tuple(p0.shape)), device=dev)
-        fd = fd_directional(inv, params0, p0, vp, vf, data, h=1e-6)
+        fd, fd_scale = fd_directional(inv, params0, p0, vp, vf, data, h=1e-6, with_scale=True)
         ad = float((gp * vp).sum() + (gf * vf).sum())
         errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+        # cancellation in the two sums: sum of |terms| over |sum|; a relative error this many
+        # times the rounding of one term is what the sums themselves allow
+        ad_scale = float((gp * vp).abs().sum() + (gf * vf).abs().sum())
+        dirder.append(ad)
+        err_scaled.append(abs(fd - ad) / max(ad_scale, 1e-300))
+        cond_ad.append(ad_scale / max(abs(ad), 1e-300))
+        cond_fd.append(fd_scale / max(abs(fd), 1e-300))
         nk, mask = kink_faces(vp[:, 1], 1e-6)
         kinks.append(nk)
         # the same direction with c left unperturbed next to those faces: the misfit is smooth along
@@ -505,6 +513,13 @@ def run_acoustic_adjoint(args):
                          "median_rel_err": float(np.median(errs)) if errs else None,
                          "rel_err_per_direction": errs_all,
                          "kink_faces_per_direction": kinks,
+                         "directional_derivative_per_direction": dirder,
+                         "cancellation_adjoint_per_direction": cond_ad,
+                         "cancellation_fd_per_direction": cond_fd,
+                         "cancellation": "sum of |terms| / |sum| of the adjoint dot product g.v and of "
+                                         "the finite difference's trace sum",
+                         "abs_err_over_sum_abs_terms_per_direction": err_scaled,
+                         "max_abs_err_over_sum_abs_terms": max(err_scaled) if err_scaled else None,
                          "rel_err_per_direction_kink_free": errs_smooth,
                          "max_rel_err_kink_free": max(errs_smooth) if errs_smooth else None,
                          "kink_free": "the same directions with the c perturbation zeroed on the cells next "

@@ -205,15 +205,21 @@ class WaveInversion:
         self.patch.close()
 
 
-def fd_directional(inv, params, field0, vp, vf, data, h=1e-6):
+def fd_directional(inv, params, field0, vp, vf, data, h=1e-6, with_scale=False):
     """Central finite difference (J(x + h v) - J(x - h v)) / (2 h) of the misfit along (vp, vf),
     evaluated as sum_k (tr+ - tr-) . ((tr+ + tr-)/2 - d) / (2 h): the same two model runs and the
-    same difference, without forming J+ and J- first (their leading digits cancel)."""
+    same difference, without forming J+ and J- first (their leading digits cancel). With
+    with_scale, also returns sum_k |(tr+ - tr-) . ((tr+ + tr-)/2 - d)| / (2 h), the scale against
+    which the sum's cancellation (and so its rounding) is measured."""
     trp = inv.forward_traces(inv.assemble(params + h * vp, field0 + h * vf))
     trm = inv.forward_traces(inv.assemble(params - h * vp, field0 - h * vf))
     diff = (trp - trm)[1:]
     mean = 0.5 * (trp + trm)[1:] - data[1:]
-    return float((diff * mean).sum()) / (2.0 * h)
+    terms = diff * mean
+    fd = float(terms.sum()) / (2.0 * h)
+    if with_scale:
+        return fd, float(terms.abs().sum()) / (2.0 * h)
+    return fd
 
 
 class Misfit(torch.autograd.Function):
