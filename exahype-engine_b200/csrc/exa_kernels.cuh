@@ -99,7 +99,8 @@ struct Shape {
   static constexpr int nd = DIM == 3 ? n * n * n : n * n;  // nodes per cell
   static constexpr int nf = DIM == 3 ? n * n : n;          // nodes per face
   static constexpr int NL = nd / n;                        // lines per direction
-  static constexpr int CPB = nd >= 256 ? 1 : 256 / nd;     // cells per CTA
+  // cells per CTA: about 256 threads, at most 32 cells (the predictors' per-CTA cell masks)
+  static constexpr int CPB = nd >= 256 ? 1 : (256 / nd > 32 ? 32 : 256 / nd);
   static constexpr int TPB = (CPB * nd + 31) / 32 * 32;    // whole warps; the tail threads idle
   static constexpr int sizeQhb = 2 * DIM * nf * D;
   static constexpr int sizeFhb = 2 * DIM * nf * V;

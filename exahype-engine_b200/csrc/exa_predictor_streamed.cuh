@@ -46,7 +46,6 @@ predictor_streamed_kernel(CellArgs a) {
   constexpr int n = T::n, V = T::V, D = T::D, nd = T::nd, NL = T::NL, BS = T::BS, nf = S::nf;
   static_assert(!PDE::kNCP, "the streamed predictor is built for PDEs without NCP");
   static_assert(T::TPB <= 1024, "one thread per node");
-  static_assert(T::TPB == nd, "each flux slot is written and read by its own node's thread");
   extern __shared__ double smem[];
   double* sF = smem;                          // [DIM][V][BS]
   constexpr int DP = T::DP;
@@ -61,7 +60,9 @@ predictor_streamed_kernel(CellArgs a) {
   __shared__ int s_grid;
 
   const int p = threadIdx.x;
-  const bool live_node = T::TPB == nd || p < nd;  // whole warps of nodes: every thread has one
+  // the tail threads of the last warp (n^3 not a multiple of 32: N = 8, 9) own no node; they
+  // take line items in the contractions and the extrapolation only
+  const bool live_node = T::TPB == nd || p < nd;
   int co[3] = {0, 0, 0};
   node_coords<DIM, n>(live_node ? p : 0, co);
   {
@@ -237,7 +238,7 @@ predictor_streamed_kernel(CellArgs a) {
             }
           }
           // no barrier: the next phase 1 rewrites only this thread's own flux slots, which this
-          // thread has just read (every node has its own thread: TPB == nd is asserted below)
+          // thread has just read (every node's slots are written and read by its own thread)
         }
       }
       // iK1 time solve (:370-405) per node, in place over the rhs slices (all n slices of a

@@ -33,6 +33,13 @@
  * node's values at position x (exa_patch_adjust_solution). Every kernel -- FP64 and mixed
  * predictors, Riemann, boundary, update and CFL -- is instantiated for the functor.
  *
+ * ORDER runs over 1..9 in 2D and 3D, the orders of the reference's generated quadrature tables.
+ * A cell whose space-time Picard state (n^(DIM+1) * D doubles, n = ORDER + 1) does not fit one
+ * CTA's shared memory runs the streamed predictor, which keeps that state in an L2-resident
+ * scratch. That predictor takes systems without an NCP, and one time node's fluxes
+ * (DIM * V * n^DIM doubles) must still fit the CTA. A static_assert names an instantiation that
+ * fits neither form.
+ *
  * Build with the same flags as the library (exahype-engine_b200/build.py: build_user_pde does it),
  * linking libexa_aderdg.so. Loading the application's library registers its instantiations; from
  * then on exa_solver_create accepts cfg.pde = the registered id through the unchanged C ABI, and

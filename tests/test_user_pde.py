@@ -5,7 +5,9 @@ adjustPointSolution, AbstractGenericADERDGSolverHeader.template:34-68, 220-338).
 tests/user_pde/user_euler.cu is such an application: Euler written from the reference's Euler app,
 with its own boundary_values (a reflective wall) and adjust_point_solution (a density wave), built
 into tests/user_pde/libuser_euler.so by the build step. Loading it registers pde EXA_PDE_USER_BASE
-for 3D and 2D order 3; the GPU tests run it through the unchanged C ABI against the oracle.
+for order 3 in 2D and 3D and for the extreme orders (1 and 9 in 2D; 1, 8 and 9 in 3D, where the
+largest cells run the streamed predictor with idle tail threads); the GPU tests run it through the
+unchanged C ABI against the oracle.
 """
 import ctypes
 import os
@@ -31,6 +33,8 @@ def test_user_pde_registers_its_instantiations():
     exa = _load()
     base = exa.PDE_USER_BASE
     assert exa.pde_available(base, 3, 3, 0) and exa.pde_available(base, 2, 3, 0)
+    for dim, order in [(2, 1), (2, 9), (3, 1), (3, 8), (3, 9)]:
+        assert exa.pde_available(base, dim, order, 0)
     assert not exa.pde_available(base, 3, 5, 0) and not exa.pde_available(base + 1, 3, 3, 0)
     assert exa.pde_available(exa.PDE_EULER, 3, 5, 0)
     lib = exa.load_library()
@@ -51,8 +55,12 @@ def density_wave(x, dim):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("dim,ncell,bc", [(3, (4, 3, 5), 4), (3, (3, 4, 3), 0), (2, (9, 7), 4), (2, (8, 6), 0)])
-def test_user_pde_adjust_and_steps_vs_oracle(dim, ncell, bc):
+@pytest.mark.parametrize("dim,ncell,bc,order", [
+    (3, (4, 3, 5), 4, 3), (3, (3, 4, 3), 0, 3), (2, (9, 7), 4, 3), (2, (8, 6), 0, 3),
+    # the extreme orders: 2D order 1 (32 cells per CTA, a ragged last CTA), 2D order 9, 3D order 1,
+    # 3D orders 8 and 9 (729 and 1000 nodes: the streamed predictor, tail threads without a node)
+    (2, (13, 7), 4, 1), (2, (4, 3), 0, 9), (3, (5, 4, 3), 4, 1), (3, (2, 3, 2), 4, 8), (3, (2, 2, 3), 0, 9)])
+def test_user_pde_adjust_and_steps_vs_oracle(dim, ncell, bc, order):
     """adjust_point_solution sets the initial state on the device (checked against the numpy
     restatement at the nodal positions); then 3 steps with the application's boundary_values on
     every domain face (EXA_BC_USER) or periodic, against the oracle's Euler system with reflective
@@ -60,7 +68,6 @@ def test_user_pde_adjust_and_steps_vs_oracle(dim, ncell, bc):
     import exa_scenarios as sc
     from pyoracle import Oracle
     exa = _load()
-    order = 3
     size = [1.0, 0.8, 1.2][:dim]
     s = exa.Solver(exa.PDE_USER_BASE, dim, order)
     p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
@@ -69,13 +76,17 @@ def test_user_pde_adjust_and_steps_vs_oracle(dim, ncell, bc):
     want = density_wave(sc.nodal_positions(ncell, size, order), dim)
     assert np.max(np.abs(luh0 - want)) <= 1e-14 * np.max(np.abs(want))
     ref = luh0.copy()
-    t_ref, _, _ = Oracle(dim, order).run(ref, ncell, size, 3, walls=bc == 4)
+    t_ref, _, pic = Oracle(dim, order).run(ref, ncell, size, 3, walls=bc == 4, want_picard=True)
     p.step(3)
     got = p.get_solution()
     assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
     assert float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))) < TOL
     assert np.abs(got - luh0).max() > 1e-4
-    assert p.status() == 0
+    # equal Picard sweeps in the last step; at order 1 some cells use all 2(N+1) sweeps in the
+    # oracle too, and the patch reports that as EXA_ST_PICARD_CAP, not as an error
+    assert list(np.bincount(pic[-1], minlength=32)[:32]) == p.stats()["picard_hist"]
+    capped = bool((pic == 2 * (order + 1)).any())
+    assert p.status() == (exa.ST_PICARD_CAP if capped else 0)
     p.close()
     s.close()
 

@@ -5,8 +5,9 @@
 //   - adjust_point_solution: at t = 0 a smooth density wave advected by a uniform velocity,
 //     rho = 1 + 0.1 sin(2 pi (x + 2y + 3z)), u = (0.3, 0.2, 0.1), p = 1 (2D: z = 0, w = 0);
 //   - boundary_values: a reflective wall (mirrored normal momentum, the normal flux of that state).
-// Registered as pde EXA_PDE_USER_BASE for 3D order 3 and 2D order 3 (no parameters). Used only by
-// the tests, which check it against the oracle's Euler system.
+// Registered as pde EXA_PDE_USER_BASE for order 3 in 2D and 3D, and for the extreme orders of the
+// reference's tables: 1 and 9 in 2D, 1, 8 and 9 in 3D (no parameters). Used only by the tests, which
+// check it against the oracle's Euler system.
 #include "exa_aderdg_user.cuh"
 
 struct UserEuler {
@@ -78,3 +79,10 @@ struct UserEuler {
 
 EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 3, 3, 0)
 EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 2, 3, 0)
+// the smallest cells (2D order 1: 4 nodes, 32 cells per CTA) and the largest (3D order 8 and 9: 729
+// and 1000 nodes, the streamed predictor with tail threads that own no node)
+EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 2, 1, 0)
+EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 2, 9, 0)
+EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 3, 1, 0)
+EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 3, 8, 0)
+EXA_REGISTER_PDE(EXA_PDE_USER_BASE, UserEuler, 3, 9, 0)
