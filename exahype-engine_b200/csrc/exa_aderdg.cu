@@ -112,6 +112,12 @@ struct exa_solver {
   int* d_iscratch = nullptr;
   int pred_variant = -1;  // predictor launch variant (-1: the measured one)
   int upd_variant = -1;   // update launch variant (-1: bulk-copy form where possible)
+  // device memory goes with the handle, also when exa_solver_create fails half-way
+  ~exa_solver() {
+    cudaFree(d_status);
+    cudaFree(d_scratch);
+    cudaFree(d_iscratch);
+  }
 };
 
 static exa::CellArgs base_args(exa_solver* s, int ncells) {
@@ -186,9 +192,6 @@ int exa_solver_create(const exa_solver_config* cfg, exa_solver** out) {
 
 int exa_solver_destroy(exa_solver* s) {
   if (!s) return EXA_OK;
-  cudaFree(s->d_status);
-  cudaFree(s->d_scratch);
-  cudaFree(s->d_iscratch);
   delete s;
   return EXA_OK;
 }
@@ -324,11 +327,12 @@ int exa_solution_update(exa_solver* s, int ncells, double* luh, const double* lu
   return EXA_OK;
 }
 
-int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
-                              double* dt_min, void* stream) {
-  if (!s || ncells < 0 || (ncells > 0 && (!luh || !dx))) return fail(EXA_ERR_INVALID, "null argument");
-  std::lock_guard<std::mutex> lk(s->mu);
-  cudaStream_t st = (cudaStream_t)stream;
+}  // extern "C"
+
+// exa_stable_time_step_size with the solver's lock already held (the per-cell shim keeps it over
+// its copies, so that no other thread can move the scratch in between)
+static int stable_dt_locked(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
+                            double* dt_min, cudaStream_t st) {
   exa::CellArgs a = base_args(s, ncells);
   a.luh = luh;
   a.cell_dt = cell_dt;
@@ -347,6 +351,15 @@ int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, cons
     EXA_CUDA(cudaStreamSynchronize(st));
   }
   return EXA_OK;
+}
+
+extern "C" {
+
+int exa_stable_time_step_size(exa_solver* s, int ncells, const double* luh, const double* dx, double* cell_dt,
+                              double* dt_min, void* stream) {
+  if (!s || ncells < 0 || (ncells > 0 && (!luh || !dx))) return fail(EXA_ERR_INVALID, "null argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  return stable_dt_locked(s, ncells, luh, dx, cell_dt, dt_min, (cudaStream_t)stream);
 }
 
 // ---- per-cell shims on host pointers ---------------------------------------------------------
@@ -515,22 +528,14 @@ int exa_solutionUpdate(exa_solver* s, double* luh, const double* luhOld, const d
 
 int exa_stableTimeStepSize(exa_solver* s, const double* luh, const double* dx, double* dt) {
   if (!s || !luh || !dx || !dt) return fail(EXA_ERR_INVALID, "null argument");
-  double* d_luh = nullptr;
-  {
-    std::lock_guard<std::mutex> lk(s->mu);
-    if (int e = shim_scratch(s, s->ops->sz_luh + 8)) return e;
-    d_luh = s->d_scratch + 8;
-    EXA_CUDA(cudaMemcpy(d_luh, luh, s->ops->sz_luh * sizeof(double), cudaMemcpyHostToDevice));
-  }
-  double* cell = nullptr;
-  EXA_CUDA(cudaMalloc(&cell, sizeof(double)));
-  int r = exa_stable_time_step_size(s, 1, d_luh, dx, cell, nullptr, 0);
-  if (r == EXA_OK) {
-    cudaError_t e = cudaMemcpy(dt, cell, sizeof(double), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) r = cuda_fail(e, "copy dt");
-  }
-  cudaFree(cell);
-  return r;
+  std::lock_guard<std::mutex> lk(s->mu);
+  // scratch: the cell's dt in entry 0, its luh from entry 8 on
+  if (int e = shim_scratch(s, s->ops->sz_luh + 8)) return e;
+  double* d_luh = s->d_scratch + 8;
+  EXA_CUDA(cudaMemcpy(d_luh, luh, s->ops->sz_luh * sizeof(double), cudaMemcpyHostToDevice));
+  if (int r = stable_dt_locked(s, 1, d_luh, dx, s->d_scratch, nullptr, 0)) return r;
+  EXA_CUDA(cudaMemcpy(dt, s->d_scratch, sizeof(double), cudaMemcpyDeviceToHost));
+  return EXA_OK;
 }
 
 // ---- mesh levels and the limiter ------------------------------------------------------------

@@ -239,6 +239,40 @@ def test_batched_riemann_surface_update_cfl_vs_oracle(exa, torch, dim, order):
     assert dtmin == ref_dt.min()
 
 
+def test_per_cell_shims_from_many_host_threads(exa):
+    """The per-cell shims on one solver from eight host threads at once, as the reference's TBB jobs
+    call its kernels on different cells (ADERDGSolver.cpp:726-729, 769-773): every result equals the
+    one-thread result bit for bit and the oracle's at 1e-12 (the per-cell CFL step at 1e-15). The
+    shims serialise on the solver's lock; exa_stableTimeStepSize keeps it over its copies, so no
+    other thread can move the shared scratch between its upload and its kernel."""
+    import concurrent.futures
+    rng = np.random.default_rng(11)
+    dim, order, ncells = 3, 3, 48
+    nd = (order + 1) ** dim
+    o = Oracle(dim, order)
+    s = exa.Solver(exa.PDE_EULER, dim, order)
+    cells = euler_cells(rng, ncells, nd).reshape(ncells, -1)
+    lduh = rng.normal(size=(ncells, nd * 5)) * 0.01
+    dx = np.array([0.1, 0.07, 0.05])
+
+    def work(c):
+        r = s.space_time_predictor(cells[c], dx, 1e-3)
+        return (r["lQhbnd"], r["lFhbnd"], s.volume_integral_cell(r["lFhi"], dx),
+                s.solution_update_cell(cells[c], lduh[c], 1e-3), s.stable_time_step_size_cell(cells[c], dx))
+
+    with concurrent.futures.ThreadPoolExecutor(8) as ex:
+        got = list(ex.map(work, range(ncells)))
+    for c in range(ncells):
+        for a, b in zip(got[c], work(c)):
+            assert np.array_equal(a, b), c
+        r = o.predictor(cells[c], dx, 1e-3)
+        assert rel(got[c][0], r["lQhbnd"]) < TOL and rel(got[c][1], r["lFhbnd"]) < TOL
+        assert rel(got[c][2], o.volume(r["lFhi"], dx)) < TOL
+        assert rel(got[c][3], o.update(cells[c], lduh[c], 1e-3)) < TOL
+        assert abs(got[c][4] - o.dt(cells[c], dx)) <= 1e-15 * o.dt(cells[c], dx)
+    assert s.status() == 0
+
+
 # ------------------------------------------------------------------------------------------
 # whole steps on device-resident patches vs the oracle's patch driver
 # ------------------------------------------------------------------------------------------
