@@ -65,6 +65,9 @@ def parse():
                          "0 one cell group per CTA, 1 persistent (mixed: 2 or 3 CTAs per SM)")
     ap.add_argument("--update-variant", type=int, default=-1, choices=[-1, 0, 1],
                     help="launch form of the Rusanov and update kernels: 0 per-thread loads, 1/-1 bulk copies")
+    ap.add_argument("--max-picard", type=int, default=0,
+                    help="euler3d: a fixed Picard sweep count (the reference's UseMaxPicardIterations mode); "
+                         "0 = the residual test (the benchmark); used to measure per-sweep costs")
     ap.add_argument("--no-workloads", action="store_true",
                     help="euler3d at N=1: skip the short runs of the other configurations (the workloads record)")
     return ap.parse_args()
@@ -222,6 +225,12 @@ PRED_BYTES_PER_CELL = 8.0 * (1080 + 1080 + 1080 + 1080)  # luh in; lduh, lQhbnd,
 # DRAM bytes per cell of one predictor launch measured by ncu on a 27^3 block (19,683 cells):
 # 172.00 MB read + 466.63 MB written
 PRED_DRAM_BYTES_PER_CELL = (171.954432e6 + 462.412288e6) / 19683
+# FP64 operations the FP64 predictor (3D Euler N=5) executes per cell, from ncu's SASS counters
+# (2 dfma + dadd + dmul, predicated on) of launches on a 27^3 block with a fixed 2 and 4 sweeps:
+# 14,437,695,109 and 31,836,609,564 per launch. Sweep 0 (closed form) with the tail costs less
+# than the algorithmic count credits it; a further sweep costs more (residual, rhs scaling).
+PRED_EXEC_FLOPS_SWEEP0_TAIL = 291532.69
+PRED_EXEC_FLOPS_PER_SWEEP = 441978.22
 
 
 def cpu_baseline(steps=20, kind="reference"):
@@ -693,7 +702,7 @@ def main():
     dof_step = cells * NVAR * (ORDER + 1) ** 3
 
     precision = exa.PREC_MIXED if args.precision == "mixed" else exa.PREC_FP64
-    solver = exa.Solver(exa.PDE_EULER, 3, ORDER, precision=precision)
+    solver = exa.Solver(exa.PDE_EULER, 3, ORDER, precision=precision, max_picard=args.max_picard)
     solver.set_update_variant(args.update_variant)
     solver.predictor_variant = args.predictor_variant
     # every rank owns one 81^3 slab of an 81 x 81 x (81 N) periodic grid (dx = 1/81 everywhere)
@@ -815,6 +824,7 @@ def main():
                if world == 1 else None)
     flops_launch = cells * (395280.0 * mean_sweeps + 116640.0)
     achieved = flops_launch / (pred_ms * 1e-3) / 1e12
+    exec_flops = cells * (PRED_EXEC_FLOPS_SWEEP0_TAIL + (mean_sweeps - 1.0) * PRED_EXEC_FLOPS_PER_SWEEP)
 
     # ---- end to end through the C ABI with host buffers: H2D state, step, D2H state ----
     e2e = None
@@ -865,7 +875,8 @@ def main():
                                "per step on 1 GPU; halo exchange + dt all-reduce over NCCL on N GPUs"
                                % (ncell[0], ncell[0], ncell[1], ncell[2] * world),
                    "cells": cells, "dof_per_step": dof_step, "l2": "inputs 4.6 GB > L2, no flush needed",
-                   "precision": args.precision},
+                   "precision": args.precision,
+                   "picard": "fixed %d sweeps" % args.max_picard if args.max_picard > 0 else "residual test"},
         "cell_updates_per_s": world * cells / (ms * 1e-3),
         "picard_sweeps_mean": stats["picard_mean"], "status_bits": status,
         "accuracy": {"t": float(t_now[0]), "l2_rho_vs_exact": l2_exact, "linf_rho_vs_exact": linf_exact,
@@ -878,6 +889,12 @@ def main():
                      "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one predictor launch "
                                        "on a 27^3 block, scaled by cells",
                      "algorithmic_flops_per_launch": flops_launch, "launch_ms": pred_ms,
+                     "executed_flops_per_launch": exec_flops if args.precision == "fp64" else None,
+                     "executed_tflops": exec_flops / (pred_ms * 1e-3) / 1e12 if args.precision == "fp64" else None,
+                     "executed_frac": (exec_flops / (pred_ms * 1e-3) / 1e12 / fp64_peak
+                                       if args.precision == "fp64" else None),
+                     "executed_source": "per-cell FP64 operations of the kernel from ncu SASS counters (27^3, "
+                                        "fixed 2 and 4 sweeps) x the launch's cells and mean sweeps",
                      "hbm_gbs_of_launch": cells * PRED_BYTES_PER_CELL / (pred_ms * 1e-3) / 1e9,
                      "hbm_peak_gbs": pk.get("hbm_gbs"), "hbm_peak_source": pk_kind},
         "gpu_launches": K * 4,
