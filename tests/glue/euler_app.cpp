@@ -1,9 +1,11 @@
 // An application on the generated glue: the user's solver class derives from the generated
 // Euler::AbstractEulerSolver_ADERDG (exahype-engine_b200/glue/generate_glue.py with
 // euler_glue_spec.json) and supplies its host-side boundaryValues, a reflective wall as in the
-// reference's Euler and SWE applications (SWE_ADERDG/MySWESolver.cpp:43-62). The extern "C"
-// functions let the tests drive the glue methods the way the reference's engine calls them.
+// reference's Euler and SWE applications (SWE_ADERDG/MySWESolver.cpp:43-62), and its
+// adjustPointSolution, a density wave at t = 0. The extern "C" functions let the tests drive the
+// glue methods the way the reference's engine calls them.
 #include <algorithm>
+#include <cmath>
 
 #include "AbstractEulerSolver_ADERDG.h"
 
@@ -28,6 +30,15 @@ class EulerSolver_ADERDG : public AbstractEulerSolver_ADERDG {
     stateOut[1 + normalNonZero] = -stateOut[1 + normalNonZero];
     flux(stateOut, fluxOut, normalNonZero);
   }
+  // rho = 1 + 0.1 sin(2 pi (x + 2y + 3z)), u = (0.3, 0.2, 0.1), p = 1
+  void adjustPointSolution(const double* const x, const double t, const double, double* const Q) override {
+    if (t != 0.0) return;
+    const double rho = 1.0 + 0.1 * std::sin(2.0 * 3.14159265358979323846 * (x[0] + 2.0 * x[1] + 3.0 * x[2]));
+    const double u[3] = {0.3, 0.2, 0.1};
+    Q[0] = rho;
+    for (int d = 0; d < 3; d++) Q[1 + d] = rho * u[d];
+    Q[4] = 1.0 / 0.4 + 0.5 * rho * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+  }
 };
 }  // namespace Euler
 
@@ -48,8 +59,23 @@ void glue_boundary(void* h, double* fluxIn, const double* stateIn, const double*
   static_cast<Euler::EulerSolver_ADERDG*>(h)->boundaryConditions(fluxIn, stateIn, nullptr, nullptr, centre, size, t,
                                                                  dt, d, o);
 }
-void glue_face(void* h, double* lduh, const double* lFhbnd, int d, int o, const double* dx) {
-  static_cast<Euler::EulerSolver_ADERDG*>(h)->faceIntegral(lduh, lFhbnd, d, o, dx);
+void glue_face(void* h, double* out, const double* lFhbnd, int d, int o, const int* subface, int levelDelta,
+               const double* dx, double dt, int addToUpdate) {
+  static_cast<Euler::EulerSolver_ADERDG*>(h)->faceIntegral(out, lFhbnd, d, o, subface, levelDelta, dx, dt,
+                                                           addToUpdate != 0);
+}
+void glue_adjust(void* h, double* luh, const double* centre, const double* size, double t, double dt) {
+  static_cast<Euler::EulerSolver_ADERDG*>(h)->adjustSolution(luh, centre, size, t, dt);
+}
+void glue_volume_prolong(void* h, double* fine, const double* coarse, int lc, int lf, const int* sub) {
+  static_cast<Euler::EulerSolver_ADERDG*>(h)->volumeUnknownsProlongation(fine, coarse, lc, lf, sub);
+}
+void glue_volume_restrict(void* h, double* coarse, const double* fine, int lc, int lf, const int* sub) {
+  static_cast<Euler::EulerSolver_ADERDG*>(h)->volumeUnknownsRestriction(coarse, fine, lc, lf, sub);
+}
+void glue_face_prolong(void* h, double* qf, double* ff, const double* qc, const double* fc, int lc, int lf,
+                       const int* sub) {
+  static_cast<Euler::EulerSolver_ADERDG*>(h)->faceUnknownsProlongation(qf, ff, qc, fc, lc, lf, sub);
 }
 void glue_update(void* h, double* luh, const double* luhOld, const double* lduh, double dt) {
   static_cast<Euler::EulerSolver_ADERDG*>(h)->addUpdateToSolution(luh, luhOld, lduh, dt);

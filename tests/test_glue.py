@@ -57,7 +57,11 @@ def _glue():
     lib.glue_predictor.restype = i
     lib.glue_riemann.argtypes = [vp, vp, vp, vp, vp, d, d, vp, i]
     lib.glue_boundary.argtypes = [vp, vp, vp, vp, vp, d, d, i, i]
-    lib.glue_face.argtypes = [vp, vp, vp, i, i, vp]
+    lib.glue_face.argtypes = [vp, vp, vp, i, i, vp, i, vp, d, i]
+    lib.glue_adjust.argtypes = [vp, vp, vp, vp, d, d]
+    lib.glue_volume_prolong.argtypes = [vp, vp, vp, i, i, vp]
+    lib.glue_volume_restrict.argtypes = [vp, vp, vp, i, i, vp]
+    lib.glue_face_prolong.argtypes = [vp, vp, vp, vp, vp, i, i, vp]
     lib.glue_update.argtypes = [vp, vp, vp, vp, d]
     lib.glue_dt.argtypes = [vp, vp, vp]
     lib.glue_dt.restype = d
@@ -69,7 +73,8 @@ def _glue():
 def test_glue_library_exports_the_engine_entry_points():
     lib = _glue()
     for name in ("glue_create", "glue_predictor", "glue_riemann", "glue_boundary", "glue_face", "glue_update",
-                 "glue_dt", "glue_grid"):
+                 "glue_dt", "glue_grid", "glue_adjust", "glue_volume_prolong", "glue_volume_restrict",
+                 "glue_face_prolong"):
         assert hasattr(lib, name)
 
 
@@ -117,11 +122,16 @@ def test_glue_methods_vs_oracle():
     ra, rb = o.riemann(FL, FR, QL, QR, dx, 2)
     assert rel(a, ra) < TOL and rel(b, rb) < TOL
     du = rng.normal(size=nd * 5)
+    no_sub = np.zeros(2, dtype=np.int32)
     for d in range(3):
         for ori in (0, 1):
             x = du.copy()
-            lib.glue_face(h, _p(x), _p(FL), d, ori, _p(dx))
+            lib.glue_face(h, _p(x), _p(FL), d, ori, _p(no_sub), 0, _p(dx), dt, 1)
             assert rel(x, o.face(du, FL, d, ori, dx)) < 1e-14
+    # addToUpdate = false: the face integral goes straight into the solution
+    x = luh.copy()
+    lib.glue_face(h, _p(x), _p(FL), 1, 0, _p(no_sub), 0, _p(dx), dt, 0)
+    assert rel(x, o.update(luh, o.face(np.zeros(nd * 5), FL, 1, 0, dx), dt)) < 1e-14
     out = luh.copy()
     lib.glue_update(h, _p(out), _p(luh), _p(du), dt)
     assert rel(out, o.update(luh, du, dt)) < 1e-14
@@ -184,7 +194,8 @@ def test_glue_engine_loop_and_uniform_grid_vs_oracle():
         l = lduh[c].copy()
         for d in range(3):
             for ori in (0, 1):
-                lib.glue_face(h, _p(l), _p(np.ascontiguousarray(fhb[c, 2 * d + ori])), d, ori, _p(dx))
+                lib.glue_face(h, _p(l), _p(np.ascontiguousarray(fhb[c, 2 * d + ori])), d, ori,
+                                  _p(np.zeros(2, dtype=np.int32)), 0, _p(dx), dt, 1)
         out = luh[c].copy()
         lib.glue_update(h, _p(out), _p(np.ascontiguousarray(luh[c])), _p(l), dt)
         luh[c] = out
@@ -198,4 +209,59 @@ def test_glue_engine_loop_and_uniform_grid_vs_oracle():
     ref3 = luh0.reshape(-1).copy()
     t3, _, _ = Oracle(3, 3).run(ref3, ncell, list(size), 3)
     assert rel(grid, ref3) < TOL and abs(t.value - t3) <= 1e-13 * t3
+    lib.glue_destroy(h)
+
+
+@pytest.mark.gpu
+def test_glue_mesh_levels_adjust_and_coarse_face_integral_vs_reference():
+    """The glue's mesh-level methods (volumeUnknownsProlongation / Restriction,
+    faceUnknownsProlongation) and faceIntegral on the face of a coarser neighbour (levelDelta > 0:
+    faceUnknownsRestriction of the flux, then the face integral with the coarse cell size) against
+    the reference's own kernels (oracle/_ref), and adjustSolution with the application's
+    adjustPointSolution against its numpy restatement."""
+    from pyoracle import Oracle, RefAmrLimiter
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "libexaref_amrlim3d.so")):
+        pytest.skip("oracle/_ref not built")
+    lib = _glue()
+    h = lib.glue_create()
+    o, ref = Oracle(3, 3), RefAmrLimiter(3, 5, 0)
+    rng = np.random.default_rng(43)
+    nd, nf = 64, 16
+    # adjustSolution: rho = 1 + 0.1 sin(2 pi (x + 2y + 3z)) at the nodes, z slowest
+    centre, size = np.array([0.3, 0.4, 0.5]), np.array([0.1, 0.2, 0.05])
+    luh = np.zeros(nd * 5)
+    lib.glue_adjust(h, _p(luh), _p(centre), _p(size), 0.0, 0.0)
+    nodes = o.tables()["nodes"]
+    z, y, x = np.meshgrid(nodes, nodes, nodes, indexing="ij")
+    X = np.stack([centre[0] + size[0] * (x - 0.5), centre[1] + size[1] * (y - 0.5),
+                  centre[2] + size[2] * (z - 0.5)], -1).reshape(-1, 3)
+    rho = 1.0 + 0.1 * np.sin(2.0 * np.pi * (X[:, 0] + 2.0 * X[:, 1] + 3.0 * X[:, 2]))
+    assert np.max(np.abs(luh.reshape(nd, 5)[:, 0] - rho)) <= 1e-15
+    assert np.max(np.abs(luh.reshape(nd, 5)[:, 4] - (2.5 + 0.5 * rho * 0.14))) <= 1e-14
+    # volume prolongation / restriction over two levels
+    coarse = euler_cells(rng, 1, nd).reshape(-1)
+    sub = np.array([2, 0, 1], dtype=np.int32)
+    fine = np.zeros(nd * 5)
+    lib.glue_volume_prolong(h, _p(fine), _p(coarse), 1, 3, _p(sub))
+    assert rel(fine, ref.volume(0, np.zeros(nd * 5), coarse, 1, 3, sub)) < TOL
+    acc = coarse.copy()
+    lib.glue_volume_restrict(h, _p(acc), _p(fine), 1, 3, _p(sub))
+    assert rel(acc, ref.volume(1, coarse, fine, 1, 3, sub)) < TOL
+    # face prolongation
+    qc, fc = euler_cells(rng, 1, nf).reshape(-1), rng.normal(size=nf * 5)
+    sf = np.array([1, 2], dtype=np.int32)
+    qf, ff = np.zeros(nf * 5), np.zeros(nf * 5)
+    lib.glue_face_prolong(h, _p(qf), _p(ff), _p(qc), _p(fc), 0, 1, _p(sf))
+    wq, wf = ref.face(0, np.zeros(nf * 5), np.zeros(nf * 5), qc, fc, 0, 1, sf)
+    assert rel(qf, wq) < TOL and rel(ff, wf) < TOL
+    # faceIntegral from a fine face into the coarse neighbour's update
+    dx = np.array([0.05, 0.05, 0.05])
+    du = rng.normal(size=nd * 5)
+    fine_flux = rng.normal(size=nf * 5)
+    for delta, sfi in ((1, [2, 1]), (2, [5, 7])):
+        sfi = np.array(sfi, dtype=np.int32)
+        out = du.copy()
+        lib.glue_face(h, _p(out), _p(fine_flux), 2, 1, _p(sfi), delta, _p(dx), 1e-3, 1)
+        _, cflux = ref.face(2, np.zeros(nf * 5), np.zeros(nf * 5), np.zeros(nf * 5), fine_flux, 0, delta, sfi)
+        assert rel(out, o.face(du, cflux, 2, 1, dx * 3 ** delta)) < 1e-13
     lib.glue_destroy(h)
