@@ -848,6 +848,10 @@ struct exa_patch {
   long long halo_lo_first = 0, halo_hi_first = 0;  // first real cell of the low / high boundary layer
   // discrete adjoint workspace (allocated on the first exa_patch_adjoint_step)
   double *adjQ = nullptr, *adjF = nullptr, *adj_iter = nullptr;
+  // halo patches: lambda of the real cells and, after them, of the ghost cells (the neighbours'
+  // boundary layers), which the transposed halo faces read
+  double* adj_lam = nullptr;
+  bool adj_forward_done = false;  // EXA_ADJ_FORWARD ran and EXA_ADJ_REVERSE has not yet
   // host-buffer steps: copy stream and per-chunk events (created on the first exa_patch_step_host)
   cudaStream_t copy_stream = nullptr, d2h_stream = nullptr;
   std::vector<cudaEvent_t> ev_in, ev_upd, ev_out;
@@ -859,7 +863,7 @@ static void patch_free(exa_patch* p) {
   if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
   void* ptrs[] = {p->luh, p->lduh, p->lQhbnd, p->lFhbnd, p->picard, p->cell_grid, p->grid_dx, p->grid_t,
                   p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status,
-                  p->grid_geo, p->grid_first_d, p->src, p->btype, p->adjQ, p->adjF, p->adj_iter};
+                  p->grid_geo, p->grid_first_d, p->src, p->btype, p->adjQ, p->adjF, p->adj_iter, p->adj_lam};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (cudaEvent_t e : p->ev_in) cudaEventDestroy(e);
@@ -1567,44 +1571,119 @@ int exa_patch_set_time(exa_patch* p, double t) {
   return EXA_OK;
 }
 
-int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
-  if (!p || !lambda) return fail(EXA_ERR_INVALID, "null argument");
+}  // extern "C"
+
+// checks and workspace of an adjoint step; the face-trace adjoints cover the ghost cells too
+static int adjoint_prepare(exa_patch* p, double dt) {
   exa::Ops& o = *p->s->ops;
   if (!o.adjoint_ok) return fail(EXA_ERR_UNSUPPORTED, "the adjoint is built for the acoustic and elastic systems");
   const int S = p->s->cfg.max_picard;
   if (S <= 0) return fail(EXA_ERR_UNSUPPORTED, "the adjoint needs a fixed Picard sweep count (max_picard > 0)");
   if (p->s->cfg.precision != EXA_PREC_FP64) return fail(EXA_ERR_UNSUPPORTED, "the adjoint runs in FP64");
-  if (p->halo_axis >= 0) return fail(EXA_ERR_UNSUPPORTED, "the adjoint of a slab with halo faces is not built");
   if (p->has_user_bc) return fail(EXA_ERR_UNSUPPORTED, "the adjoint supports periodic, wall and outflow faces");
   if (!(dt > 0)) return fail(EXA_ERR_INVALID, "the adjoint needs the fixed time step of the forward step");
-  const size_t nc = (size_t)p->ncells;
-  if (!p->adjQ) EXA_CUDA(cudaMalloc(&p->adjQ, nc * o.sz_qhb * sizeof(double)));
-  if (!p->adjF) EXA_CUDA(cudaMalloc(&p->adjF, nc * o.sz_fhb * sizeof(double)));
+  const size_t nc = (size_t)p->ncells, nt = nc + (size_t)p->nghost;
+  if (!p->adjQ) EXA_CUDA(cudaMalloc(&p->adjQ, nt * o.sz_qhb * sizeof(double)));
+  if (!p->adjF) EXA_CUDA(cudaMalloc(&p->adjF, nt * o.sz_fhb * sizeof(double)));
   if (!p->adj_iter) EXA_CUDA(cudaMalloc(&p->adj_iter, nc * (size_t)S * o.sz_lQi / (o.nvar + o.npar) * o.nvar * sizeof(double)));
+  if (p->nghost > 0 && !p->adj_lam) EXA_CUDA(cudaMalloc(&p->adj_lam, nt * o.sz_luh * sizeof(double)));
   const int ng = (int)p->grids.size();
   if (dt != p->fixed_dt) {
     exa::fill_kernel<<<(ng + 127) / 128, 128, 0, p->stream>>>(ng, p->grid_dt, dt);
     EXA_CUDA(cudaGetLastError());
     p->fixed_dt = dt;
   }
-  // forward predictor at u_k: the face traces the Rusanov adjoint linearises around, and the
-  // Picard iterates the reverse sweeps need (written into the adjoint scratch)
+  return EXA_OK;
+}
+
+// forward predictor at u_k: the face traces the Rusanov adjoint linearises around, and the Picard
+// iterates the reverse sweeps need (written into the adjoint scratch)
+static int adjoint_forward(exa_patch* p) {
   exa::CellArgs c = patch_args(p);
   c.ex_iter = p->adj_iter;
-  EXA_CUDA(o.predictor(c, p->stream, false, p->s->pred_variant));
-  c.ex_iter = nullptr;
+  EXA_CUDA(p->s->ops->predictor(c, p->stream, false, p->s->pred_variant));
+  return EXA_OK;
+}
+
+// transposed faces (interior, halo and domain) and transposed predictors; lam holds the real
+// cells' lambda, followed by the ghost cells' on a halo patch
+static int adjoint_reverse(exa_patch* p, double* lam) {
   exa::AdjArgs a;
-  a.c = c;
+  a.c = patch_args(p);
   a.f = patch_faces(p);
   a.fb = a.f;
   a.fb.nfaces = p->nbfaces;
-  a.lam = lambda;
+  a.lam = lam;
   a.adjQ = p->adjQ;
   a.adjF = p->adjF;
   a.iter = p->adj_iter;
-  a.sweeps = S;
+  a.sweeps = p->s->cfg.max_picard;
   a.have_iter = 1;
   EXA_CUDA(p->s->ops->adjoint(a, p->stream));
+  return EXA_OK;
+}
+
+extern "C" {
+
+int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt) {
+  if (!p || !lambda) return fail(EXA_ERR_INVALID, "null argument");
+  if (p->halo_axis >= 0)
+    return fail(EXA_ERR_INVALID, "a patch with EXA_BC_HALO runs the adjoint through exa_patch_adjoint_phase "
+                                 "and a halo exchange");
+  if (int r = adjoint_prepare(p, dt)) return r;
+  if (int r = adjoint_forward(p)) return r;
+  return adjoint_reverse(p, lambda);
+}
+
+int exa_patch_adjoint_phase(exa_patch* p, int phase, double* lambda, double dt) {
+  if (!p || !lambda) return fail(EXA_ERR_INVALID, "null argument");
+  const exa::Ops& o = *p->s->ops;
+  const size_t bytes = (size_t)p->ncells * o.sz_luh * sizeof(double);
+  if (phase == EXA_ADJ_FORWARD) {
+    if (int r = adjoint_prepare(p, dt)) return r;
+    if (int r = adjoint_forward(p)) return r;
+    if (p->nghost > 0) EXA_CUDA(cudaMemcpyAsync(p->adj_lam, lambda, bytes, cudaMemcpyDeviceToDevice, p->stream));
+    p->adj_forward_done = true;
+    return EXA_OK;
+  }
+  if (phase != EXA_ADJ_REVERSE) return fail(EXA_ERR_INVALID, "unknown adjoint phase");
+  if (!p->adj_forward_done) return fail(EXA_ERR_INVALID, "EXA_ADJ_REVERSE needs EXA_ADJ_FORWARD first");
+  if (dt != p->fixed_dt) return fail(EXA_ERR_INVALID, "EXA_ADJ_REVERSE needs the time step of EXA_ADJ_FORWARD");
+  p->adj_forward_done = false;
+  if (p->nghost == 0) return adjoint_reverse(p, lambda);
+  if (int r = adjoint_reverse(p, p->adj_lam)) return r;
+  EXA_CUDA(cudaMemcpyAsync(lambda, p->adj_lam, bytes, cudaMemcpyDeviceToDevice, p->stream));
+  return EXA_OK;
+}
+
+long long exa_patch_adjoint_halo_doubles(const exa_patch* p) {
+  if (!p || p->halo_axis < 0) return 0;
+  return p->layer * (long long)p->s->ops->sz_luh;
+}
+
+int exa_patch_adjoint_halo_pack(exa_patch* p, double* send_lo, double* send_hi) {
+  if (!p || p->halo_axis < 0) return fail(EXA_ERR_INVALID, "patch has no halo");
+  if (!send_lo || !send_hi) return fail(EXA_ERR_INVALID, "null buffer");
+  if (!p->adj_forward_done) return fail(EXA_ERR_INVALID, "pack lambda between EXA_ADJ_FORWARD and EXA_ADJ_REVERSE");
+  const size_t blk = (size_t)p->s->ops->sz_luh, bytes = (size_t)p->layer * blk * sizeof(double);
+  // the low and the high layer of real cells: lambda of u_{k+1}, as EXA_ADJ_FORWARD took it
+  EXA_CUDA(cudaMemcpyAsync(send_lo, p->adj_lam + (size_t)p->halo_lo_first * blk, bytes, cudaMemcpyDeviceToDevice,
+                           p->stream));
+  EXA_CUDA(cudaMemcpyAsync(send_hi, p->adj_lam + (size_t)p->halo_hi_first * blk, bytes, cudaMemcpyDeviceToDevice,
+                           p->stream));
+  return EXA_OK;
+}
+
+int exa_patch_adjoint_halo_unpack(exa_patch* p, const double* recv_lo, const double* recv_hi) {
+  if (!p || p->halo_axis < 0) return fail(EXA_ERR_INVALID, "patch has no halo");
+  if (!recv_lo || !recv_hi) return fail(EXA_ERR_INVALID, "null buffer");
+  if (!p->adj_forward_done) return fail(EXA_ERR_INVALID, "unpack lambda between EXA_ADJ_FORWARD and EXA_ADJ_REVERSE");
+  const size_t blk = (size_t)p->s->ops->sz_luh, bytes = (size_t)p->layer * blk * sizeof(double);
+  // recv_lo: the lower neighbour's high layer -> low ghost cells; recv_hi: the upper one's low layer
+  EXA_CUDA(cudaMemcpyAsync(p->adj_lam + (size_t)p->ncells * blk, recv_lo, bytes, cudaMemcpyDeviceToDevice,
+                           p->stream));
+  EXA_CUDA(cudaMemcpyAsync(p->adj_lam + ((size_t)p->ncells + p->layer) * blk, recv_hi, bytes,
+                           cudaMemcpyDeviceToDevice, p->stream));
   return EXA_OK;
 }
 

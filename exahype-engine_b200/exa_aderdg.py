@@ -60,6 +60,7 @@ class FaceLists(ctypes.Structure):
 
 PHASE_PREDICTOR, PHASE_FACES, PHASE_UPDATE, PHASE_ADVANCE = 0, 1, 2, 3
 PHASE_FACES_INTERIOR, PHASE_FACES_HALO = 4, 5
+ADJ_FORWARD, ADJ_REVERSE = 0, 1
 BC_HALO, BC_OUTFLOW, BC_USER = 2, 3, 4
 PDE_USER_BASE = 64
 
@@ -137,6 +138,9 @@ def load_library(path=None):
         "exa_patch_step_host": [vp, vp, vp, d],
         "exa_patch_run_host": [vp, vp, vp, i, d],
         "exa_patch_adjoint_step": [vp, vp, d],
+        "exa_patch_adjoint_phase": [vp, i, vp, d],
+        "exa_patch_adjoint_halo_pack": [vp, vp, vp],
+        "exa_patch_adjoint_halo_unpack": [vp, vp, vp],
         "exa_patch_adjust_solution": [vp],
         "exa_register_pde": [i, i, i, i, vp],
         "exa_pde_available": [i, i, i, i],
@@ -173,6 +177,8 @@ def load_library(path=None):
     lib.exa_patch_stream.restype = ctypes.c_void_p
     lib.exa_patch_halo_doubles.argtypes = [vp]
     lib.exa_patch_halo_doubles.restype = ctypes.c_longlong
+    lib.exa_patch_adjoint_halo_doubles.argtypes = [vp]
+    lib.exa_patch_adjoint_halo_doubles.restype = ctypes.c_longlong
     _lib = lib
     return lib
 
@@ -613,6 +619,23 @@ class Patch:
     def adjoint_step(self, lam, dt):
         """lam (CUDA float64 tensor, luh layout): dJ/du_{k+1} in, dJ/du_k out (parameters accumulate)."""
         _check(self.lib.exa_patch_adjoint_step(self.h, _ptr(lam), float(dt)), "exa_patch_adjoint_step")
+
+    def adjoint_phase(self, phase, lam, dt):
+        """ADJ_FORWARD takes lam (this patch's cells) in; ADJ_REVERSE writes the result into it. A halo
+        patch exchanges the face traces (halo_pack / halo_unpack) and the boundary layers' lambda
+        (adjoint_halo_pack / adjoint_halo_unpack) in between."""
+        _check(self.lib.exa_patch_adjoint_phase(self.h, int(phase), _ptr(lam), float(dt)), "exa_patch_adjoint_phase")
+
+    def adjoint_halo_doubles(self):
+        return int(self.lib.exa_patch_adjoint_halo_doubles(self.h))
+
+    def adjoint_halo_pack(self, send_lo, send_hi):
+        _check(self.lib.exa_patch_adjoint_halo_pack(self.h, _ptr(send_lo), _ptr(send_hi)),
+               "exa_patch_adjoint_halo_pack")
+
+    def adjoint_halo_unpack(self, recv_lo, recv_hi):
+        _check(self.lib.exa_patch_adjoint_halo_unpack(self.h, _ptr(recv_lo), _ptr(recv_hi)),
+               "exa_patch_adjoint_halo_unpack")
 
     def close(self):
         if getattr(self, "h", None):

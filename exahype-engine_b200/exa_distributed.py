@@ -139,6 +139,32 @@ class SlabPatch:
                     p.dt_next_copy(self.dtbuf, 1)
                 p.step_phase(exa.PHASE_ADVANCE, fixed_dt)
 
+    def adjoint_step(self, lam, dt):
+        """The discrete adjoint of one fixed-dt step over all ranks: lam (CUDA float64, this rank's
+        cells, luh layout) holds dJ/du_{k+1} on entry and this rank's part of dJ/du_k on exit. The
+        transposed faces between slabs need the neighbours' face traces (the forward exchange) and
+        their boundary layers' lambda (a second exchange on the same ring)."""
+        p = self.patch
+        if self.world == 1:
+            p.adjoint_step(lam, dt)
+            return
+        if not hasattr(self, "lam_send_lo"):
+            nl = p.adjoint_halo_doubles()
+            self.lam_send_lo = torch.zeros(nl, dtype=torch.float64, device=lam.device)
+            self.lam_send_hi = torch.zeros_like(self.lam_send_lo)
+            self.lam_recv_lo = torch.zeros_like(self.lam_send_lo)
+            self.lam_recv_hi = torch.zeros_like(self.lam_send_lo)
+        with torch.cuda.stream(self.stream):
+            p.adjoint_phase(exa.ADJ_FORWARD, lam, dt)
+            p.halo_pack(self.send_lo, self.send_hi)
+            p.adjoint_halo_pack(self.lam_send_lo, self.lam_send_hi)
+            halo_exchange(self.send_lo, self.send_hi, self.recv_lo, self.recv_hi, self.rank, self.world, self.group)
+            halo_exchange(self.lam_send_lo, self.lam_send_hi, self.lam_recv_lo, self.lam_recv_hi, self.rank,
+                          self.world, self.group)
+            p.halo_unpack(self.recv_lo, self.recv_hi)
+            p.adjoint_halo_unpack(self.lam_recv_lo, self.lam_recv_hi)
+            p.adjoint_phase(exa.ADJ_REVERSE, lam, dt)
+
     def get_solution(self, out=None):
         return self.patch.get_solution(out)
 

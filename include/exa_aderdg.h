@@ -459,8 +459,8 @@ int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int 
  * No reference counterpart: the reference has no adjoint. The forward step differentiated is
  * exa_patch_step(p, 1, dt) with a fixed dt and a solver created with max_picard > 0 (the
  * reference's UseMaxPicardIterations mode: a fixed Picard sweep count, no residual test), FP64,
- * on grids whose domain faces are periodic, reflective walls or outflow (EXA_BC_USER faces and
- * halo slabs are refused with EXA_ERR_UNSUPPORTED).
+ * on grids whose domain faces are periodic, reflective walls, outflow or halo slabs (EXA_BC_USER
+ * faces are refused with EXA_ERR_UNSUPPORTED).
  *
  * exa_patch_adjoint_step: the patch's current solution is u_k at time t_k (exa_patch_set_time).
  * lambda (device, luh layout: D doubles per node) holds dJ/du_{k+1} on entry and
@@ -470,6 +470,24 @@ int exa_patch_run_host(exa_patch* p, const double* luh_in, double* luh_out, int 
  * patch stream. */
 int exa_patch_set_time(exa_patch* p, double t);
 int exa_patch_adjoint_step(exa_patch* p, double* lambda, double dt);
+
+/* The same adjoint step in two phases around two halo exchanges, for a rank's slab (EXA_BC_HALO;
+ * on other patches the two phases equal exa_patch_adjoint_step). The transposed Rusanov flux of a
+ * face between slabs needs the neighbour cell's lambda and trace as well as this rank's:
+ *   EXA_ADJ_FORWARD   the forward predictor at u_k; takes lambda (this rank's cells) in;
+ *   then exchange the face traces (exa_patch_halo_pack / _unpack, as in a forward step) and the
+ *   boundary layers' lambda (exa_patch_adjoint_halo_pack / _unpack, the same ring: recv_lo is the
+ *   lower neighbour's send_hi, recv_hi the upper neighbour's send_lo);
+ *   EXA_ADJ_REVERSE   the transposed faces and predictors; writes the result into lambda.
+ * Each rank writes only its own cells' adjoints, so the ranks' results together equal the
+ * adjoint step of the whole grid. exa_patch_adjoint_halo_doubles: doubles per buffer (cells per
+ * layer x nodes x D). The buffers are device memory. */
+#define EXA_ADJ_FORWARD 0
+#define EXA_ADJ_REVERSE 1
+int exa_patch_adjoint_phase(exa_patch* p, int phase, double* lambda, double dt);
+long long exa_patch_adjoint_halo_doubles(const exa_patch* p);
+int exa_patch_adjoint_halo_pack(exa_patch* p, double* send_lo, double* send_hi);
+int exa_patch_adjoint_halo_unpack(exa_patch* p, const double* recv_lo, const double* recv_hi);
 
 /* ---- binomial checkpointing (host only) -------------------------------------------------------
  * A schedule that reverses `steps` time steps while holding at most `snaps` stored states (the

@@ -249,3 +249,77 @@ def test_adjoint_rejects_unsupported(exa, torch):
         p2.adjoint_step(lam2, 1e-3)
     p.close()
     p2.close()
+
+
+@pytest.mark.parametrize("name,order", CASES)
+@pytest.mark.parametrize("bc_other", [0, 1], ids=["periodic", "walls"])
+def test_adjoint_of_two_slabs_matches_whole_grid(exa, torch, name, order, bc_other):
+    """The multi-GPU adjoint step emulated on one GPU: two halo patches (the lower and upper slab of
+    a grid periodic along z) with their exchange buffers swapped by hand between EXA_ADJ_FORWARD
+    and EXA_ADJ_REVERSE (face traces, then the boundary layers' lambda) give the whole-grid adjoint
+    step's lambda, parameter entries included, to 1e-12."""
+    from exa_adjoint import cfl_dt
+    pde = exa.PDE_ACOUSTIC if name == "acoustic" else exa.PDE_ELASTIC
+    V, P = exa.NVAR[pde], exa.NPAR[pde]
+    ncell, size, split = (3, 2, 5), [0.75, 0.5, 1.25], 2
+    nc, nd = int(np.prod(ncell)), (order + 1) ** 3
+    rng = np.random.default_rng(21)
+    params, cmax = _params(exa, pde, nc, rng)
+    dt = cfl_dt(ncell, size, order, cmax)
+    s = exa.Solver(pde, 3, order, npar=P, max_picard=order + 1)
+    luh = _luh(params, rng.normal(size=(nc, nd, V)), nd).reshape(-1)
+    w = rng.normal(size=nc * nd * (V + P))  # nonzero parameter entries: they accumulate
+    whole = exa.Patch(s, [dict(ncell=ncell, size=size, bc=(bc_other, bc_other, 0))])
+    whole.set_solution(luh)
+    lam_w = torch.tensor(w, device="cuda")
+    whole.adjoint_step(lam_w, dt)
+    whole.sync()
+    ref = lam_w.cpu().numpy()
+    layer = ncell[0] * ncell[1] * nd * (V + P)
+    hz = size[2] / ncell[2]
+    slabs = []
+    for first, count in ((0, split), (split, ncell[2] - split)):
+        p = exa.Patch(s, [dict(ncell=(ncell[0], ncell[1], count), size=[size[0], size[1], count * hz],
+                               offset=[0, 0, first * hz], bc=[bc_other, bc_other, exa.BC_HALO])])
+        p.set_solution(luh[first * layer:(first + count) * layer])
+        lam = torch.tensor(w[first * layer:(first + count) * layer], device="cuda")
+        nt, nl = p.halo_doubles(), p.adjoint_halo_doubles()
+        assert nl == ncell[0] * ncell[1] * nd * (V + P)
+        bufs = {k: torch.zeros(nt if k[0] == "t" else nl, dtype=torch.float64, device="cuda")
+                for k in ("tslo", "tshi", "trlo", "trhi", "lslo", "lshi", "lrlo", "lrhi")}
+        slabs.append((p, lam, bufs))
+    torch.cuda.synchronize()
+    with pytest.raises(exa.ExaError):
+        slabs[0][0].adjoint_step(slabs[0][1], dt)  # halo patches refuse the one-call step
+    with pytest.raises(exa.ExaError):
+        slabs[0][0].adjoint_phase(exa.ADJ_REVERSE, slabs[0][1], dt)  # REVERSE needs FORWARD first
+    for p, lam, b in slabs:
+        p.adjoint_phase(exa.ADJ_FORWARD, lam, dt)
+        p.halo_pack(b["tslo"], b["tshi"])
+        p.adjoint_halo_pack(b["lslo"], b["lshi"])
+    torch.cuda.synchronize()
+    (_, _, a), (_, _, b) = slabs
+    for k in ("t", "l"):  # periodic: each slab is the other's lower and upper neighbour
+        a[k + "rlo"].copy_(b[k + "shi"])
+        a[k + "rhi"].copy_(b[k + "slo"])
+        b[k + "rlo"].copy_(a[k + "shi"])
+        b[k + "rhi"].copy_(a[k + "slo"])
+    torch.cuda.synchronize()
+    for p, lam, bf in slabs:
+        p.halo_unpack(bf["trlo"], bf["trhi"])
+        p.adjoint_halo_unpack(bf["lrlo"], bf["lrhi"])
+        p.adjoint_phase(exa.ADJ_REVERSE, lam, dt)
+        p.sync()
+    got = np.concatenate([lam.cpu().numpy() for _, lam, _ in slabs])
+    assert float(np.max(np.abs(got - ref)) / np.max(np.abs(ref))) < 1e-12
+    assert np.abs(ref - w).max() > 1e-3  # the step changed lambda
+    # the phases on a patch without halo equal the one-call step
+    lam2 = torch.tensor(w, device="cuda")
+    torch.cuda.synchronize()
+    whole.adjoint_phase(exa.ADJ_FORWARD, lam2, dt)
+    whole.adjoint_phase(exa.ADJ_REVERSE, lam2, dt)
+    whole.sync()
+    assert np.array_equal(lam2.cpu().numpy(), ref)
+    for p, _, _ in slabs:
+        p.close()
+    whole.close()
