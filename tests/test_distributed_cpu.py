@@ -3,6 +3,8 @@
 * slab_partition covers the cut axis exactly once;
 * halo_exchange (the function the GPU path calls, here on CPU tensors) delivers the lower rank's
   high layer and the upper rank's low layer, for 2 and 3 ranks;
+* SlabPatch.adjoint_step (around a fake patch) runs FORWARD, both exchanges on the ring and REVERSE
+  in order;
 * one emulated time step per rank -- the C library's own face lists with ghost cells
   (exa_build_face_lists, host-only), the halo packing layout of exa_patch_halo_pack/unpack, the
   exchange and the all-reduce(min) of the time step, with the oracle doing each cell's and each
@@ -168,3 +170,73 @@ def test_slab_steps_match_single_domain(world):
     ref = _euler_cells(np.random.default_rng(1), int(np.prod(NCELL)), o.nd)
     o.run(ref, NCELL, SIZE, STEPS)
     assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-12
+
+
+class _FakeSlabPatch:
+    """Stands in for a rank's halo patch: records the adjoint step's calls and fills the send
+    buffers with rank-coded values (traces 1000 r + 1 / + 2, lambda 1000 r + 3 / + 4)."""
+
+    def __init__(self, rank):
+        self.rank, self.calls, self.got = rank, [], {}
+
+    def adjoint_halo_doubles(self):
+        return 4
+
+    def adjoint_phase(self, phase, lam, dt):
+        self.calls.append(("phase", phase))
+
+    def halo_pack(self, lo, hi):
+        self.calls.append(("pack",))
+        lo.fill_(1000.0 * self.rank + 1)
+        hi.fill_(1000.0 * self.rank + 2)
+
+    def adjoint_halo_pack(self, lo, hi):
+        self.calls.append(("lam_pack",))
+        lo.fill_(1000.0 * self.rank + 3)
+        hi.fill_(1000.0 * self.rank + 4)
+
+    def halo_unpack(self, lo, hi):
+        self.calls.append(("unpack",))
+        self.got["traces"] = (lo[0].item(), hi[0].item())
+
+    def adjoint_halo_unpack(self, lo, hi):
+        self.calls.append(("lam_unpack",))
+        self.got["lam"] = (lo[0].item(), hi[0].item())
+
+
+def _adjoint_exchange_worker(rank, world, port, q):
+    _paths()
+    import exa_aderdg as exa
+    from exa_distributed import SlabPatch
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    try:
+        sp = object.__new__(SlabPatch)  # the rank's SlabPatch around a fake patch, CPU tensors
+        sp.patch, sp.rank, sp.world, sp.group, sp.stream = _FakeSlabPatch(rank), rank, world, None, None
+        sp.send_lo, sp.send_hi, sp.recv_lo, sp.recv_hi = (torch.zeros(3, dtype=torch.float64) for _ in range(4))
+        lam = torch.zeros(8, dtype=torch.float64)
+        sp.adjoint_step(lam, 1e-3)
+        q.put((rank, sp.patch.got, sp.patch.calls, exa.ADJ_FORWARD, exa.ADJ_REVERSE))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_adjoint_step_exchanges_traces_and_lambda(world):
+    """SlabPatch.adjoint_step on gloo ranks around a fake patch: FORWARD, both packs, both
+    exchanges on the ring (the lower rank's high layer into recv_lo, the upper rank's low layer
+    into recv_hi, for the traces and for lambda), both unpacks, then REVERSE."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    pc = mp.start_processes(_adjoint_exchange_worker, args=(world, _free_port(), q), nprocs=world,
+                            start_method="spawn", join=False)
+    got = {r: (g, c, fw, rv) for r, g, c, fw, rv in (q.get(timeout=120) for _ in range(world))}
+    while not pc.join(timeout=60):
+        pass
+    for r, (g, calls, fw, rv) in got.items():
+        down, up = (r - 1) % world, (r + 1) % world
+        assert g["traces"] == (1000.0 * down + 2, 1000.0 * up + 1)
+        assert g["lam"] == (1000.0 * down + 4, 1000.0 * up + 3)
+        names = [c[0] for c in calls]
+        assert calls[0] == ("phase", fw) and calls[-1] == ("phase", rv)
+        assert set(names[1:-1]) == {"pack", "lam_pack", "unpack", "lam_unpack"}
+        assert names.index("pack") < names.index("unpack") and names.index("lam_pack") < names.index("lam_unpack")
