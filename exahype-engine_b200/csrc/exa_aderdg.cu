@@ -1642,7 +1642,12 @@ int exa_patch_adjoint_phase(exa_patch* p, int phase, double* lambda, double dt) 
   if (phase == EXA_ADJ_FORWARD) {
     if (int r = adjoint_prepare(p, dt)) return r;
     if (int r = adjoint_forward(p)) return r;
-    if (p->nghost > 0) EXA_CUDA(cudaMemcpyAsync(p->adj_lam, lambda, bytes, cudaMemcpyDeviceToDevice, p->stream));
+    if (p->nghost > 0) {
+      EXA_CUDA(cudaMemcpyAsync(p->adj_lam, lambda, bytes, cudaMemcpyDeviceToDevice, p->stream));
+      // the ghost cells' lambda is zero until exa_patch_adjoint_halo_unpack delivers the neighbours'
+      EXA_CUDA(cudaMemsetAsync(p->adj_lam + (size_t)p->ncells * o.sz_luh, 0,
+                               (size_t)p->nghost * o.sz_luh * sizeof(double), p->stream));
+    }
     p->adj_forward_done = true;
     return EXA_OK;
   }
