@@ -127,6 +127,7 @@ static exa::CellArgs base_args(exa_solver* s, int ncells) {
   a.status = s->d_status;
   a.max_picard = s->cfg.max_picard;
   a.cfl_pnpm = s->cfl * s->pnpm;
+  a.pnpm = s->pnpm;
   return a;
 }
 
@@ -267,11 +268,16 @@ int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double*
 
 static int check_faces(int nfaces) { return nfaces < 0 ? fail(EXA_ERR_INVALID, "nfaces < 0") : EXA_OK; }
 
-int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, const int* right, const signed char* dir,
-                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+}  // extern "C"
+
+// the batched face entry points; dx (3 doubles, nullable) sets the faces' cell size, which a
+// viscous flux needs
+static int riemann_call(exa_solver* s, int nfaces, const int* left, const int* right, const signed char* dir,
+                        const double* lQhbnd, double* lFhbnd, const double* dx, void* stream) {
   if (!s) return fail(EXA_ERR_INVALID, "null solver");
   if (int e = check_faces(nfaces)) return e;
   if (nfaces > 0 && (!left || !right || !dir || !lQhbnd || !lFhbnd)) return fail(EXA_ERR_INVALID, "null argument");
+  if (s->ops->viscous && !dx) return fail(EXA_ERR_INVALID, "a viscous flux needs the cell size: use the _dx entry point");
   exa::FaceArgs f;
   memset(&f, 0, sizeof(f));
   f.nfaces = nfaces;
@@ -280,15 +286,17 @@ int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, con
   f.dir = reinterpret_cast<const int8_t*>(dir);
   f.lQhbnd = lQhbnd;
   f.lFhbnd = lFhbnd;
+  for (int d = 0; d < 3; d++) f.u_dx[d] = dx && d < s->cfg.dim ? dx[d] : 1.0;
   EXA_CUDA(s->ops->riemann(f, (cudaStream_t)stream));
   return EXA_OK;
 }
 
-int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, const signed char* face,
-                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+static int boundary_call(exa_solver* s, int nfaces, const int* cell, const signed char* face, const double* lQhbnd,
+                         double* lFhbnd, const double* dx, void* stream) {
   if (!s) return fail(EXA_ERR_INVALID, "null solver");
   if (int e = check_faces(nfaces)) return e;
   if (nfaces > 0 && (!cell || !face || !lQhbnd || !lFhbnd)) return fail(EXA_ERR_INVALID, "null argument");
+  if (s->ops->viscous && !dx) return fail(EXA_ERR_INVALID, "a viscous flux needs the cell size: use the _dx entry point");
   exa::FaceArgs f;
   memset(&f, 0, sizeof(f));
   f.nfaces = nfaces;
@@ -296,8 +304,34 @@ int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, con
   f.bface = reinterpret_cast<const int8_t*>(face);
   f.lQhbnd = lQhbnd;
   f.lFhbnd = lFhbnd;
+  for (int d = 0; d < 3; d++) f.u_dx[d] = dx && d < s->cfg.dim ? dx[d] : 1.0;
   EXA_CUDA(s->ops->boundary(f, (cudaStream_t)stream));
   return EXA_OK;
+}
+
+extern "C" {
+
+int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, const int* right, const signed char* dir,
+                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+  return riemann_call(s, nfaces, left, right, dir, lQhbnd, lFhbnd, nullptr, stream);
+}
+
+int exa_riemann_solver_nonlinear_dx(exa_solver* s, int nfaces, const int* left, const int* right,
+                                    const signed char* dir, const double* lQhbnd, double* lFhbnd, const double* dx,
+                                    void* stream) {
+  if (!dx) return fail(EXA_ERR_INVALID, "null dx");
+  return riemann_call(s, nfaces, left, right, dir, lQhbnd, lFhbnd, dx, stream);
+}
+
+int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, const signed char* face,
+                                 const double* lQhbnd, double* lFhbnd, void* stream) {
+  return boundary_call(s, nfaces, cell, face, lQhbnd, lFhbnd, nullptr, stream);
+}
+
+int exa_boundary_conditions_wall_dx(exa_solver* s, int nfaces, const int* cell, const signed char* face,
+                                    const double* lQhbnd, double* lFhbnd, const double* dx, void* stream) {
+  if (!dx) return fail(EXA_ERR_INVALID, "null dx");
+  return boundary_call(s, nfaces, cell, face, lQhbnd, lFhbnd, dx, stream);
 }
 
 int exa_surface_integral_and_update(exa_solver* s, int ncells, double* luh, const double* lduh, const double* lFhbnd,
@@ -460,8 +494,8 @@ int exa_faceIntegralNonlinear(exa_solver* s, double* lduh, const double* lFhbnd,
 
 int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const double* QL, const double* QR, double t,
                                double dt, const double* dx, int direction) {
-  (void)t; (void)dt; (void)dx;
-  if (!s || !FL || !FR || !QL || !QR) return fail(EXA_ERR_INVALID, "null argument");
+  (void)t; (void)dt;
+  if (!s || !FL || !FR || !QL || !QR || !dx) return fail(EXA_ERR_INVALID, "null argument");
   if (direction < 0 || direction >= s->cfg.dim) return fail(EXA_ERR_INVALID, "direction out of range");
   std::lock_guard<std::mutex> lk(s->mu);
   const exa::Ops& o = *s->ops;
@@ -488,6 +522,7 @@ int exa_riemannSolverNonlinear(exa_solver* s, double* FL, double* FR, const doub
   f.dir = reinterpret_cast<const int8_t*>(idx + 2);
   f.lQhbnd = qhb;
   f.lFhbnd = fhb;
+  for (int d = 0; d < 3; d++) f.u_dx[d] = d < o.dim ? dx[d] : 1.0;  // a viscous flux's Rusanov speed
   EXA_CUDA(s->ops->riemann(f, 0));
   EXA_CUDA(cudaMemcpy(FL, fhb + (2 * direction + 1) * ff, ff * sizeof(double), cudaMemcpyDeviceToHost));
   EXA_CUDA(cudaMemcpy(FR, fhb + o.sz_fhb + (2 * direction) * ff, ff * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1542,7 +1577,8 @@ extern "C" int exa_stable_time_step_size_noalloc(const exa_solver_config* cfg, i
     a.cell_dt = d_cell;
     a.grid_dt_next = d_min;  // every cell counts as grid 0: per-cell minima atomic-min into d_min
     a.status = d_status;
-    a.cfl_pnpm = (cfg->cfl > 0 ? cfg->cfl : 0.9) * (cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order));
+    a.pnpm = cfg->pnpm > 0 ? cfg->pnpm : default_pnpm(cfg->order);
+    a.cfl_pnpm = (cfg->cfl > 0 ? cfg->cfl : 0.9) * a.pnpm;
     for (int d = 0; d < 3; d++) a.u_dx[d] = d < cfg->dim ? dx[d] : 1.0;
     EXA_CUDA(ops->update(a, false, false, st));
     if (cell_dt) EXA_CUDA(cudaMemcpyAsync(cell_dt, d_cell, sizeof(double) * ncells, cudaMemcpyDeviceToDevice, st));

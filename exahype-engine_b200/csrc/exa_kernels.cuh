@@ -173,6 +173,7 @@ struct CellArgs {
   unsigned* status;         // error bits (nullable)
   int max_picard;           // 0: residual test, 2(N+1) cap; > 0: fixed sweep count
   double cfl_pnpm;          // CFL * PNPM
+  double pnpm;              // PNPM alone (the viscous term of the CFL denominator)
   // point source (nullable): {x, y, z, f0, t0, amplitude, width, variable}; needs the geometry
   const double* src;
   const double* grid_geo;        // [grid][6]: lower corner xyz, cells per axis xyz
@@ -320,9 +321,12 @@ __device__ __forceinline__ void ghost_state(const double* qin, int normal, doubl
 // that side is the outside of a domain face; ghost(fn, qin, fin, qout, fout) then supplies the outer
 // state (D values) and its normal flux (V values) at face node fn from the inner ones, as the
 // reference's boundaryConditions + boundaryValues do (3d/boundaryConditions.cpph:29-122).
+// face_dx: the cells' size along the face normal; a viscous flux (useViscousFlux) adds
+// 2 (2N+1) / (face_dx sqrt(pi/2)) times the larger side's maximal viscous eigenvalue to the
+// Rusanov speed (riemannSolverNonlinear :73-87).
 template <class PDE, int DIM, int N, int P, class Ghost>
 __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR, double* FL, double* FR, int d,
-                                             int lane, bool ghostL, bool ghostR, Ghost ghost) {
+                                             int lane, bool ghostL, bool ghostR, Ghost ghost, double face_dx) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = S::n, V = S::V, D = S::D, nf = S::nf;
@@ -366,7 +370,21 @@ __device__ __forceinline__ void rusanov_face(const double* QL, const double* QR,
     sL = fmax(sL, fabs(lL[m]));
     sR = fmax(sR, fabs(lR[m]));
   }
-  const double smax = fmax(sL, sR);
+  double smax = fmax(sL, sR);
+  if constexpr (is_viscous<PDE>::value) {
+    PDE::template viscous_eigenvalues<DIM>(aL, d, lL);
+    PDE::template viscous_eigenvalues<DIM>(aR, d, lR);
+    double vL = fabs(lL[0]), vR = fabs(lR[0]);
+#pragma unroll
+    for (int m = 1; m < V; m++) {
+      vL = fmax(vL, fabs(lL[m]));
+      vR = fmax(vR, fabs(lR[m]));
+    }
+    const double factor = 2 * (2 * N + 1) / (face_dx * sqrt(0.5 * 3.14159265358979323846));
+    smax += factor * fmax(vL, vR);
+  } else {
+    (void)face_dx;
+  }
   for (int fn = lane; fn < nf; fn += 32) {
     double ql[D], qr[D], fl[V], fr[V];
 #pragma unroll
@@ -469,6 +487,39 @@ struct UserGhost {
   }
 };
 
+// CFL denominator of one node (stableTimeStepSize :36-56): sum_d max_m |lambda_d| / dx_d, where
+// a viscous flux adds max_m |viscous lambda_d| 2 / PNPM / dx_d to the maximum
+template <class PDE, int DIM>
+__device__ __forceinline__ double cfl_denominator(const double* q, const double* invDx, double pnpm) {
+  constexpr int V = PDE::V;
+  double den = 0.0;
+#pragma unroll
+  for (int d = 0; d < DIM; d++) {
+    double lam[V];
+    PDE::template eigenvalues<DIM>(q, d, lam);
+    double mx = 0.0;
+#pragma unroll
+    for (int m = 0; m < V; m++) mx = fmax(fabs(lam[m]), mx);
+    if constexpr (is_viscous<PDE>::value) {
+      PDE::template viscous_eigenvalues<DIM>(q, d, lam);
+      double mv = 0.0;
+#pragma unroll
+      for (int m = 0; m < V; m++) mv = fmax(fabs(lam[m]), mv);
+      mx += mv * (2.0 / pnpm) * invDx[d];
+    } else {
+      (void)pnpm;
+    }
+    den += mx * invDx[d];
+  }
+  return den;
+}
+
+// the size along direction d of cell c's cells (its grid's, or the uniform one)
+__device__ __forceinline__ double face_size(const FaceArgs& f, long c, int d) {
+  const int g = f.cell_grid ? f.cell_grid[c] : 0;
+  return f.grid_dx ? f.grid_dx[g * 3 + d] : f.u_dx[d];
+}
+
 template <class PDE, int DIM, int N, int P>
 __global__ void __launch_bounds__(256) riemann_kernel(FaceArgs f) {
   using S = Shape<PDE, DIM, N, P>;
@@ -481,7 +532,8 @@ __global__ void __launch_bounds__(256) riemann_kernel(FaceArgs f) {
   const double* QR = f.lQhbnd + cr * S::sizeQhb + (2 * d) * S::nf * S::D;
   double* FL = f.lFhbnd + cl * S::sizeFhb + (2 * d + 1) * S::nf * S::V;
   double* FR = f.lFhbnd + cr * S::sizeFhb + (2 * d) * S::nf * S::V;
-  rusanov_face<PDE, DIM, N, P>(QL, QR, FL, FR, d, lane, false, false, BuiltinGhost<PDE, DIM, N, P>{d, d});
+  rusanov_face<PDE, DIM, N, P>(QL, QR, FL, FR, d, lane, false, false, BuiltinGhost<PDE, DIM, N, P>{d, d},
+                               is_viscous<PDE>::value ? face_size(f, cl, d) : 1.0);
 }
 
 // Rusanov on interior faces with bulk copies: persistent warps (8 per CTA), each walking faces
@@ -543,7 +595,8 @@ __global__ void __launch_bounds__(256) riemann_bulk_kernel(FaceArgs f) {
     double* st = base + (size_t)b * R::face;
     const int d = f.dir[fc];
     rusanov_face<PDE, DIM, N, P>(st, st + R::nQ, st + 2 * R::nQ, st + 2 * R::nQ + R::nF, d, lane, false, false,
-                                 BuiltinGhost<PDE, DIM, N, P>{d, d});
+                                 BuiltinGhost<PDE, DIM, N, P>{d, d},
+                                 is_viscous<PDE>::value ? face_size(f, f.left[fc], d) : 1.0);
     fence_proxy_async_smem();
     __syncwarp();
     if (lane == 0) {
@@ -592,17 +645,18 @@ __global__ void __launch_bounds__(256) boundary_kernel(FaceArgs f) {
     gh.face = face;
     gh.d = d;
     if (o == 0)
-      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh);
+      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh, gh.dx[d]);
     else
-      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh);
+      rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh, gh.dx[d]);
     return;
   }
   // EXA_BC_OUTFLOW (3): ghost = inner state; otherwise the functor's reflective wall
   const BuiltinGhost<PDE, DIM, N, P> gh{type == 3 ? -1 : d, d};
+  const double fdx = is_viscous<PDE>::value ? face_size(f, c, d) : 1.0;
   if (o == 0)
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, true, false, gh, fdx);
   else
-    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh);
+    rusanov_face<PDE, DIM, N, P>(Q, Q, F, F, d, lane, false, true, gh, fdx);
 }
 
 // adjustPointSolution at every node (3d/solutionAdjustment.cpph:17-58): x = cell centre +
@@ -726,16 +780,7 @@ update_kernel(CellArgs a) {
   // CFL of the (new) state (stableTimeStepSize :14-62)
   double dtp = __longlong_as_double(0x7ff0000000000000ll);
   if (live && (a.grid_dt_next || a.cell_dt)) {
-    double den = 0.0;
-#pragma unroll
-    for (int d = 0; d < DIM; d++) {
-      double lam[V];
-      PDE::template eigenvalues<DIM>(q, d, lam);
-      double mx = 0.0;
-#pragma unroll
-      for (int m = 0; m < V; m++) mx = fmax(fabs(lam[m]), mx);
-      den += mx * invDx[d];
-    }
+    const double den = cfl_denominator<PDE, DIM>(q, invDx, a.pnpm);
     dtp = a.cfl_pnpm / den;
     // a non-finite state gives no time step (fmax drops NaN eigenvalues, so den alone can look fine)
     bool qok = true;
@@ -936,16 +981,7 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_bulk_kernel
     // CFL of the new state (stableTimeStepSize :14-62)
     double dtp = __longlong_as_double(0x7ff0000000000000ll);
     if (live && (a.grid_dt_next || a.cell_dt)) {
-      double den = 0.0;
-#pragma unroll
-      for (int d = 0; d < DIM; d++) {
-        double lam[V];
-        PDE::template eigenvalues<DIM>(qv, d, lam);
-        double mx = 0.0;
-#pragma unroll
-        for (int m = 0; m < V; m++) mx = fmax(fabs(lam[m]), mx);
-        den += mx * invDx[d];
-      }
+      const double den = cfl_denominator<PDE, DIM>(qv, invDx, a.pnpm);
       dtp = a.cfl_pnpm / den;
       bool qok = true;
 #pragma unroll

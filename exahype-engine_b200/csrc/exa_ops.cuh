@@ -19,11 +19,12 @@ namespace exa {
 struct Ops {
   // layout version of this interface: an application library compiled against another layout is
   // refused by exa_register_pde (its object would be read with the wrong offsets)
-  static constexpr int kAbi = 5;
+  static constexpr int kAbi = 6;
   int abi = kAbi;
   int dim, order, nvar, npar, nd, nf, cpb;
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
   bool ncp;
+  bool viscous = false;  // the flux depends on the gradient (useViscousFlux)
   virtual ~Ops() {}
   bool mixed_ok = false;  // mixed-precision predictor instantiated
   // Riemann launch form for all solvers of this instantiation: 0 riemann_kernel, otherwise
@@ -67,8 +68,10 @@ struct OpsImpl final : Ops {
   // cells whose space-time state does not fit a CTA run the streamed predictor
   static constexpr bool kStreamed = S::predictor_smem + 4096 > 227 * 1024;
   // the mixed form needs PDEs without NCP and its larger shared-memory footprint must fit a CTA
-  static constexpr bool kMixed = !kStreamed && !PDE::kNCP && MixShape<PDE, DIM, N, P>::smem_for(2) + 4096 <= 227 * 1024;
-  static constexpr bool kAdj = PDE::kAdjoint && !PDE::kNCP && AdjShape<PDE, DIM, N, P>::smem <= 227 * 1024;
+  static constexpr bool kMixed = !kStreamed && !PDE::kNCP && !is_viscous<PDE>::value &&
+                                 MixShape<PDE, DIM, N, P>::smem_for(2) + 4096 <= 227 * 1024;
+  static constexpr bool kAdj = PDE::kAdjoint && !PDE::kNCP && !is_viscous<PDE>::value &&
+                               AdjShape<PDE, DIM, N, P>::smem <= 227 * 1024;
   // streamed predictor: scratch per device, grown on demand
   std::mutex scratch_mu;
   double* scratch[64] = {};
@@ -325,6 +328,7 @@ struct OpsImpl final : Ops {
   OpsImpl() {
     adjoint_ok = kAdj;
     mixed_ok = kMixed;
+    viscous = is_viscous<PDE>::value;
     adjust_ok = has_adjust_point_solution<PDE, DIM>::value;
     user_bc_ok = has_boundary_values<PDE, DIM>::value;
     dim = DIM;

@@ -20,6 +20,12 @@
 //                                                boundaryValues for faces of type EXA_BC_USER:
 //                                                Qout (D values, pre-filled with Qin) and Fout (V,
 //                                                the normal flux of the outer state) at face node x
+//   static constexpr bool kViscous = true        the flux depends on the gradient (useViscousFlux):
+//   viscous_flux<DIM>(Q, gradQ, F)               viscousFlux, gradQ[d*V + m], replacing flux in
+//                                                the predictor
+//   viscous_eigenvalues<DIM>(Q, d, lambda)       viscousEigenvalues: the Rusanov speed adds
+//                                                2 (2N+1) / (dx_d sqrt(pi/2)) max|lambda| and the
+//                                                CFL denominator max|lambda| 2 / (PNPM dx_d)
 //
 // The bodies restate the reference applications' formulas in the same operation order so that
 // the FP64 path agrees with the reference to rounding.
@@ -42,6 +48,11 @@ struct has_boundary_values<PDE, DIM,
                            std::void_t<decltype(PDE::template boundary_values<DIM>(
                                (const double*)nullptr, 0.0, 0.0, 0, 0, (const double*)nullptr, (const double*)nullptr,
                                (double*)nullptr, (double*)nullptr))>> : std::true_type {};
+
+template <class PDE, class = void>
+struct is_viscous : std::false_type {};
+template <class PDE>
+struct is_viscous<PDE, std::void_t<decltype(PDE::kViscous)>> : std::integral_constant<bool, PDE::kViscous> {};
 
 // correctly rounded reciprocal: the same value as 1 / x (IEEE round to nearest), fewer instructions
 __device__ __forceinline__ double recip(double x) { return __drcp_rn(x); }

@@ -18,14 +18,16 @@
 //            distributed over the time nodes).
 // The new iterate lives in registers (n*V doubles per thread); the old iterate stays in the
 // shared slices [t][node][D] for the whole sweep (phase 1 and the residual read only the
-// thread's own node; the NCP gradients read neighbours) and is overwritten by the new one once
-// the per-cell residual has decided that another sweep follows.
+// thread's own node; the gradients of an NCP or of a viscous flux read neighbours) and is
+// overwritten by the new one once the per-cell residual has decided that another sweep follows.
+// A viscous flux (useViscousFlux) is evaluated from the node's state and the gradient of the old
+// iterate at the same time node (:99-212).
 //
 // Sweep 0 starts from lQi[., t] = luh (:71-82), which is constant in time, so its flux and
 // contractions are computed once and its time solve has a closed form (an exact identity, not
-// an approximation). For PDEs without NCP the time-averaged flux lFhi is accumulated in
-// registers from the final old iterate after the loop instead of being carried through every
-// sweep.
+// an approximation). For PDEs with neither an NCP nor a viscous flux the time-averaged flux lFhi
+// is accumulated in registers from the final old iterate after the loop instead of being carried
+// through every sweep.
 #pragma once
 
 namespace exa {
@@ -54,6 +56,8 @@ predictor_kernel(CellArgs a) {
   constexpr int DQ = S::DQ;  // per-node stride of the iterate slices and the luh block (odd)
   constexpr int FCS = S::FCS;  // stride between the cells' flux blocks
   constexpr bool NCP = PDE::kNCP;
+  constexpr bool VISC = is_viscous<PDE>::value;  // viscousFlux(Q, gradQ) replaces flux(Q)
+  constexpr bool GRAD = NCP || VISC;               // the sweeps need the iterate's gradient
   static_assert(CPB <= 32, "the per-CTA cell mask holds 32 cells");
   extern __shared__ __align__(128) double smem[];
   double* sQ = smem;              // [CPB][n][nd][DQ]: old iterate slices, lQhi in the tail
@@ -213,20 +217,20 @@ predictor_kernel(CellArgs a) {
     // new iterate of the sweep, accumulated in registers time node by time node (the iK1 time
     // solve distributed over phase 3); the old iterate is staged in the slices q_s [t][node][D]
     double qn[n][V];
-    if (NCP && inr) {  // neighbours' old iterate is read by the gradients
+    if (GRAD && inr) {  // neighbours' old iterate is read by the gradients
 #pragma unroll
       for (int t = 0; t < n; t++)
 #pragma unroll
         for (int m = 0; m < D; m++) q_s[(t * nd + p) * DQ + m] = u[m];
     }
-    double fh[NCP ? DIM : 1][V];   // time-averaged flux / source of the sweep (NCP path only)
+    double fh[GRAD ? DIM : 1][V];  // time-averaged flux / source of the sweep (gradient path only)
     double sh[V];
     (void)fh;
     (void)sh;
-    // s_lw and the NCP slices are visible
+    // s_lw and the gradient path's slices are visible
     __syncthreads();
 
-    // gradient of the old iterate at time node ti and this node (:111-175), NCP only
+    // gradient of the old iterate at time node ti and this node (:111-175), NCP or viscous flux only
     auto gradient = [&](int ti, double* gq) {
       const double invDx[3] = {s_invdx[lc][0], s_invdx[lc][1], s_invdx[lc][2]};
 #pragma unroll
@@ -303,9 +307,9 @@ predictor_kernel(CellArgs a) {
     bool last_old_is_luh = true;  // the last sweep started from lQi = luh (sweep 0)
     for (int s = 0; s < maxIter; s++) {
       const bool work = live && ((active >> lc) & 1u);
-      if (NCP && work) {
+      if (GRAD && work) {
 #pragma unroll
-        for (int d = 0; d < (NCP ? DIM : 1); d++)
+        for (int d = 0; d < (GRAD ? DIM : 1); d++)
 #pragma unroll
           for (int m = 0; m < V; m++) fh[d][m] = 0.0;
 #pragma unroll
@@ -316,27 +320,33 @@ predictor_kernel(CellArgs a) {
         // the iterate is luh at every time node: one flux, one set of contractions
         double F[DIM * V];
         double S0[V];
-        PDE::template flux<DIM>(u, F);
+        double gq0[GRAD ? DIM * V : 1];
+        if constexpr (GRAD) gradient(0, gq0);
+        if constexpr (VISC)
+          PDE::template viscous_flux<DIM>(u, gq0, F);
+        else
+          PDE::template flux<DIM>(u, F);
         store_flux(F);
-        if (NCP) {
-          double gq[DIM * V], B[V];
-          gradient(0, gq);
-          PDE::template ncp<DIM>(u, gq, B);
+        if constexpr (NCP) {
+          double B[V];
+          PDE::template ncp<DIM>(u, gq0, B);
 #pragma unroll
           for (int m = 0; m < V; m++) S0[m] = -B[m];
-          if (work) {
-            for (int i = 0; i < n; i++) {
-              const double wi = G::weights(i);
+        }
+        if (GRAD && work) {
+          for (int i = 0; i < n; i++) {
+            const double wi = G::weights(i);
 #pragma unroll
-              for (int d = 0; d < (NCP ? DIM : 1); d++)
+            for (int d = 0; d < (GRAD ? DIM : 1); d++)
 #pragma unroll
-                for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+            if (NCP) {
 #pragma unroll
               for (int m = 0; m < V; m++) sh[m] = fma(S0[m], wi, sh[m]);
             }
           }
         }
-        if (NCP && a.ex_lFi && work)
+        if (GRAD && a.ex_lFi && work)
           for (int i = 0; i < n; i++) export_flux(i, F, S0);
         __syncthreads();
         contract(1.0);
@@ -392,25 +402,31 @@ predictor_kernel(CellArgs a) {
           for (int m = 0; m < D; m++) q[m] = m < V ? q_s[(i * nd + p) * DQ + m] : u[m];
           double F[DIM * V];
           double Si[V];
-          PDE::template flux<DIM>(q, F);
+          double gqi[GRAD ? DIM * V : 1];
+          if constexpr (GRAD) gradient(i, gqi);
+          if constexpr (VISC)
+            PDE::template viscous_flux<DIM>(q, gqi, F);
+          else
+            PDE::template flux<DIM>(q, F);
           store_flux(F);
           const double wi = G::weights(i);
-          if (NCP) {
-            double gq[DIM * V], B[V];
-            gradient(i, gq);
-            PDE::template ncp<DIM>(q, gq, B);
+          if constexpr (NCP) {
+            double B[V];
+            PDE::template ncp<DIM>(q, gqi, B);
 #pragma unroll
             for (int m = 0; m < V; m++) Si[m] = -B[m];
-            if (work) {
+          }
+          if (GRAD && work) {
 #pragma unroll
-              for (int d = 0; d < (NCP ? DIM : 1); d++)
+            for (int d = 0; d < (GRAD ? DIM : 1); d++)
 #pragma unroll
-                for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+            if (NCP) {
 #pragma unroll
               for (int m = 0; m < V; m++) sh[m] = fma(Si[m], wi, sh[m]);
             }
-            if (a.ex_lFi && work) export_flux(i, F, Si);
           }
+          if (GRAD && a.ex_lFi && work) export_flux(i, F, Si);
           __syncthreads();
           // phase 2
           contract(wi);
@@ -495,7 +511,7 @@ predictor_kernel(CellArgs a) {
       if (tid < CPB) s_res[(s + 1) & 1][tid] = 0.0;
       active &= ~conv;
       // the gradients of the next sweep read the neighbours' copied iterate
-      if (NCP) __syncthreads();
+      if (GRAD) __syncthreads();
       if (!active) break;
     }
     if (live && a.picard && p == 0) a.picard[cell] = sweeps;
@@ -521,12 +537,12 @@ predictor_kernel(CellArgs a) {
     }
     // the old iterate of the last sweep, before its slot 0 takes lQhi (each thread reads and
     // writes only its own node, so no barrier is needed in between)
-    double fa[NCP ? 1 : DIM * V];
+    double fa[GRAD ? 1 : DIM * V];
     (void)fa;
-    if (!NCP && inr) {
+    if (!GRAD && inr) {
       // lFhi = sum_t w_t F(old iterate at t), accumulated in registers
 #pragma unroll
-      for (int k = 0; k < (NCP ? 1 : DIM * V); k++) fa[k] = 0.0;
+      for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = 0.0;
       if (last_old_is_luh) {
         // the old iterate is luh at every time node: one flux, the same weighted sum
         double F[DIM * V];
@@ -535,7 +551,7 @@ predictor_kernel(CellArgs a) {
         for (int i = 0; i < n; i++) {
           const double wi = G::weights(i);
 #pragma unroll
-          for (int k = 0; k < (NCP ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
+          for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
           if (live && a.ex_lFi) export_flux(i, F, nullptr);
         }
       } else {
@@ -547,7 +563,7 @@ predictor_kernel(CellArgs a) {
           PDE::template flux<DIM>(q, F);
           const double wi = G::weights(i);
 #pragma unroll
-          for (int k = 0; k < (NCP ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
+          for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
           if (live && a.ex_lFi) export_flux(i, F, nullptr);
         }
       }
@@ -559,18 +575,20 @@ predictor_kernel(CellArgs a) {
     if (inr) {
 #pragma unroll
       for (int m = 0; m < D; m++) qh_s[p * DQ + m] = qh[m];
-      if (NCP) {
+      if (GRAD) {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[NCP ? d : 0][m];
+          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[GRAD ? d : 0][m];
+        if (NCP) {
 #pragma unroll
-        for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
+          for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
+        }
       } else {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(NCP ? 0 : d * V + m)];
+          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(GRAD ? 0 : d * V + m)];
       }
     }
     if (live && a.ex_lQhi) {

@@ -108,6 +108,8 @@ def load_library(path=None):
         "exa_fused_predictor_volume_integral": [vp, i, vp, vp, vp, vp, vp, dp, d, d, vp],
         "exa_riemann_solver_nonlinear": [vp, i, vp, vp, vp, vp, vp, vp],
         "exa_boundary_conditions_wall": [vp, i, vp, vp, vp, vp, vp],
+        "exa_riemann_solver_nonlinear_dx": [vp, i, vp, vp, vp, vp, vp, vp, vp],
+        "exa_boundary_conditions_wall_dx": [vp, i, vp, vp, vp, vp, vp, vp],
         "exa_surface_integral_and_update": [vp, i, vp, vp, vp, dp, d, vp],
         "exa_solution_update": [vp, i, vp, vp, vp, d, vp],
         "exa_stable_time_step_size": [vp, i, vp, dp, vp, dp, vp],
@@ -288,14 +290,26 @@ class Solver:
             self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(picard), _dx3(dx, self.dim),
             float(t), float(dt), _stream(stream)), "exa_fused_predictor_volume_integral")
 
-    def riemann(self, left, right, direction, lQhbnd, lFhbnd, stream=None):
-        _check(self.lib.exa_riemann_solver_nonlinear(self.h, left.numel(), _ptr(left), _ptr(right), _ptr(direction),
-                                                     _ptr(lQhbnd), _ptr(lFhbnd), _stream(stream)),
-               "exa_riemann_solver_nonlinear")
+    def riemann(self, left, right, direction, lQhbnd, lFhbnd, stream=None, dx=None):
+        """dx (the cells' size) is needed by PDEs with a viscous flux."""
+        if dx is None:
+            _check(self.lib.exa_riemann_solver_nonlinear(self.h, left.numel(), _ptr(left), _ptr(right),
+                                                         _ptr(direction), _ptr(lQhbnd), _ptr(lFhbnd),
+                                                         _stream(stream)), "exa_riemann_solver_nonlinear")
+        else:
+            _check(self.lib.exa_riemann_solver_nonlinear_dx(self.h, left.numel(), _ptr(left), _ptr(right),
+                                                            _ptr(direction), _ptr(lQhbnd), _ptr(lFhbnd),
+                                                            _dx3(dx, self.dim), _stream(stream)),
+                   "exa_riemann_solver_nonlinear_dx")
 
-    def boundary_wall(self, cell, face, lQhbnd, lFhbnd, stream=None):
-        _check(self.lib.exa_boundary_conditions_wall(self.h, cell.numel(), _ptr(cell), _ptr(face), _ptr(lQhbnd),
-                                                     _ptr(lFhbnd), _stream(stream)), "exa_boundary_conditions_wall")
+    def boundary_wall(self, cell, face, lQhbnd, lFhbnd, stream=None, dx=None):
+        if dx is None:
+            _check(self.lib.exa_boundary_conditions_wall(self.h, cell.numel(), _ptr(cell), _ptr(face), _ptr(lQhbnd),
+                                                         _ptr(lFhbnd), _stream(stream)), "exa_boundary_conditions_wall")
+        else:
+            _check(self.lib.exa_boundary_conditions_wall_dx(self.h, cell.numel(), _ptr(cell), _ptr(face),
+                                                            _ptr(lQhbnd), _ptr(lFhbnd), _dx3(dx, self.dim),
+                                                            _stream(stream)), "exa_boundary_conditions_wall_dx")
 
     def surface_integral_and_update(self, luh, lduh, lFhbnd, dx, dt, stream=None):
         ncells = luh.numel() // self.sizes["luh"]

@@ -160,12 +160,20 @@ int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double*
  * reference (ADERDGSolver.cpp:1781-1785). left/right/dir are device arrays. */
 int exa_riemann_solver_nonlinear(exa_solver* s, int nfaces, const int* left, const int* right,
                                  const signed char* dir, const double* lQhbnd, double* lFhbnd, void* stream);
+/* The same with the cells' size dx (DIM doubles, host), which riemannSolverNonlinear<useNCP,true>
+ * needs for the viscous term of the Rusanov speed (:73-87); PDEs with a viscous flux refuse the
+ * call without dx. */
+int exa_riemann_solver_nonlinear_dx(exa_solver* s, int nfaces, const int* left, const int* right,
+                                    const signed char* dir, const double* lQhbnd, double* lFhbnd, const double* dx,
+                                    void* stream);
 
 /* Replaces boundaryConditions (3d/boundaryConditions.cpph:29-122) + the Riemann call of the
  * glue's boundaryConditions (...Implementation.template:307-350) with a reflective wall
  * (the SWE app's boundaryValues, MySWESolver.cpp:43-62) on faces face[f] of cells cell[f]. */
 int exa_boundary_conditions_wall(exa_solver* s, int nfaces, const int* cell, const signed char* face,
                                  const double* lQhbnd, double* lFhbnd, void* stream);
+int exa_boundary_conditions_wall_dx(exa_solver* s, int nfaces, const int* cell, const signed char* face,
+                                    const double* lQhbnd, double* lFhbnd, const double* dx, void* stream);
 
 /* Replaces surfaceIntegralNonlinear (3d/surfaceIntegralNonlinear.cpph:21-90) followed by
  * solutionUpdate (3d/solutionUpdate.cpph:28-67): luh += dt/w * (lduh - surface terms). lduh is

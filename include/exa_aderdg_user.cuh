@@ -23,6 +23,11 @@
  *                                                                     double dt, double* Q);
  *     template <int DIM> static __device__ void boundary_values(const double* x, double t, double dt,
  *         int faceIndex, int normal, const double* Fin, const double* Qin, double* Fout, double* Qout);
+ *     // a flux that depends on the gradient (the reference's useViscousFlux, viscousFlux and
+ *     // viscousEigenvalues): gradQ[d * V + m]
+ *     static constexpr bool kViscous = true;
+ *     template <int DIM> static __device__ void viscous_flux(const double* Q, const double* gradQ, double* F);
+ *     template <int DIM> static __device__ void viscous_eigenvalues(const double* Q, int d, double* lambda);
  *   };
  *   EXA_REGISTER_PDE(EXA_PDE_USER_BASE, MyEuler, 3, 5, 0)  // id, functor, DIM, Order, NumberOfParameters
  *
@@ -39,6 +44,14 @@
  * scratch. That predictor takes systems without an NCP, and one time node's fluxes
  * (DIM * V * n^DIM doubles) must still fit the CTA. A static_assert names an instantiation that
  * fits neither form.
+ *
+ * With kViscous the predictor evaluates viscous_flux at every node and time node with the gradient
+ * of the Picard iterate there; the Rusanov speed and the CFL step add the viscous eigenvalues' terms
+ * of the reference. flux is still required: the built-in wall and outflow faces take the inviscid
+ * flux of their ghost state. Systems with a viscous flux have no mixed-precision form, no
+ * streamed predictor and no adjoint. The batched face entry points need the cell size for them
+ * (exa_riemann_solver_nonlinear_dx). The time-averaged gradient's face values (lGradQhbnd, which the
+ * reference passes to boundaryValues) are not produced.
  *
  * Build with the same flags as the library (exahype-engine_b200/build.py: build_user_pde does it),
  * linking libexa_aderdg.so. Loading the application's library registers its instantiations; from

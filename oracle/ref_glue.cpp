@@ -194,6 +194,37 @@ struct ElasticPDE {
   }
 };
 
+// Advection-diffusion of three scalars with their own velocities and diffusivities: the test
+// system of the viscous-flux path (useViscousFlux). viscousFlux F_d[m] = a_m,d Q[m] - nu_m dQ[m]/dx_d
+// (gradQ[d][m] as the predictor passes it, 3d/spaceTimePredictorNonlinear.cpph:206-208);
+// viscousEigenvalues nu_m. The GPU functor of the tests defines the same system.
+struct AdvDiffPDE {
+  static constexpr int NumberOfVariables = 3;
+  static constexpr bool HasSource = false;
+  static constexpr double a[3][3] = {{0.3, -0.2, 0.1}, {-0.5, 0.25, 0.4}, {0.0, 0.6, -0.3}};
+  static constexpr double nu[3] = {0.01, 0.005, 0.02};
+  static void flux(const double* const Q, double** const F) {
+    for (int d = 0; d < DIMENSIONS; d++)
+      for (int m = 0; m < 3; m++) F[d][m] = a[m][d] * Q[m];
+  }
+  static void viscousFlux(const double* const Q, const double* const gradQ, double** const F) {
+    for (int d = 0; d < DIMENSIONS; d++)
+      for (int m = 0; m < 3; m++) F[d][m] = a[m][d] * Q[m] - nu[m] * gradQ[d * 3 + m];
+  }
+  static void eigenvalues(const double* const, const int d, double* const lambda) {
+    for (int m = 0; m < 3; m++) lambda[m] = a[m][d];
+  }
+  static void viscousEigenvalues(const double* const, const int, double* const lambda) {
+    for (int m = 0; m < 3; m++) lambda[m] = nu[m];
+  }
+  static void nonConservativeProduct(const double* const, const double* const, double* const B) {
+    std::fill_n(B, 3, 0.0);
+  }
+  static void wall(const double* QIn, int, double* QOut) { std::copy_n(QIn, 3, QOut); }
+};
+constexpr double AdvDiffPDE::a[3][3];
+constexpr double AdvDiffPDE::nu[3];
+
 // Point source of the acoustic / elastic solvers (x, y, z, f0, t0, amplitude, width, variable):
 // a unit-mass Gaussian of the given width times a Ricker wavelet, acting only on cells whose
 // centre is within 6 widths plus a cell diagonal (the per-cell truncation the GPU path and the
@@ -284,6 +315,16 @@ template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::dudx =
 template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::iK1 = kernels::legendre::iK1;
 template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::FCoeff = kernels::legendre::FCoeff;
 
+// The solver of a PDE with a viscous flux: the kernels call these members when instantiated with
+// useViscousFlux = true (they hide the base's empty ones).
+template <class PDE, int ORDER>
+struct RefViscSolver : RefSolver<PDE, ORDER, 0> {
+  void viscousFlux(const double* const Q, const double* const gradQ, double** const F) {
+    PDE::viscousFlux(Q, gradQ, F);
+  }
+  void viscousEigenvalues(const double* const Q, const int d, double* const l) { PDE::viscousEigenvalues(Q, d, l); }
+};
+
 template <class S>
 struct Sizes {
   static constexpr int n = S::Order + 1;
@@ -310,14 +351,17 @@ inline tarch::la::Vector<DIMENSIONS, double> vec(const double* x) {
 
 // One whole cell predictor exactly as the generated glue does it
 // (AbstractGenericADERDGSolverImplementation.template:168-211).
-template <class S, bool useNCP, bool useSource>
+// VISC: useViscousFlux (the extrapolator then also writes the time-averaged gradient's face values).
+template <class S, bool useNCP, bool useSource, bool VISC = false>
 int predictor(S& s, const double* luh, const double* centre, const double* dx, double t, double dt,
               double* lQi, double* rhs, double* lFi, double* gradQ, double* lQhi, double* lFhi,
               double* lQhbnd, double* lFhbnd) {
   auto invDx = tarch::la::invertEntries(vec(dx));
   tl_src_on = useSource && source_near(centre, dx);
-  return kernels::aderdg::generic::c::spaceTimePredictorNonlinear<useSource, true, false, useNCP, false, S>(
-      s, lQhbnd, nullptr, lFhbnd, lQi, rhs, lFi, gradQ, lQhi, lFhi, luh, vec(centre), invDx, t, dt);
+  std::vector<double> lGradQhbnd(VISC ? 2 * DIMENSIONS * Sizes<S>::nf * Sizes<S>::v * DIMENSIONS : 1);
+  return kernels::aderdg::generic::c::spaceTimePredictorNonlinear<useSource, true, VISC, useNCP, false, S>(
+      s, lQhbnd, VISC ? lGradQhbnd.data() : nullptr, lFhbnd, lQi, rhs, lFi, gradQ, lQhi, lFhi, luh, vec(centre),
+      invDx, t, dt);
 }
 
 // Uniform patch driver in the global non-fused order: dt = min_cells stableTimeStepSize(luh)
@@ -326,7 +370,7 @@ int predictor(S& s, const double* luh, const double* centre, const double* dx, d
 // through boundaryConditions: 1 reflective walls, 3 outflow, 3d/boundaryConditions.cpph:29-122 and glue
 // :307-350). Cell c = (iz*ny + iy)*nx + ix. The reference's TBB/Peano scheduler is absent from
 // the checkout; an OpenMP loop over cells and faces stands in for it.
-template <class S, bool useNCP, bool useSource>
+template <class S, bool useNCP, bool useSource, bool VISC = false>
 int run_patch(const int* ncell, const double* offset, const double* size, int walls, double* luh_all,
               int nsteps, double t0, double fixed_dt, double* t_out, double* dts, int* picard,
               int nthreads) {
@@ -349,7 +393,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
 #pragma omp parallel for reduction(min : dt) schedule(static)
       for (long c = 0; c < nc; c++) {
         S s;
-        dt = std::min(dt, kernels::aderdg::generic::c::stableTimeStepSize<S, false>(
+        dt = std::min(dt, kernels::aderdg::generic::c::stableTimeStepSize<S, VISC>(
                               s, luh_all + c * Z::luh, vec(dx)));
       }
     }
@@ -364,7 +408,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
         const int ix = c % nx, iy = (c / nx) % ny, iz = (int)(c / ((long)nx * ny));
         double centre[3] = {offset[0] + (ix + 0.5) * dx[0], offset[1] + (iy + 0.5) * dx[1],
                             DIMENSIONS == 3 ? offset[2] + (iz + 0.5) * dx[2] : 0.0};
-        int it = predictor<S, useNCP, useSource>(s, luh_all + c * Z::luh, centre, dx, t, dt, lQi.data(),
+        int it = predictor<S, useNCP, useSource, VISC>(s, luh_all + c * Z::luh, centre, dx, t, dt, lQi.data(),
                                       rhs.data(), lFi.data(), gradQ.data(), lQhi.data(), lFhi.data(),
                                       lQhbnd.data() + c * Z::lQhbnd, lFhbnd.data() + c * Z::lFhbnd);
         iters += it;
@@ -393,7 +437,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
                                 DIMENSIONS == 3 ? offset[2] + (iz + 0.5) * dx[2] : 0.0};
             kernels::aderdg::generic::c::boundaryConditions<false, S>(
                 s, FOut.data(), QOut.data(), FL, QL, nullptr, vec(centre), vec(dx), t, dt, 2 * d + 1, d);
-            kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, false, S>(
+            kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, VISC, S>(
                 s, FL, FOut.data(), QL, QOut.data(), t, dt, vec(dx), d);
           } else {
             j = 0;
@@ -403,7 +447,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
           long c2 = cellIndex(jx, jy, jz);
           double* FR = lFhbnd.data() + c2 * Z::lFhbnd + (2 * d) * Z::nf * Z::v;
           const double* QR = lQhbnd.data() + c2 * Z::lQhbnd + (2 * d) * Z::nf * Z::D;
-          kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, false, S>(s, FL, FR, QL, QR, t, dt,
+          kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, VISC, S>(s, FL, FR, QL, QR, t, dt,
                                                                                vec(dx), d);
         }
         // left domain boundary of this cell
@@ -416,7 +460,7 @@ int run_patch(const int* ncell, const double* offset, const double* size, int wa
                               DIMENSIONS == 3 ? offset[2] + (iz + 0.5) * dx[2] : 0.0};
           kernels::aderdg::generic::c::boundaryConditions<false, S>(
               s, FOut.data(), QOut.data(), FRb, QRb, nullptr, vec(centre), vec(dx), t, dt, 2 * d, d);
-          kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, false, S>(
+          kernels::aderdg::generic::c::riemannSolverNonlinear<useNCP, VISC, S>(
               s, FOut.data(), FRb, QOut.data(), QRb, t, dt, vec(dx), d);
         }
       }
@@ -728,57 +772,60 @@ extern "C" void exalin_eigenvalues(int elastic, const double* Q, double* l) {
 
 #define EXAREF_S(PDE, O, P, X) exaref::RefSolver<exaref::PDE, O, P, X>
 #define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false, false)
-#define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC, FIXED)                                               \
+#define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC, FIXED) \
+  EXAREF_DEFINE_G(NAME, EXAREF_S(PDE, O, P, FIXED), exaref::PDE::NumberOfVariables, O, NCP, SRC, false)
+// a PDE with a viscous flux (useViscousFlux = true), no parameters
+#define EXAREF_DEFINE_V(NAME, PDE, O) \
+  EXAREF_DEFINE_G(NAME, exaref::RefViscSolver<exaref::PDE COMMA O>, exaref::PDE::NumberOfVariables, O, false, false, true)
+#define COMMA ,
+// ST: the SolverType; NV: its NumberOfVariables
+#define EXAREF_DEFINE_G(NAME, ST, NV, O, NCP, SRC, VISC)                                                    \
   extern "C" int NAME##_predictor(const double* luh, const double* centre, const double* dx, double t,     \
                                   double dt, double* lQi, double* rhs, double* lFi, double* gradQ,          \
                                   double* lQhi, double* lFhi, double* lQhbnd, double* lFhbnd) {             \
-    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
-    return exaref::predictor<EXAREF_S(PDE, O, P, FIXED), NCP, SRC>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ,     \
-                                                       lQhi, lFhi, lQhbnd, lFhbnd);                         \
+    ST s;                                                                                                   \
+    return exaref::predictor<ST, NCP, SRC, VISC>(s, luh, centre, dx, t, dt, lQi, rhs, lFi, gradQ, lQhi,    \
+                                                 lFhi, lQhbnd, lFhbnd);                                     \
   }                                                                                                         \
   extern "C" void NAME##_volume(double* lduh, const double* lFhi, const double* dx) {                        \
-    kernels::aderdg::generic::c::volumeIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED), NCP || SRC, true, false,      \
-                                                         exaref::PDE::NumberOfVariables, O + 1>(            \
+    kernels::aderdg::generic::c::volumeIntegralNonlinear<ST, NCP || SRC, true, false, NV, O + 1>(           \
         lduh, lFhi, exaref::vec(dx));                                                                       \
   }                                                                                                         \
   extern "C" void NAME##_riemann(double* FL, double* FR, const double* QL, const double* QR, double t,      \
                                  double dt, const double* dx, int direction) {                              \
-    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
-    kernels::aderdg::generic::c::riemannSolverNonlinear<NCP, false, EXAREF_S(PDE, O, P, FIXED)>(                   \
-        s, FL, FR, QL, QR, t, dt, exaref::vec(dx), direction);                                              \
+    ST s;                                                                                                   \
+    kernels::aderdg::generic::c::riemannSolverNonlinear<NCP, VISC, ST>(s, FL, FR, QL, QR, t, dt,           \
+                                                                       exaref::vec(dx), direction);         \
   }                                                                                                         \
   extern "C" void NAME##_surface(double* lduh, const double* lFhbnd, const double* dx) {                    \
-    kernels::aderdg::generic::c::surfaceIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED),                              \
-                                                          exaref::PDE::NumberOfVariables, O + 1>(           \
-        lduh, lFhbnd, exaref::vec(dx));                                                                     \
+    kernels::aderdg::generic::c::surfaceIntegralNonlinear<ST, NV, O + 1>(lduh, lFhbnd, exaref::vec(dx));   \
   }                                                                                                         \
   extern "C" void NAME##_face(double* lduh, const double* lFhbnd, int direction, int orientation,           \
                               const double* dx) {                                                           \
-    kernels::aderdg::generic::c::faceIntegralNonlinear<EXAREF_S(PDE, O, P, FIXED), exaref::PDE::NumberOfVariables, \
-                                                       O + 1>(lduh, lFhbnd, direction, orientation,         \
-                                                              exaref::vec(dx));                             \
+    kernels::aderdg::generic::c::faceIntegralNonlinear<ST, NV, O + 1>(lduh, lFhbnd, direction, orientation, \
+                                                                      exaref::vec(dx));                     \
   }                                                                                                         \
   extern "C" void NAME##_update(double* luh, const double* luhOld, const double* lduh, double dt) {        \
-    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
-    kernels::aderdg::generic::c::solutionUpdate<EXAREF_S(PDE, O, P, FIXED)>(s, luh, luhOld, lduh, dt);             \
+    ST s;                                                                                                   \
+    kernels::aderdg::generic::c::solutionUpdate<ST>(s, luh, luhOld, lduh, dt);                              \
   }                                                                                                         \
   extern "C" double NAME##_dt(const double* luh, const double* dx) {                                        \
-    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
-    return kernels::aderdg::generic::c::stableTimeStepSize<EXAREF_S(PDE, O, P, FIXED), false>(s, luh,              \
-                                                                                       exaref::vec(dx));    \
+    ST s;                                                                                                   \
+    return kernels::aderdg::generic::c::stableTimeStepSize<ST, VISC>(s, luh, exaref::vec(dx));            \
   }                                                                                                         \
   extern "C" void NAME##_boundary(double* FOut, double* QOut, const double* FIn, const double* QIn,        \
                                   const double* centre, const double* dx, double t, double dt,              \
                                   int faceIndex, int normal) {                                              \
-    EXAREF_S(PDE, O, P, FIXED) s;                                                                                  \
-    kernels::aderdg::generic::c::boundaryConditions<false, EXAREF_S(PDE, O, P, FIXED)>(                            \
-        s, FOut, QOut, FIn, QIn, nullptr, exaref::vec(centre), exaref::vec(dx), t, dt, faceIndex, normal);  \
+    ST s;                                                                                                   \
+    kernels::aderdg::generic::c::boundaryConditions<false, ST>(s, FOut, QOut, FIn, QIn, nullptr,            \
+                                                               exaref::vec(centre), exaref::vec(dx), t, dt, \
+                                                               faceIndex, normal);                          \
   }                                                                                                         \
   extern "C" int NAME##_run(const int* ncell, const double* offset, const double* size, int walls,         \
                             double* luh, int nsteps, double t0, double fixed_dt, double* t_out,             \
                             double* dts, int* picard, int nthreads) {                                       \
-    return exaref::run_patch<EXAREF_S(PDE, O, P, FIXED), NCP, SRC>(ncell, offset, size, walls, luh, nsteps, t0,         \
-                                                       fixed_dt, t_out, dts, picard, nthreads);             \
+    return exaref::run_patch<ST, NCP, SRC, VISC>(ncell, offset, size, walls, luh, nsteps, t0, fixed_dt,    \
+                                                 t_out, dts, picard, nthreads);                             \
   }
 
 extern "C" void exaref_set_source(const double* src, int active) {
@@ -797,10 +844,12 @@ EXAREF_DEFINE(exaref3d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref3d_euler_o5_p0, EulerPDE, 5, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o2_p0, EulerPDE, 2, 0, false)
+EXAREF_DEFINE_V(exaref3d_advdiff_o3_p0, AdvDiffPDE, 3)
 #else
 EXAREF_DEFINE(exaref2d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref2d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref2d_euler_o5_p0, EulerPDE, 5, 0, false)
 EXAREF_DEFINE(exaref2d_swe_o4_p0, SWEPDE, 4, 0, true)
 EXAREF_DEFINE(exaref2d_swe_o2_p0, SWEPDE, 2, 0, true)
+EXAREF_DEFINE_V(exaref2d_advdiff_o3_p0, AdvDiffPDE, 3)
 #endif

@@ -100,3 +100,78 @@ def test_builtin_functor_without_hooks_refuses_them():
     p = exa.Patch(s, [dict(ncell=(2, 2, 2), size=[1.0] * 3)])
     with pytest.raises(exa.ExaError):
         p.adjust_solution()
+
+
+ADV_LIB = os.path.join(REPO, "tests", "user_pde", "libuser_advdiff.so")
+
+
+def _advdiff_state(rng, ncell, order, size):
+    """Three smooth periodic fields plus a little noise on the nodes."""
+    import exa_scenarios as sc
+    dim = len(ncell)
+    x = sc.nodal_positions(ncell, size, order)
+    f = np.zeros(x.shape[:-1] + (3,))
+    for m in range(3):
+        k = rng.integers(1, 3, dim)
+        f[..., m] = 1.0 + 0.5 * np.sin(2 * np.pi * (x * (k / np.array(size))).sum(-1) + rng.uniform(0, 6.3))
+    return (f + 0.01 * rng.normal(size=f.shape)).reshape(-1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,ncell", [(3, (4, 3, 5)), (2, (9, 7))])
+def test_viscous_flux_pde_vs_reference_kernels(dim, ncell):
+    """A PDE with a viscous flux (useViscousFlux) through the application-functor route
+    (tests/user_pde/user_advdiff.cu) against the reference's own generic kernels instantiated with
+    useViscousFlux = true for the same system: three periodic steps to 1e-12 with equal time steps;
+    the per-cell predictor (its return value included), the Rusanov face with the viscous term of
+    its speed, and the CFL step with the viscous term of its denominator on their own."""
+    from pyoracle import RefKernels
+    exa = _load()
+    if not os.path.exists(ADV_LIB):
+        pytest.skip("the application library was not built")
+    exa.load_user_pde(ADV_LIB)
+    order = 3
+    pde = exa.PDE_USER_BASE + 1
+    assert exa.pde_available(pde, dim, order, 0)
+    s = exa.Solver(pde, dim, order)
+    with pytest.raises(exa.ExaError):
+        exa.Solver(pde, dim, order, precision=exa.PREC_MIXED)  # the mixed form has no viscous flux
+    ref = RefKernels(dim, order, "advdiff")
+    rng = np.random.default_rng(3 + dim)
+    size = [1.0, 0.75, 1.25][:dim]
+    nc, nd = int(np.prod(ncell)), (order + 1) ** dim
+    luh0 = _advdiff_state(rng, ncell, order, size)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size)])
+    p.set_solution(luh0)
+    p.step(3)
+    got = p.get_solution()
+    want = luh0.copy()
+    t_ref, _, _ = ref.run(want, ncell, size, 3)
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert float(np.max(np.abs(got - want)) / np.max(np.abs(want))) < TOL
+    assert np.abs(got - luh0).max() > 1e-3
+    assert p.status() == 0
+    dx = np.array(size) / np.array(ncell)
+    for c in (0, nc // 2, nc - 1):
+        cell = luh0.reshape(nc, -1)[c]
+        dt = ref.dt(cell, dx)
+        assert abs(s.stable_time_step_size_cell(cell, dx) - dt) <= 1e-15 * dt
+        a, b = s.space_time_predictor(cell, dx, dt), ref.predictor(cell, dx, dt)
+        assert a["ret"] == b["ret"]
+        for k in ("lQhbnd", "lFhbnd", "lQhi"):
+            assert float(np.max(np.abs(a[k] - b[k])) / np.max(np.abs(b[k]))) < TOL, k
+        assert float(np.max(np.abs(a["lFhi"][:dim * nd * 3] - b["lFhi"][:dim * nd * 3])) /
+                     np.max(np.abs(b["lFhi"][:dim * nd * 3]))) < TOL
+    nf = (order + 1) ** (dim - 1)
+    for d in range(dim):
+        QL, QR = rng.normal(size=nf * 3), rng.normal(size=nf * 3)
+        FL, FR = rng.normal(size=nf * 3), rng.normal(size=nf * 3)
+        ga, gb = s.riemann_cell(FL, FR, QL, QR, dx, d)
+        ra, rb = ref.riemann(FL, FR, QL, QR, dx, d)
+        assert float(np.max(np.abs(ga - ra)) / np.max(np.abs(ra))) < 1e-14
+        assert float(np.max(np.abs(gb - rb)) / np.max(np.abs(rb))) < 1e-14
+    # the batched face entry point needs the cell size for a viscous flux
+    lib = exa.load_library()
+    assert lib.exa_riemann_solver_nonlinear(s.h, 0, None, None, None, None, None, None) != 0
+    p.close()
+    s.close()
