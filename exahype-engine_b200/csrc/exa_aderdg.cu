@@ -248,22 +248,42 @@ static void set_uniform(exa::CellArgs& a, const exa_solver* s, const double* dx,
   a.u_dt = dt;
 }
 
-int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double* luh, double* lduh, double* lQhbnd,
-                                        double* lFhbnd, int* picard_sweeps, const double* dx, double t, double dt,
-                                        void* stream) {
-  (void)t;
+}  // extern "C"
+
+static int fused_call(exa_solver* s, int ncells, const double* luh, double* lduh, double* lQhbnd, double* lFhbnd,
+                      int* picard_sweeps, const double* dx, const double* centres, double t, double dt,
+                      void* stream) {
   if (!s || ncells < 0 || (ncells > 0 && (!luh || !lduh || !lQhbnd || !lFhbnd || !dx)))
     return fail(EXA_ERR_INVALID, "null argument");
+  if (s->ops->alg_source && !centres)
+    return fail(EXA_ERR_INVALID, "an algebraic source needs the cells' centres: use the _x entry point");
   exa::CellArgs a = base_args(s, ncells);
   a.luh = luh;
   a.lduh = lduh;
   a.lQhbnd = lQhbnd;
   a.lFhbnd = lFhbnd;
   a.picard = picard_sweeps;
+  a.centres = centres;
+  a.u_t = t;
   set_uniform(a, s, dx, dt);
   EXA_CUDA(s->ops->reserve(ncells));
   EXA_CUDA(s->ops->predictor(a, (cudaStream_t)stream, s->cfg.precision == EXA_PREC_MIXED, s->pred_variant));
   return EXA_OK;
+}
+
+extern "C" {
+
+int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double* luh, double* lduh, double* lQhbnd,
+                                        double* lFhbnd, int* picard_sweeps, const double* dx, double t, double dt,
+                                        void* stream) {
+  return fused_call(s, ncells, luh, lduh, lQhbnd, lFhbnd, picard_sweeps, dx, nullptr, t, dt, stream);
+}
+
+int exa_fused_predictor_volume_integral_x(exa_solver* s, int ncells, const double* luh, double* lduh,
+                                          double* lQhbnd, double* lFhbnd, int* picard_sweeps, const double* dx,
+                                          const double* centres, double t, double dt, void* stream) {
+  if (ncells > 0 && !centres) return fail(EXA_ERR_INVALID, "null centres");
+  return fused_call(s, ncells, luh, lduh, lQhbnd, lFhbnd, picard_sweeps, dx, centres, t, dt, stream);
 }
 
 static int check_faces(int nfaces) { return nfaces < 0 ? fail(EXA_ERR_INVALID, "nfaces < 0") : EXA_OK; }
@@ -411,21 +431,26 @@ static int shim_scratch(exa_solver* s, size_t doubles) {
 int exa_spaceTimePredictorNonlinear(exa_solver* s, double* lQhbnd, double* lFhbnd, double* lQi, double* lFi,
                                     double* lQhi, double* lFhi, const double* luh, const double* cellCenter,
                                     const double* invDx, double t, double dt) {
-  (void)cellCenter;
-  (void)t;
-  if (!s || !lQhbnd || !lFhbnd || !luh || !invDx) {
+  if (!s || !lQhbnd || !lFhbnd || !luh || !invDx || (s->ops->alg_source && !cellCenter)) {
     fail(EXA_ERR_INVALID, "null argument");
     return -1;
   }
   std::lock_guard<std::mutex> lk(s->mu);
   const exa::Ops& o = *s->ops;
-  const size_t total = o.sz_luh + o.sz_lduh + o.sz_qhb + o.sz_fhb + o.sz_lQi + o.sz_lFi + o.sz_lQhi + o.sz_lFhi;
+  const size_t total = o.sz_luh + o.sz_lduh + o.sz_qhb + o.sz_fhb + o.sz_lQi + o.sz_lFi + o.sz_lQhi + o.sz_lFhi + 3;
   if (shim_scratch(s, total)) return -1;
   double* d = s->d_scratch;
   double *d_luh = d, *d_lduh = d_luh + o.sz_luh, *d_qhb = d_lduh + o.sz_lduh, *d_fhb = d_qhb + o.sz_qhb;
   double *d_lQi = d_fhb + o.sz_fhb, *d_lFi = d_lQi + o.sz_lQi, *d_lQhi = d_lFi + o.sz_lFi, *d_lFhi = d_lQhi + o.sz_lQhi;
+  double* d_centre = d_lFhi + o.sz_lFhi;
   if (cudaMemcpy(d_luh, luh, o.sz_luh * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+  // the cell's position and time reach an algebraic source (:339-345)
+  double centre[3] = {0.0, 0.0, 0.0};
+  for (int k = 0; k < s->cfg.dim && cellCenter; k++) centre[k] = cellCenter[k];
+  if (cudaMemcpy(d_centre, centre, sizeof(centre), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
   exa::CellArgs a = base_args(s, 1);
+  a.centres = d_centre;
+  a.u_t = t;
   a.luh = d_luh;
   a.lduh = d_lduh;
   a.lQhbnd = d_qhb;

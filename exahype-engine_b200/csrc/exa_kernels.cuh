@@ -178,6 +178,7 @@ struct CellArgs {
   const double* src;
   const double* grid_geo;        // [grid][6]: lower corner xyz, cells per axis xyz
   const long long* grid_first;   // [grid] first cell of the grid in the batch
+  const double* centres;         // [cell][3] cell centres (nullable: from grid_geo), for sources
   const double* grid_t;          // [grid] time at the start of the step (nullable: u_t)
   double u_t;
   // optional export of the predictor's internals, reference layouts (per-cell shims, tests)
@@ -280,6 +281,11 @@ __device__ __forceinline__ bool source_near(const double* src, const double* cen
 }
 // centre of cell `cell` of grid g from the grid geometry
 __device__ __forceinline__ void cell_centre(const CellArgs& a, long cell, int g, const double* dx, double* c) {
+  if (a.centres) {  // the caller's cell centres
+#pragma unroll
+    for (int k = 0; k < 3; k++) c[k] = a.centres[3 * cell + k];
+    return;
+  }
   const double* G = a.grid_geo + 6 * g;
   const long long loc = cell - (a.grid_first ? a.grid_first[g] : 0);
   const long long nx = (long long)G[3], ny = (long long)G[4];

@@ -25,6 +25,7 @@ struct Ops {
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
   bool ncp;
   bool viscous = false;  // the flux depends on the gradient (useViscousFlux)
+  bool alg_source = false;  // the functor has an algebraic source (useSource): needs cell positions
   virtual ~Ops() {}
   bool mixed_ok = false;  // mixed-precision predictor instantiated
   // Riemann launch form for all solvers of this instantiation: 0 riemann_kernel, otherwise
@@ -69,8 +70,10 @@ struct OpsImpl final : Ops {
   static constexpr bool kStreamed = S::predictor_smem + 4096 > 227 * 1024;
   // the mixed form needs PDEs without NCP and its larger shared-memory footprint must fit a CTA
   static constexpr bool kMixed = !kStreamed && !PDE::kNCP && !is_viscous<PDE>::value &&
+                                 !has_algebraic_source<PDE, DIM>::value &&
                                  MixShape<PDE, DIM, N, P>::smem_for(2) + 4096 <= 227 * 1024;
   static constexpr bool kAdj = PDE::kAdjoint && !PDE::kNCP && !is_viscous<PDE>::value &&
+                               !has_algebraic_source<PDE, DIM>::value &&
                                AdjShape<PDE, DIM, N, P>::smem <= 227 * 1024;
   // streamed predictor: scratch per device, grown on demand
   std::mutex scratch_mu;
@@ -329,6 +332,7 @@ struct OpsImpl final : Ops {
     adjoint_ok = kAdj;
     mixed_ok = kMixed;
     viscous = is_viscous<PDE>::value;
+    alg_source = has_algebraic_source<PDE, DIM>::value;
     adjust_ok = has_adjust_point_solution<PDE, DIM>::value;
     user_bc_ok = has_boundary_values<PDE, DIM>::value;
     dim = DIM;

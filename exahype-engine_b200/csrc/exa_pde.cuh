@@ -20,6 +20,9 @@
 //                                                boundaryValues for faces of type EXA_BC_USER:
 //                                                Qout (D values, pre-filled with Qin) and Fout (V,
 //                                                the normal flux of the outer state) at face node x
+//   algebraic_source<DIM>(x, t, Q, S)            algebraicSource: S[V] at the space-time node (x, t)
+//                                                (useSource), in the predictor's rhs and the volume
+//                                                integral's time-averaged source, minus the NCP
 //   static constexpr bool kViscous = true        the flux depends on the gradient (useViscousFlux):
 //   viscous_flux<DIM>(Q, gradQ, F)               viscousFlux, gradQ[d*V + m], replacing flux in
 //                                                the predictor
@@ -48,6 +51,14 @@ struct has_boundary_values<PDE, DIM,
                            std::void_t<decltype(PDE::template boundary_values<DIM>(
                                (const double*)nullptr, 0.0, 0.0, 0, 0, (const double*)nullptr, (const double*)nullptr,
                                (double*)nullptr, (double*)nullptr))>> : std::true_type {};
+
+template <class PDE, int DIM, class = void>
+struct has_algebraic_source : std::false_type {};
+template <class PDE, int DIM>
+struct has_algebraic_source<PDE, DIM,
+                            std::void_t<decltype(PDE::template algebraic_source<DIM>(
+                                (const double*)nullptr, 0.0, (const double*)nullptr, (double*)nullptr))>>
+    : std::true_type {};
 
 template <class PDE, class = void>
 struct is_viscous : std::false_type {};

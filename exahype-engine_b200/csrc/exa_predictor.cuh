@@ -9,8 +9,8 @@
 //
 // Work decomposition: one CTA per cell (several cells per CTA when a cell has fewer than 256
 // nodes), one thread per spatial node. A Picard sweep walks the n time nodes; per time node
-//   phase 1  each thread evaluates the flux (and the NCP source) of the old iterate at its node
-//            and writes it to shared memory,
+//   phase 1  each thread evaluates the flux (and the source, algebraicSource - NCP) of the old
+//            iterate at its node and writes it to shared memory,
 //   phase 2  every thread contracts whole lines (direction, variable, line) with Kxi, in place
 //            and already scaled by w_t w_a w_b dt/dx_d,
 //   phase 3  each thread forms its node's rhs of time node i, scaled by 1/w_xyz, and folds it
@@ -58,6 +58,8 @@ predictor_kernel(CellArgs a) {
   constexpr bool NCP = PDE::kNCP;
   constexpr bool VISC = is_viscous<PDE>::value;  // viscousFlux(Q, gradQ) replaces flux(Q)
   constexpr bool GRAD = NCP || VISC;               // the sweeps need the iterate's gradient
+  constexpr bool ALG = has_algebraic_source<PDE, DIM>::value;  // algebraicSource (useSource)
+  constexpr bool SRCT = NCP || ALG;                // a source slot S = algebraicSource - NCP
   static_assert(CPB <= 32, "the per-CTA cell mask holds 32 cells");
   extern __shared__ __align__(128) double smem[];
   double* sQ = smem;              // [CPB][n][nd][DQ]: old iterate slices, lQhi in the tail
@@ -202,6 +204,35 @@ predictor_kernel(CellArgs a) {
       srcOn = source_near<DIM>(a.src, cc, dxv);
       tcell = a.grid_t ? a.grid_t[g] : a.u_t;
     }
+    if (ALG && live) {
+      const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+      tcell = a.grid_t ? a.grid_t[g] : a.u_t;
+    }
+    // position of this node: cell centre + dx (node - 0.5), dx as 1 / (1 / dx) (:339-342)
+    auto node_x = [&](double* x) {
+      const int g = a.cell_grid ? a.cell_grid[cell] : 0;
+      const double dxv[3] = {1.0 / s_invdx[lc][0], DIM > 1 ? 1.0 / s_invdx[lc][1] : 1.0,
+                             DIM > 2 ? 1.0 / s_invdx[lc][2] : 1.0};
+      double cc[3];
+      cell_centre(a, cell, g, dxv, cc);
+#pragma unroll
+      for (int d = 0; d < 3; d++) x[d] = d < DIM ? cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5) : 0.0;
+    };
+    // S = algebraicSource(x, t + node_i dt, q) - NCP at time node i (:323-367); ncp_part holds -NCP
+    auto source_at = [&](int i, const double* q, const double* ncp_part, double* Sv) {
+      if constexpr (ALG) {
+        double x[3];
+        node_x(x);
+        PDE::template algebraic_source<DIM>(x, tcell + G::nodes(i) * dt, q, Sv);
+      } else {
+#pragma unroll
+        for (int m = 0; m < V; m++) Sv[m] = 0.0;
+      }
+      if (NCP) {
+#pragma unroll
+        for (int m = 0; m < V; m++) Sv[m] = ALG ? Sv[m] + ncp_part[m] : ncp_part[m];
+      }
+    };
     // source value of this node at time node i (evaluated only where srcOn)
     auto src_at = [&](int i) -> double {
       const int g = a.cell_grid ? a.cell_grid[cell] : 0;
@@ -299,7 +330,7 @@ predictor_kernel(CellArgs a) {
       double* e = a.ex_lFi + (size_t)cell * n * nd * (DIM + 1) * V + ((size_t)(i * nd + p) * (DIM + 1)) * V;
       for (int d = 0; d < DIM; d++)
         for (int m = 0; m < V; m++) e[d * V + m] = F[d * V + m];
-      for (int m = 0; m < V; m++) e[DIM * V + m] = NCP ? Sv[m] : 0.0;
+      for (int m = 0; m < V; m++) e[DIM * V + m] = SRCT ? Sv[m] : 0.0;
     };
 
     int sweeps = 0;
@@ -307,7 +338,7 @@ predictor_kernel(CellArgs a) {
     bool last_old_is_luh = true;  // the last sweep started from lQi = luh (sweep 0)
     for (int s = 0; s < maxIter; s++) {
       const bool work = live && ((active >> lc) & 1u);
-      if (GRAD && work) {
+      if ((GRAD || SRCT) && work) {
 #pragma unroll
         for (int d = 0; d < (GRAD ? DIM : 1); d++)
 #pragma unroll
@@ -340,14 +371,35 @@ predictor_kernel(CellArgs a) {
             for (int d = 0; d < (GRAD ? DIM : 1); d++)
 #pragma unroll
               for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
-            if (NCP) {
+            if (NCP && !ALG) {
 #pragma unroll
               for (int m = 0; m < V; m++) sh[m] = fma(S0[m], wi, sh[m]);
             }
           }
         }
-        if (GRAD && a.ex_lFi && work)
+        // an algebraic source depends on the time node: lShi, and its part of the closed-form
+        // time solve, dt sum_i iK1[t][i] w_i S_i, accumulated in qn
+        if (ALG && work) {
+#pragma unroll
+          for (int t = 0; t < n; t++)
+#pragma unroll
+            for (int m = 0; m < V; m++) qn[t][m] = 0.0;
+          for (int i = 0; i < n; i++) {
+            const double wi = G::weights(i);
+            double Si[V];
+            source_at(i, u, S0, Si);
+#pragma unroll
+            for (int m = 0; m < V; m++) sh[m] = fma(Si[m], wi, sh[m]);
+            const double wdt = wi * dt;
+#pragma unroll
+            for (int m = 0; m < V; m++)
+#pragma unroll
+              for (int t = 0; t < n; t++) qn[t][m] = fma(G::iK1(t, i), wdt * Si[m], qn[t][m]);
+            if (a.ex_lFi) export_flux(i, F, Si);
+          }
+        } else if (GRAD && a.ex_lFi && work) {
           for (int i = 0; i < n; i++) export_flux(i, F, S0);
+        }
         __syncthreads();
         contract(1.0);
         __syncthreads();
@@ -379,7 +431,8 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
             for (int t = 0; t < n; t++) {
               double q1 = u[m] * s_A[t] - iweight * o[m] * s_B[t];
-              if (NCP) q1 += dt * S0[m] * s_B[t];
+              if (NCP && !ALG) q1 += dt * S0[m] * s_B[t];
+              if (ALG) q1 += qn[t][m];
               if (PDE::kSource && srcOn && m == srcVar) q1 += cs[t];
               const double dl = q1 - u[m];
               res = fma(dl, dl, res);
@@ -396,7 +449,7 @@ predictor_kernel(CellArgs a) {
         }
 #pragma unroll
         for (int i = 0; i < n; i++) {
-          // phase 1: flux (and NCP source) of the old iterate at time node i (:196-227, :323-367)
+          // phase 1: flux (and source) of the old iterate at time node i (:196-227, :323-367)
           double q[D];
 #pragma unroll
           for (int m = 0; m < D; m++) q[m] = m < V ? q_s[(i * nd + p) * DQ + m] : u[m];
@@ -416,17 +469,25 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
             for (int m = 0; m < V; m++) Si[m] = -B[m];
           }
-          if (GRAD && work) {
+          if constexpr (ALG) {
+            double nS[V];
 #pragma unroll
-            for (int d = 0; d < (GRAD ? DIM : 1); d++)
+            for (int m = 0; m < V; m++) nS[m] = NCP ? Si[m] : 0.0;
+            source_at(i, q, nS, Si);
+          }
+          if ((GRAD || SRCT) && work) {
+            if (GRAD) {
 #pragma unroll
-              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
-            if (NCP) {
+              for (int d = 0; d < (GRAD ? DIM : 1); d++)
+#pragma unroll
+                for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+            }
+            if (SRCT) {
 #pragma unroll
               for (int m = 0; m < V; m++) sh[m] = fma(Si[m], wi, sh[m]);
             }
           }
-          if (GRAD && a.ex_lFi && work) export_flux(i, F, Si);
+          if ((GRAD || SRCT) && a.ex_lFi && work) export_flux(i, F, Si);
           __syncthreads();
           // phase 2
           contract(wi);
@@ -441,7 +502,7 @@ predictor_kernel(CellArgs a) {
               if (PDE::kSource && srcOn && m == srcVar) rhs += wi * w_sp * dt * si;
 #pragma unroll
               for (int d = 0; d < DIM; d++) rhs -= f_s[(d * V + m) * BS + off[d]];
-              if (NCP) rhs += wi * w_sp * dt * Si[m];
+              if (SRCT) rhs += wi * w_sp * dt * Si[m];
               // iK1 time solve (:370-405), one time node of the rhs at a time
               const double r = iweight * rhs;
 #pragma unroll
@@ -552,7 +613,7 @@ predictor_kernel(CellArgs a) {
           const double wi = G::weights(i);
 #pragma unroll
           for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
-          if (live && a.ex_lFi) export_flux(i, F, nullptr);
+          if (!SRCT && live && a.ex_lFi) export_flux(i, F, nullptr);  // else exported by the sweeps
         }
       } else {
 #pragma unroll
@@ -564,7 +625,7 @@ predictor_kernel(CellArgs a) {
           const double wi = G::weights(i);
 #pragma unroll
           for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
-          if (live && a.ex_lFi) export_flux(i, F, nullptr);
+          if (!SRCT && live && a.ex_lFi) export_flux(i, F, nullptr);  // else exported by the sweeps
         }
       }
     }
@@ -580,15 +641,15 @@ predictor_kernel(CellArgs a) {
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[GRAD ? d : 0][m];
-        if (NCP) {
-#pragma unroll
-          for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
-        }
       } else {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
           for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(GRAD ? 0 : d * V + m)];
+      }
+      if (SRCT) {
+#pragma unroll
+        for (int m = 0; m < V; m++) sh_s[p * V + m] = sh[m];
       }
     }
     if (live && a.ex_lQhi) {
@@ -601,7 +662,7 @@ predictor_kernel(CellArgs a) {
         const int idx = node_line<DIM, n>(p, d) * n + co[d];
         for (int m = 0; m < V; m++) e[(size_t)d * nd * V + idx * V + m] = f_s[(d * V + m) * BS + off[d]];
       }
-      for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = NCP ? sh[m] : 0.0;
+      for (int m = 0; m < V; m++) e[(size_t)DIM * nd * V + p * V + m] = SRCT ? sh[m] : 0.0;
     }
     __syncthreads();
 
@@ -626,7 +687,7 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
           for (int mm = 0; mm < n; mm++) acc[m] += kr[mm] * f_s[(d * V + m) * BS + base + mm * st] * us;
       }
-      if (NCP) {
+      if (SRCT) {  // time-averaged source lShi (volumeIntegralNonlinear :211-221)
 #pragma unroll
         for (int m = 0; m < V; m++) acc[m] += w_sp * sh_s[p * V + m];
       }

@@ -44,8 +44,8 @@ predictor_streamed_kernel(CellArgs a) {
   using S = Shape<PDE, DIM, N, P>;
   using G = GL<N>;
   constexpr int n = T::n, V = T::V, D = T::D, nd = T::nd, NL = T::NL, BS = T::BS, nf = S::nf;
-  static_assert(!PDE::kNCP && !is_viscous<PDE>::value,
-                "the streamed predictor is built for PDEs without NCP or viscous flux");
+  static_assert(!PDE::kNCP && !is_viscous<PDE>::value && !has_algebraic_source<PDE, DIM>::value,
+                "the streamed predictor is built for PDEs without NCP, viscous flux or algebraic source");
   static_assert(T::TPB <= 1024, "one thread per node");
   extern __shared__ double smem[];
   double* sF = smem;                          // [DIM][V][BS]

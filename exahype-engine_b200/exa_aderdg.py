@@ -106,6 +106,7 @@ def load_library(path=None):
         "exa_solver_set_update_variant": [vp, i],
         "exa_solver_status": [vp, ctypes.POINTER(ctypes.c_uint)],
         "exa_fused_predictor_volume_integral": [vp, i, vp, vp, vp, vp, vp, dp, d, d, vp],
+        "exa_fused_predictor_volume_integral_x": [vp, i, vp, vp, vp, vp, vp, dp, vp, d, d, vp],
         "exa_riemann_solver_nonlinear": [vp, i, vp, vp, vp, vp, vp, vp],
         "exa_boundary_conditions_wall": [vp, i, vp, vp, vp, vp, vp],
         "exa_riemann_solver_nonlinear_dx": [vp, i, vp, vp, vp, vp, vp, vp, vp],
@@ -284,11 +285,19 @@ class Solver:
         _check(self.lib.exa_solver_set_predictor_variant(self.h, int(v)), "exa_solver_set_predictor_variant")
 
     # ---- batched, device tensors -------------------------------------------------------
-    def fused_predictor_volume_integral(self, luh, lduh, lQhbnd, lFhbnd, dx, dt, t=0.0, picard=None, stream=None):
+    def fused_predictor_volume_integral(self, luh, lduh, lQhbnd, lFhbnd, dx, dt, t=0.0, picard=None, stream=None,
+                                        centres=None):
+        """centres (CUDA float64 [cells][3]): the cells' centres, which an algebraic source needs."""
         ncells = luh.numel() // self.sizes["luh"]
-        _check(self.lib.exa_fused_predictor_volume_integral(
-            self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(picard), _dx3(dx, self.dim),
-            float(t), float(dt), _stream(stream)), "exa_fused_predictor_volume_integral")
+        if centres is None:
+            _check(self.lib.exa_fused_predictor_volume_integral(
+                self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(picard),
+                _dx3(dx, self.dim), float(t), float(dt), _stream(stream)), "exa_fused_predictor_volume_integral")
+        else:
+            _check(self.lib.exa_fused_predictor_volume_integral_x(
+                self.h, ncells, _ptr(luh), _ptr(lduh), _ptr(lQhbnd), _ptr(lFhbnd), _ptr(picard),
+                _dx3(dx, self.dim), _ptr(centres), float(t), float(dt), _stream(stream)),
+                "exa_fused_predictor_volume_integral_x")
 
     def riemann(self, left, right, direction, lQhbnd, lFhbnd, stream=None, dx=None):
         """dx (the cells' size) is needed by PDEs with a viscous flux."""

@@ -153,6 +153,13 @@ int exa_solver_set_update_variant(exa_solver* s, int variant);
 int exa_fused_predictor_volume_integral(exa_solver* s, int ncells, const double* luh, double* lduh,
                                         double* lQhbnd, double* lFhbnd, int* picard_sweeps, const double* dx,
                                         double t, double dt, void* stream);
+/* The same with the cells' centres (device, [cell][3]), which an application functor's
+ * algebraic_source needs (the reference's algebraicSource at x = centre + dx (node - 0.5) and
+ * t + node_i dt, 3d/spaceTimePredictorNonlinear.cpph:323-367); PDEs with an algebraic source refuse
+ * the call without them. */
+int exa_fused_predictor_volume_integral_x(exa_solver* s, int ncells, const double* luh, double* lduh,
+                                          double* lQhbnd, double* lFhbnd, int* picard_sweeps, const double* dx,
+                                          const double* centres, double t, double dt, void* stream);
 
 /* Replaces riemannSolverNonlinear<useNCP,false> (3d/riemannSolverNonlinear.cpph:37-128) for a
  * list of interior faces: face f joins cell left[f] (its face 2*dir[f]+1) and cell right[f]

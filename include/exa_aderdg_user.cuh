@@ -23,6 +23,9 @@
  *                                                                     double dt, double* Q);
  *     template <int DIM> static __device__ void boundary_values(const double* x, double t, double dt,
  *         int faceIndex, int normal, const double* Fin, const double* Qin, double* Fout, double* Qout);
+ *     // the reference's algebraicSource (useSource): S[V] at the space-time node (x[3], t)
+ *     template <int DIM> static __device__ void algebraic_source(const double* x, double t,
+ *                                                                const double* Q, double* S);
  *     // a flux that depends on the gradient (the reference's useViscousFlux, viscousFlux and
  *     // viscousEigenvalues): gradQ[d * V + m]
  *     static constexpr bool kViscous = true;
@@ -44,6 +47,12 @@
  * scratch. That predictor takes systems without an NCP, and one time node's fluxes
  * (DIM * V * n^DIM doubles) must still fit the CTA. A static_assert names an instantiation that
  * fits neither form.
+ *
+ * With algebraic_source the predictor adds S(x, t + node_i dt, Q) - NCP at every space-time node
+ * and the volume integral its time average, as the reference does; x = cell centre + dx (node -
+ * 0.5), with z = 0 in 2D. The cell positions come from the patch, from the per-cell shim's
+ * cellCenter, or from exa_fused_predictor_volume_integral_x (the batched call without centres
+ * refuses such a PDE). No mixed-precision form, streamed predictor or adjoint for it.
  *
  * With kViscous the predictor evaluates viscous_flux at every node and time node with the gradient
  * of the Picard iterate there; the Rusanov speed and the CFL step add the viscous eigenvalues' terms

@@ -157,7 +157,7 @@ class RefKernels:
             raise AttributeError("instantiation %s not built" % self.prefix)
         self.dim, self.n = dim, order + 1
         self.v = {"euler": 5, "swe": 4, "acoustic": 4, "elastic": 9, "acousticfixed": 4, "elasticfixed": 9,
-                  "advdiff": 3}[pde]
+                  "advdiff": 3, "advreact": 3}[pde]
         src = (ctypes.c_double * 8)(*(list(source) if source is not None else [0, 0, 0, 0, 0, 0, 1, 0]))
         self.lib.exaref_set_source(src, 1 if source is not None else 0)
         self.D = self.v + npar

@@ -225,6 +225,29 @@ struct AdvDiffPDE {
 constexpr double AdvDiffPDE::a[3][3];
 constexpr double AdvDiffPDE::nu[3];
 
+// The same three advected scalars with a space-, time- and state-dependent algebraic source: the
+// test system of the algebraicSource path (useSource). The GPU functor of the tests defines the same
+// system.
+struct AdvReactPDE {
+  static constexpr int NumberOfVariables = 3;
+  static constexpr bool HasSource = true;
+  static void flux(const double* const Q, double** const F) { AdvDiffPDE::flux(Q, F); }
+  static void eigenvalues(const double* const Q, const int d, double* const lambda) {
+    AdvDiffPDE::eigenvalues(Q, d, lambda);
+  }
+  // x: 3 coordinates (z = 0 in 2D)
+  static void algebraicSource(const double* x, double t, const double* const Q, double* S) {
+    const double pi = 3.14159265358979323846;
+    S[0] = -0.5 * Q[0] + 0.2 * Q[1] + 0.1 * std::sin(2.0 * pi * (x[0] + 2.0 * x[1] + 3.0 * x[2]) - t);
+    S[1] = -0.3 * Q[1] * Q[2];
+    S[2] = 0.05 * std::cos(2.0 * pi * x[0]) - 0.4 * Q[2];
+  }
+  static void nonConservativeProduct(const double* const, const double* const, double* const B) {
+    std::fill_n(B, 3, 0.0);
+  }
+  static void wall(const double* QIn, int, double* QOut) { std::copy_n(QIn, 3, QOut); }
+};
+
 // Point source of the acoustic / elastic solvers (x, y, z, f0, t0, amplitude, width, variable):
 // a unit-mass Gaussian of the given width times a Ricker wavelet, acting only on cells whose
 // centre is within 6 widths plus a cell diagonal (the per-cell truncation the GPU path and the
@@ -314,6 +337,16 @@ template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::Kxi = 
 template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::dudx = kernels::legendre::dudx;
 template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::iK1 = kernels::legendre::iK1;
 template <class P, int O, int N, bool X> double*** RefSolver<P, O, N, X>::FCoeff = kernels::legendre::FCoeff;
+
+// The solver of a PDE with its own algebraic source (useSource = true): hides the base's point source.
+template <class PDE, int ORDER>
+struct RefSrcSolver : RefSolver<PDE, ORDER, 0> {
+  void algebraicSource(const tarch::la::Vector<DIMENSIONS, double>& x, double t, const double* const Q, double* S) {
+    double xs[3] = {0.0, 0.0, 0.0};
+    for (int d = 0; d < DIMENSIONS; d++) xs[d] = x[d];
+    PDE::algebraicSource(xs, t, Q, S);
+  }
+};
 
 // The solver of a PDE with a viscous flux: the kernels call these members when instantiated with
 // useViscousFlux = true (they hide the base's empty ones).
@@ -774,6 +807,9 @@ extern "C" void exalin_eigenvalues(int elastic, const double* Q, double* l) {
 #define EXAREF_DEFINE(NAME, PDE, O, P, NCP) EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, false, false)
 #define EXAREF_DEFINE_S(NAME, PDE, O, P, NCP, SRC, FIXED) \
   EXAREF_DEFINE_G(NAME, EXAREF_S(PDE, O, P, FIXED), exaref::PDE::NumberOfVariables, O, NCP, SRC, false)
+// a PDE with its own algebraic source (useSource = true), no parameters
+#define EXAREF_DEFINE_A(NAME, PDE, O) \
+  EXAREF_DEFINE_G(NAME, exaref::RefSrcSolver<exaref::PDE COMMA O>, exaref::PDE::NumberOfVariables, O, false, true, false)
 // a PDE with a viscous flux (useViscousFlux = true), no parameters
 #define EXAREF_DEFINE_V(NAME, PDE, O) \
   EXAREF_DEFINE_G(NAME, exaref::RefViscSolver<exaref::PDE COMMA O>, exaref::PDE::NumberOfVariables, O, false, false, true)
@@ -845,6 +881,7 @@ EXAREF_DEFINE(exaref3d_euler_o3_p1, EulerPDE, 3, 1, false)
 EXAREF_DEFINE(exaref3d_euler_o5_p0, EulerPDE, 5, 0, false)
 EXAREF_DEFINE(exaref3d_euler_o2_p0, EulerPDE, 2, 0, false)
 EXAREF_DEFINE_V(exaref3d_advdiff_o3_p0, AdvDiffPDE, 3)
+EXAREF_DEFINE_A(exaref3d_advreact_o3_p0, AdvReactPDE, 3)
 #else
 EXAREF_DEFINE(exaref2d_euler_o3_p0, EulerPDE, 3, 0, false)
 EXAREF_DEFINE(exaref2d_euler_o3_p1, EulerPDE, 3, 1, false)
@@ -852,4 +889,5 @@ EXAREF_DEFINE(exaref2d_euler_o5_p0, EulerPDE, 5, 0, false)
 EXAREF_DEFINE(exaref2d_swe_o4_p0, SWEPDE, 4, 0, true)
 EXAREF_DEFINE(exaref2d_swe_o2_p0, SWEPDE, 2, 0, true)
 EXAREF_DEFINE_V(exaref2d_advdiff_o3_p0, AdvDiffPDE, 3)
+EXAREF_DEFINE_A(exaref2d_advreact_o3_p0, AdvReactPDE, 3)
 #endif

@@ -175,3 +175,72 @@ def test_viscous_flux_pde_vs_reference_kernels(dim, ncell):
     assert lib.exa_riemann_solver_nonlinear(s.h, 0, None, None, None, None, None, None) != 0
     p.close()
     s.close()
+
+
+REACT_LIB = os.path.join(REPO, "tests", "user_pde", "libuser_advreact.so")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dim,ncell,bc", [(3, (4, 3, 5), 0), (3, (3, 4, 3), 1), (2, (9, 7), 0), (2, (8, 6), 1)])
+def test_algebraic_source_pde_vs_reference_kernels(dim, ncell, bc):
+    """A PDE with its own algebraic source (useSource: position-, time- and state-dependent)
+    through the application-functor route (tests/user_pde/user_advreact.cu) against the reference's
+    own generic kernels instantiated with useSource for the same system: three steps on periodic or
+    wall-bounded grids to 1e-12 with equal time steps; the per-cell predictor at a non-zero time
+    (its return value, the face values, lQhi and lFhi with the time-averaged source block); and the
+    batched predictor with the cells' centres against the reference's volume integral."""
+    import torch
+    from pyoracle import RefKernels
+    exa = _load()
+    if not os.path.exists(REACT_LIB):
+        pytest.skip("the application library was not built")
+    exa.load_user_pde(REACT_LIB)
+    order = 3
+    pde = exa.PDE_USER_BASE + 2
+    s = exa.Solver(pde, dim, order)
+    ref = RefKernels(dim, order, "advreact")
+    rng = np.random.default_rng(11 + dim + bc)
+    size = [1.0, 0.75, 1.25][:dim]
+    nc, nd = int(np.prod(ncell)), (order + 1) ** dim
+    luh0 = _advdiff_state(rng, ncell, order, size)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=bc)])
+    p.set_solution(luh0)
+    p.step(3)
+    got = p.get_solution()
+    want = luh0.copy()
+    t_ref, _, _ = ref.run(want, ncell, size, 3, walls=bc == 1)
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert float(np.max(np.abs(got - want)) / np.max(np.abs(want))) < TOL
+    assert np.abs(got - luh0).max() > 1e-4
+    assert p.status() == 0
+    dx = np.array(size) / np.array(ncell)
+    cells = luh0.reshape(nc, -1)
+    centres = np.zeros((nc, 3))
+    idx = np.arange(nc)
+    for d in range(dim):
+        stride = int(np.prod(ncell[:d]))
+        centres[:, d] = ((idx // stride) % ncell[d] + 0.5) * dx[d]
+    t0, dt = 0.3, 0.5 * ref.dt(cells[0], dx)
+    for c in (0, nc // 2, nc - 1):
+        a = s.space_time_predictor(cells[c], dx, dt, centre=centres[c], t=t0)
+        b = ref.predictor(cells[c], dx, dt, centre=centres[c], t=t0)
+        assert a["ret"] == b["ret"]
+        for k in ("lQhbnd", "lFhbnd", "lQhi", "lFhi"):
+            assert float(np.max(np.abs(a[k] - b[k])) / np.max(np.abs(b[k]))) < TOL, (c, k)
+    dev = torch.device("cuda")
+    t_luh = torch.from_numpy(luh0).to(dev)
+    lduh = torch.zeros(nc * nd * 3, dtype=torch.float64, device=dev)
+    qhb = torch.zeros(nc * s.sizes["lQhbnd"], dtype=torch.float64, device=dev)
+    fhb = torch.zeros_like(qhb)
+    with pytest.raises(exa.ExaError):  # the cells' positions are needed
+        s.fused_predictor_volume_integral(t_luh, lduh, qhb, fhb, dx, dt, t=t0)
+    s.fused_predictor_volume_integral(t_luh, lduh, qhb, fhb, dx, dt, t=t0,
+                                      centres=torch.from_numpy(centres).to(dev))
+    torch.cuda.synchronize()
+    lduh = lduh.cpu().numpy().reshape(nc, -1)
+    for c in (1, nc // 3, nc - 2):
+        b = ref.predictor(cells[c], dx, dt, centre=centres[c], t=t0)
+        want_du = ref.volume(b["lFhi"], dx)
+        assert float(np.max(np.abs(lduh[c] - want_du)) / np.max(np.abs(want_du))) < TOL, c
+    p.close()
+    s.close()
