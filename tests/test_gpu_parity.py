@@ -308,6 +308,34 @@ def test_patch_steps_vs_oracle(exa, dim, order, ncell, steps, walls):
     assert p.status() == 0
 
 
+@pytest.mark.parametrize("dim,ncell,walls", [
+    (3, (1, 1, 1), False), (3, (1, 2, 3), False), (3, (3, 1, 2), False), (3, (1, 1, 4), True),
+    (3, (2, 1, 1), True), (2, (1, 1), False), (2, (7, 1), False), (2, (1, 5), True), (2, (1, 1), True)])
+def test_degenerate_grids_vs_oracle(exa, dim, ncell, walls):
+    """Grids one cell thick along some axes: a periodic axis of one cell makes the cell its own
+    neighbour (the face joins its high and its low face), a wall-bounded one gives the cell two
+    domain faces on that axis. Three steps against the oracle at 1e-12 with equal time steps and
+    the last step's Picard-sweep histogram."""
+    order = 3
+    rng = np.random.default_rng(17)
+    nc, nd = int(np.prod(ncell)), (order + 1) ** dim
+    luh0 = euler_cells(rng, nc, nd, amp=0.05, dim=dim).reshape(-1)
+    size = [0.5, 0.6, 0.7][:dim]
+    o = Oracle(dim, order)
+    ref = luh0.copy()
+    t_ref, _, pic = o.run(ref, ncell, size, 3, walls=walls, want_picard=True)
+    s = exa.Solver(exa.PDE_EULER, dim, order)
+    p = exa.Patch(s, [dict(ncell=ncell, size=size, bc=exa.BC_WALL if walls else exa.BC_PERIODIC)])
+    p.set_solution(luh0)
+    p.step(3)
+    got = p.get_solution()
+    assert abs(p.time()[0][0] - t_ref) <= 1e-13 * t_ref
+    assert rel(got, ref) < TOL
+    assert list(np.bincount(pic[-1], minlength=32)[:32]) == p.stats()["picard_hist"]
+    assert p.status() == 0
+    p.close()
+
+
 def test_patch_swe_walls_vs_oracle(exa):
     """2D shallow water with bathymetry (NCP) and reflective walls."""
     rng = np.random.default_rng(9)
