@@ -917,3 +917,38 @@ def test_step_host_fixed_then_cfl_and_halo_refusal(exa, torch):
         halo.step_host(buf, buf)
     for p in (dev, host, halo):
         p.close()
+
+
+def test_empty_batches_and_argument_checks(exa, torch):
+    """Zero cells or faces are valid batches that launch nothing and leave the outputs untouched;
+    null arrays with a non-empty batch, negative counts and out-of-range directions are refused on
+    the host with EXA_ERR_INVALID, before any launch (the reference's kernels take one cell at a
+    time, so these are the batched interface's own edge cases)."""
+    lib = exa.load_library()
+    s = exa.Solver(exa.PDE_EULER, 3, 3)
+    dev = torch.device("cuda")
+    sentinel = torch.full((64,), 7.0, dtype=torch.float64, device=dev)
+    ptr = sentinel.data_ptr()
+    import ctypes
+    dx = (ctypes.c_double * 3)(0.1, 0.1, 0.1)
+    null = None
+    # empty batches: OK, nothing written
+    assert lib.exa_fused_predictor_volume_integral(s.h, 0, null, null, null, null, null, dx, 0.0, 1e-3, null) == 0
+    assert lib.exa_riemann_solver_nonlinear(s.h, 0, null, null, null, null, null, null) == 0
+    assert lib.exa_boundary_conditions_wall(s.h, 0, null, null, null, null, null) == 0
+    assert lib.exa_surface_integral_and_update(s.h, 0, null, null, null, dx, 1e-3, null) == 0
+    assert lib.exa_solution_update(s.h, 0, null, null, null, 1e-3, null) == 0
+    torch.cuda.synchronize()
+    assert bool((sentinel == 7.0).all())
+    # refused on the host
+    assert lib.exa_fused_predictor_volume_integral(s.h, 1, null, ptr, ptr, ptr, null, dx, 0.0, 1e-3, null) == 1
+    assert lib.exa_fused_predictor_volume_integral(s.h, -1, ptr, ptr, ptr, ptr, null, dx, 0.0, 1e-3, null) == 1
+    assert lib.exa_riemann_solver_nonlinear(s.h, -1, null, null, null, null, null, null) == 1
+    assert lib.exa_riemann_solver_nonlinear(s.h, 2, null, null, null, ptr, ptr, null) == 1
+    assert lib.exa_stable_time_step_size(s.h, -1, null, dx, null, null, null) == 1
+    FL = FR = QL = QR = np.zeros(16 * 5)
+    with pytest.raises(exa.ExaError):
+        s.riemann_cell(FL, FR, QL, QR, 0.1, 3)  # direction out of range in 3D
+    assert s.status() == 0
+    assert bool((sentinel == 7.0).all())
+    s.close()
