@@ -58,6 +58,9 @@ predictor_kernel(CellArgs a) {
   constexpr bool NCP = PDE::kNCP;
   constexpr bool VISC = is_viscous<PDE>::value;  // viscousFlux(Q, gradQ) replaces flux(Q)
   constexpr bool GRAD = NCP || VISC;               // the sweeps need the iterate's gradient
+  // the time-averaged flux is accumulated during the sweeps only where the flux needs the gradient;
+  // otherwise the tail recomputes it from the last old iterate (fewer registers in the sweeps)
+  constexpr bool FHACC = VISC;
   constexpr bool ALG = has_algebraic_source<PDE, DIM>::value;  // algebraicSource (useSource)
   constexpr bool SRCT = NCP || ALG;                // a source slot S = algebraicSource - NCP
   static_assert(CPB <= 32, "the per-CTA cell mask holds 32 cells");
@@ -254,7 +257,7 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
         for (int m = 0; m < D; m++) q_s[(t * nd + p) * DQ + m] = u[m];
     }
-    double fh[GRAD ? DIM : 1][V];  // time-averaged flux / source of the sweep (gradient path only)
+    double fh[FHACC ? DIM : 1][V];  // time-averaged flux of the sweep (viscous flux only)
     double sh[V];
     (void)fh;
     (void)sh;
@@ -338,9 +341,9 @@ predictor_kernel(CellArgs a) {
     bool last_old_is_luh = true;  // the last sweep started from lQi = luh (sweep 0)
     for (int s = 0; s < maxIter; s++) {
       const bool work = live && ((active >> lc) & 1u);
-      if ((GRAD || SRCT) && work) {
+      if ((FHACC || SRCT) && work) {
 #pragma unroll
-        for (int d = 0; d < (GRAD ? DIM : 1); d++)
+        for (int d = 0; d < (FHACC ? DIM : 1); d++)
 #pragma unroll
           for (int m = 0; m < V; m++) fh[d][m] = 0.0;
 #pragma unroll
@@ -364,13 +367,15 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
           for (int m = 0; m < V; m++) S0[m] = -B[m];
         }
-        if (GRAD && work) {
+        if ((FHACC || (NCP && !ALG)) && work) {
           for (int i = 0; i < n; i++) {
             const double wi = G::weights(i);
+            if (FHACC) {
 #pragma unroll
-            for (int d = 0; d < (GRAD ? DIM : 1); d++)
+              for (int d = 0; d < (FHACC ? DIM : 1); d++)
 #pragma unroll
-              for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+                for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
+            }
             if (NCP && !ALG) {
 #pragma unroll
               for (int m = 0; m < V; m++) sh[m] = fma(S0[m], wi, sh[m]);
@@ -475,10 +480,10 @@ predictor_kernel(CellArgs a) {
             for (int m = 0; m < V; m++) nS[m] = NCP ? Si[m] : 0.0;
             source_at(i, q, nS, Si);
           }
-          if ((GRAD || SRCT) && work) {
-            if (GRAD) {
+          if ((FHACC || SRCT) && work) {
+            if (FHACC) {
 #pragma unroll
-              for (int d = 0; d < (GRAD ? DIM : 1); d++)
+              for (int d = 0; d < (FHACC ? DIM : 1); d++)
 #pragma unroll
                 for (int m = 0; m < V; m++) fh[d][m] = fma(F[d * V + m], wi, fh[d][m]);
             }
@@ -598,12 +603,12 @@ predictor_kernel(CellArgs a) {
     }
     // the old iterate of the last sweep, before its slot 0 takes lQhi (each thread reads and
     // writes only its own node, so no barrier is needed in between)
-    double fa[GRAD ? 1 : DIM * V];
+    double fa[FHACC ? 1 : DIM * V];
     (void)fa;
-    if (!GRAD && inr) {
+    if (!FHACC && inr) {
       // lFhi = sum_t w_t F(old iterate at t), accumulated in registers
 #pragma unroll
-      for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = 0.0;
+      for (int k = 0; k < (FHACC ? 1 : DIM * V); k++) fa[k] = 0.0;
       if (last_old_is_luh) {
         // the old iterate is luh at every time node: one flux, the same weighted sum
         double F[DIM * V];
@@ -612,7 +617,7 @@ predictor_kernel(CellArgs a) {
         for (int i = 0; i < n; i++) {
           const double wi = G::weights(i);
 #pragma unroll
-          for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
+          for (int k = 0; k < (FHACC ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
           if (!SRCT && live && a.ex_lFi) export_flux(i, F, nullptr);  // else exported by the sweeps
         }
       } else {
@@ -624,7 +629,7 @@ predictor_kernel(CellArgs a) {
           PDE::template flux<DIM>(q, F);
           const double wi = G::weights(i);
 #pragma unroll
-          for (int k = 0; k < (GRAD ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
+          for (int k = 0; k < (FHACC ? 1 : DIM * V); k++) fa[k] = fma(F[k], wi, fa[k]);
           if (!SRCT && live && a.ex_lFi) export_flux(i, F, nullptr);  // else exported by the sweeps
         }
       }
@@ -636,16 +641,16 @@ predictor_kernel(CellArgs a) {
     if (inr) {
 #pragma unroll
       for (int m = 0; m < D; m++) qh_s[p * DQ + m] = qh[m];
-      if (GRAD) {
+      if (FHACC) {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[GRAD ? d : 0][m];
+          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fh[FHACC ? d : 0][m];
       } else {
 #pragma unroll
         for (int d = 0; d < DIM; d++)
 #pragma unroll
-          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(GRAD ? 0 : d * V + m)];
+          for (int m = 0; m < V; m++) f_s[(d * V + m) * BS + off[d]] = fa[(FHACC ? 0 : d * V + m)];
       }
       if (SRCT) {
 #pragma unroll
