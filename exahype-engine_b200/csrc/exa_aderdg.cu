@@ -899,6 +899,11 @@ struct exa_patch {
   double* grid_geo = nullptr;       // [grid][6]: lower corner, cells per axis
   long long* grid_first_d = nullptr; // [grid] first cell
   double* src = nullptr;            // point source parameters (8 doubles), nullptr when unset
+  // the source's slot table (Ops::source_slots) and its values per slot, time node and node
+  int* src_slot = nullptr;
+  int* src_cells = nullptr;
+  double* src_vals = nullptr;
+  int nsrc = 0;
   int8_t* btype = nullptr;          // boundary type of every domain face
   // halo (slab decomposition): ghost cells appended after the real cells, face traces only
   long long nghost = 0;      // 2 * layer cells, or 0
@@ -923,7 +928,7 @@ static void patch_free(exa_patch* p) {
   if (p->graph_fixed) cudaGraphExecDestroy(p->graph_fixed);
   void* ptrs[] = {p->luh, p->lduh, p->lQhbnd, p->lFhbnd, p->picard, p->cell_grid, p->grid_dx, p->grid_t,
                   p->grid_dt, p->grid_dt_next, p->steps, p->fL, p->fR, p->fdir, p->bcell, p->bface, p->status,
-                  p->grid_geo, p->grid_first_d, p->src, p->btype, p->adjQ, p->adjF, p->adj_iter, p->adj_lam};
+                  p->grid_geo, p->grid_first_d, p->src, p->src_slot, p->src_cells, p->src_vals, p->btype, p->adjQ, p->adjF, p->adj_iter, p->adj_lam};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   for (cudaEvent_t e : p->ev_in) cudaEventDestroy(e);
@@ -951,6 +956,12 @@ static exa::CellArgs patch_args(exa_patch* p) {
   a.grid_geo = p->grid_geo;
   a.grid_first = p->grid_first_d;
   a.src = p->src;
+  if (p->src && p->src_slot) {
+    a.src_slot = p->src_slot;
+    a.src_cells = p->src_cells;
+    a.src_vals = p->src_vals;
+    a.nsrc = p->nsrc;
+  }
   return a;
 }
 
@@ -1499,7 +1510,26 @@ int exa_patch_set_point_source(exa_patch* p, const exa_point_source* src) {
                          (double)src->variable};
     // ordered after any step still running on the patch's stream
     EXA_CUDA(cudaMemcpyAsync(p->src, h, sizeof(h), cudaMemcpyHostToDevice, p->stream));
+    // the cells the source reaches, and room for its values at their nodes
+    exa::Ops& o = *p->s->ops;
+    if (!p->src_slot) {
+      EXA_CUDA(cudaMalloc(&p->src_slot, (size_t)std::max<long long>(p->ncells, 1) * sizeof(int)));
+      EXA_CUDA(cudaMalloc(&p->src_cells, (size_t)std::max<long long>(p->ncells, 1) * sizeof(int) + sizeof(int)));
+    }
+    int* d_count = p->src_cells + std::max<long long>(p->ncells, 1);
+    EXA_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), p->stream));
+    exa::CellArgs a = patch_args(p);
+    EXA_CUDA(o.source_slots(a, p->src_slot, p->src_cells, d_count, p->stream));
+    int nsrc = 0;
+    EXA_CUDA(cudaMemcpyAsync(&nsrc, d_count, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     EXA_CUDA(cudaStreamSynchronize(p->stream));
+    const size_t per = (size_t)o.nd * (o.order + 1);
+    if (nsrc > p->nsrc || !p->src_vals) {
+      if (p->src_vals) cudaFree(p->src_vals);
+      p->src_vals = nullptr;
+      EXA_CUDA(cudaMalloc(&p->src_vals, (size_t)std::max(nsrc, 1) * per * sizeof(double)));
+    }
+    p->nsrc = nsrc;
   }
   // the captured step graphs hold the old pointer: rebuild them on the next step
   if (p->graph_cfl) cudaGraphExecDestroy(p->graph_cfl);

@@ -181,6 +181,13 @@ struct CellArgs {
   const double* centres;         // [cell][3] cell centres (nullable: from grid_geo), for sources
   const double* grid_t;          // [grid] time at the start of the step (nullable: u_t)
   double u_t;
+  // the point source's values, evaluated ahead of the FP64 predictor (source_values_kernel):
+  // src_slot [cell] = the cell's slot, -1 for cells the source does not reach; src_cells [slot]
+  // = its cell; src_vals [slot][t][node] = the source at the node and time node t (nullable)
+  const int* src_slot;
+  const int* src_cells;
+  double* src_vals;
+  int nsrc;
   // optional export of the predictor's internals, reference layouts (per-cell shims, tests)
   // scratch of the streamed predictor: one slot per resident CTA (set by the launcher)
   double* scratch;
@@ -293,6 +300,63 @@ __device__ __forceinline__ void cell_centre(const CellArgs& a, long cell, int g,
   c[0] = G[0] + (ix + 0.5) * dx[0];
   c[1] = G[1] + (iy + 0.5) * dx[1];
   c[2] = G[2] + (iz + 0.5) * dx[2];
+}
+
+// node spacing as the predictor derives it: 1 / (1 / dx), the reference's 1 / invDx (:339-342)
+template <int DIM>
+__device__ __forceinline__ void source_dx(const CellArgs& a, int g, double* dxv) {
+#pragma unroll
+  for (int d = 0; d < 3; d++) dxv[d] = d < DIM ? 1.0 / (1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d])) : 1.0;
+}
+
+// The cells the point source reaches (source_near, the predictor's test) get consecutive slots;
+// one thread per cell. count starts at zero; the slots' order is immaterial.
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) source_slot_kernel(CellArgs a, int* slot, int* cells, int* count) {
+  const long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.ncells) return;
+  int sl = -1;
+  if (PDE::kSource && a.src) {
+    const int g = a.cell_grid ? a.cell_grid[c] : 0;
+    double dxv[3], cc[3];
+    source_dx<DIM>(a, g, dxv);
+    cell_centre(a, c, g, dxv, cc);
+    if (source_near<DIM>(a.src, cc, dxv)) {
+      sl = atomicAdd(count, 1);
+      cells[sl] = (int)c;
+    }
+  }
+  slot[c] = sl;
+}
+
+// The point source at every node and time node of every slot's cell for the coming step (the
+// algebraicSource values the predictor adds, :323-337): one CTA per slot. It does not depend on
+// the iterate, so the predictor reads these values instead of evaluating the source itself, which
+// keeps that code out of the sweeps' registers.
+template <class PDE, int DIM, int N, int P>
+__global__ void __launch_bounds__(256) source_values_kernel(CellArgs a) {
+  using G = GL<N>;
+  constexpr int n = N + 1, nd = DIM == 3 ? n * n * n : n * n;
+  const int sl = blockIdx.x;
+  if (sl >= a.nsrc) return;
+  const long c = a.src_cells[sl];
+  if (c < a.cell_begin || c >= a.ncells) return;  // another launch's range
+  const int g = a.cell_grid ? a.cell_grid[c] : 0;
+  double dxv[3], cc[3];
+  source_dx<DIM>(a, g, dxv);
+  cell_centre(a, c, g, dxv, cc);
+  const double tcell = a.grid_t ? a.grid_t[g] : a.u_t;
+  const double dt = a.grid_dt ? a.grid_dt[g] : a.u_dt;
+  for (int p = threadIdx.x; p < nd; p += blockDim.x) {
+    int co[3];
+    node_coords<DIM, n>(p, co);
+    double x[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) x[d] = cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5);
+#pragma unroll 1
+    for (int i = 0; i < n; i++)
+      a.src_vals[((size_t)sl * n + i) * nd + p] = point_source<DIM>(a.src, x, tcell + G::nodes(i) * dt);
+  }
 }
 
 __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {

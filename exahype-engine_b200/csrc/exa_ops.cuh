@@ -19,7 +19,7 @@ namespace exa {
 struct Ops {
   // layout version of this interface: an application library compiled against another layout is
   // refused by exa_register_pde (its object would be read with the wrong offsets)
-  static constexpr int kAbi = 6;
+  static constexpr int kAbi = 7;
   int abi = kAbi;
   int dim, order, nvar, npar, nd, nf, cpb;
   size_t sz_luh, sz_lduh, sz_qhb, sz_fhb, sz_lQi, sz_lFi, sz_lQhi, sz_lFhi;
@@ -52,6 +52,10 @@ struct Ops {
   // (faces of type EXA_BC_USER)
   bool adjust_ok = false, user_bc_ok = false;
   virtual cudaError_t adjust(const CellArgs& a, cudaStream_t st) = 0;
+  // the point source's slot table: slot[cell] (-1 off the source), cells[slot], *count slots
+  // (count zeroed by the caller); the FP64 predictor then reads the values source_values_kernel
+  // evaluates ahead of it
+  virtual cudaError_t source_slots(const CellArgs& a, int* slot, int* cells, int* count, cudaStream_t st) = 0;
   // per-cell volume (mode 0), surface (1) and face (2) integrals of one cell (cell_integral_kernel)
   virtual cudaError_t cell_integral(int mode, double* lduh, const double* in, int direction, int orientation,
                                     const double* dx, cudaStream_t st) = 0;
@@ -149,6 +153,14 @@ struct OpsImpl final : Ops {
         grid = sms * std::max(occ, 1);
       }
       blocks = std::min<long long>(groups, grid);
+    }
+    if constexpr (PDE::kSource) {
+      // the point source's values at the slot cells' nodes, ahead of the predictor that reads them
+      if (a.src && a.src_slot && a.nsrc > 0) {
+        constexpr int tpb = S::nd >= 256 ? 256 : (S::nd + 31) / 32 * 32;
+        source_values_kernel<PDE, DIM, N, P><<<(unsigned)a.nsrc, tpb, 0, st>>>(a);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
     }
     CellArgs b = a;
     b.bulk_luh = (reinterpret_cast<uintptr_t>(a.luh) % 16 == 0) && ((S::nd * S::D) % 2 == 0);
@@ -327,6 +339,11 @@ struct OpsImpl final : Ops {
       (void)a, (void)st;
       return cudaErrorNotSupported;
     }
+  }
+  cudaError_t source_slots(const CellArgs& a, int* slot, int* cells, int* count, cudaStream_t st) override {
+    if (a.ncells <= 0) return cudaSuccess;
+    source_slot_kernel<PDE, DIM, N, P><<<(unsigned)((a.ncells + 255) / 256), 256, 0, st>>>(a, slot, cells, count);
+    return cudaGetLastError();
   }
   OpsImpl() {
     adjoint_ok = kAdj;

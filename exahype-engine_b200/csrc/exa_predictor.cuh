@@ -196,17 +196,11 @@ predictor_kernel(CellArgs a) {
     const double dt = s_dt[lc];
 
     // point source (algebraicSource at x_p, t + node_i dt, :323-337): only cells near the source
-    bool srcOn = false;
+    // (slot >= 0), whose values source_values_kernel evaluated ahead of this launch. Only patches
+    // carry a source, and a patch's source always comes with its slot table.
+    const int srcSlot = (PDE::kSource && a.src && a.src_slot && live) ? a.src_slot[cell] : -1;
+    const bool srcOn = srcSlot >= 0;
     double tcell = 0.0;
-    if (PDE::kSource && a.src && live) {
-      const int g = a.cell_grid ? a.cell_grid[cell] : 0;
-      const double dxv[3] = {1.0 / s_invdx[lc][0], DIM > 1 ? 1.0 / s_invdx[lc][1] : 1.0,
-                             DIM > 2 ? 1.0 / s_invdx[lc][2] : 1.0};
-      double cc[3];
-      cell_centre(a, cell, g, dxv, cc);
-      srcOn = source_near<DIM>(a.src, cc, dxv);
-      tcell = a.grid_t ? a.grid_t[g] : a.u_t;
-    }
     if (ALG && live) {
       const int g = a.cell_grid ? a.cell_grid[cell] : 0;
       tcell = a.grid_t ? a.grid_t[g] : a.u_t;
@@ -236,17 +230,8 @@ predictor_kernel(CellArgs a) {
         for (int m = 0; m < V; m++) Sv[m] = ALG ? Sv[m] + ncp_part[m] : ncp_part[m];
       }
     };
-    // source value of this node at time node i (evaluated only where srcOn)
-    auto src_at = [&](int i) -> double {
-      const int g = a.cell_grid ? a.cell_grid[cell] : 0;
-      const double dxv[3] = {1.0 / s_invdx[lc][0], DIM > 1 ? 1.0 / s_invdx[lc][1] : 1.0,
-                             DIM > 2 ? 1.0 / s_invdx[lc][2] : 1.0};
-      double cc[3], x[3];
-      cell_centre(a, cell, g, dxv, cc);
-#pragma unroll
-      for (int d = 0; d < 3; d++) x[d] = cc[d] + dxv[d] * (G::nodes(co[d]) - 0.5);
-      return point_source<DIM>(a.src, x, tcell + G::nodes(i) * s_dt[lc]);
-    };
+    // source value of this node at time node i (read only where srcOn)
+    auto src_at = [&](int i) -> double { return a.src_vals[((size_t)srcSlot * n + i) * nd + p]; };
 
     // new iterate of the sweep, accumulated in registers time node by time node (the iK1 time
     // solve distributed over phase 3); the old iterate is staged in the slices q_s [t][node][D]
