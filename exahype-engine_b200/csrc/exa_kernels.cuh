@@ -359,6 +359,20 @@ __global__ void __launch_bounds__(256) source_values_kernel(CellArgs a) {
   }
 }
 
+// Picard residual of a cell whose nd nodes run on consecutive threads: the segment head of each
+// warp the cell spans stores its warp's partial in slot (warp - the cell's first warp); the sum
+// runs over the slots in order. A shared-memory atomic would add the partials in arrival order,
+// whose rounding differs from run to run and can flip the exit test of a cell at the tolerance.
+template <int nd>
+__host__ __device__ constexpr int res_slots() { return (nd + 30) / 32 + 1; }
+template <int nd>
+__device__ __forceinline__ double cell_residual(const double* slots, int c) {
+  const int k = ((c * nd + nd - 1) >> 5) - ((c * nd) >> 5);
+  double r = slots[0];
+  for (int j = 1; j <= k; j++) r += slots[j];
+  return r;
+}
+
 __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
   // non-negative doubles order like their bit patterns
   atomicMin(reinterpret_cast<unsigned long long*>(addr), static_cast<unsigned long long>(__double_as_longlong(v)));
@@ -989,6 +1003,9 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_bulk_kernel
     mbar_init(&s_bar[1], 1);
     fence_mbar_init();
   }
+  // per-cell CFL minima; from then on the thread that reads a cell's minimum resets it, so that
+  // every reset is ordered before the next group's additions by the barrier that ends a group
+  if (tid < CPB) s_min[tid] = __longlong_as_double(0x7ff0000000000000ll);
   __syncthreads();
   if (tid == 0 && (int)blockIdx.x < ngroups) issue(blockIdx.x, 0);
   int co[3];
@@ -1014,7 +1031,6 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_bulk_kernel
     double* st = smem + (size_t)b * B::stage;
     const int cell = a.cell_begin + grp * CPB + lc;
     const bool live = inr && cell < a.ncells;
-    if (tid < CPB) s_min[tid] = __longlong_as_double(0x7ff0000000000000ll);
     const int g = (live && a.cell_grid) ? a.cell_grid[cell] : 0;
     double invDx[3];
 #pragma unroll
@@ -1081,10 +1097,12 @@ __global__ void __launch_bounds__(Shape<PDE, DIM, N, P>::TPB) update_bulk_kernel
       bulk_commit();
     }
     if (p == 0 && live) {
-      if (a.cell_dt) a.cell_dt[cell] = s_min[lc];
-      if (a.grid_dt_next) atomic_min_pos(&a.grid_dt_next[g], s_min[lc]);
+      const double mn = s_min[lc];
+      s_min[lc] = __longlong_as_double(0x7ff0000000000000ll);
+      if (a.cell_dt) a.cell_dt[cell] = mn;
+      if (a.grid_dt_next) atomic_min_pos(&a.grid_dt_next[g], mn);
     }
-    // s_min and this buffer are reused two groups on
+    // s_min is reused by the next group, this buffer two groups on
     __syncthreads();
   }
   if (tid == 0) {
