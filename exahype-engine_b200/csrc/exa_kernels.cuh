@@ -359,19 +359,17 @@ __global__ void __launch_bounds__(256) source_values_kernel(CellArgs a) {
   }
 }
 
-// Picard residual of a cell whose nd nodes run on consecutive threads: the segment head of each
-// warp the cell spans stores its warp's partial in slot (warp - the cell's first warp); the sum
-// runs over the slots in order. A shared-memory atomic would add the partials in arrival order,
-// whose rounding differs from run to run and can flip the exit test of a cell at the tolerance.
-template <int nd>
-__host__ __device__ constexpr int res_slots() { return (nd + 30) / 32 + 1; }
-template <int nd>
-__device__ __forceinline__ double cell_residual(const double* slots, int c) {
-  const int k = ((c * nd + nd - 1) >> 5) - ((c * nd) >> 5);
-  double r = slots[0];
-  for (int j = 1; j <= k; j++) r += slots[j];
-  return r;
+// Picard residual of a cell whose nodes span several warps: each warp's partial (a fixed shuffle
+// tree) is added to the cell's sum as an unsigned 64-bit fixed-point number in units of 2^-100.
+// Integer addition does not depend on the order in which the warps arrive, so a cell at the
+// tolerance takes the same number of sweeps in every run (shared-memory atomics on doubles add in
+// arrival order, whose rounding varies). A partial is clamped to 2^60 units (about 9e-13, far
+// above the 1e-14 tolerance; at most 8 warps per cell keep the sum below 2^63); non-finite
+// partials clamp there too, so their cell does not converge, and the caller flags them.
+__device__ __forceinline__ unsigned long long residual_units(double res) {
+  return (unsigned long long)fmin(res * 0x1p100, 0x1p60);
 }
+constexpr double kResidualTolUnits = 1e-7 * 1e-7 * 0x1p100;  // the exit test |res|^2 < 1e-7^2
 
 __device__ __forceinline__ void atomic_min_pos(double* addr, double v) {
   // non-negative doubles order like their bit patterns

@@ -72,9 +72,7 @@ predictor_kernel(CellArgs a) {
   __shared__ double s_A[n], s_B[n];  // sum_i iK1[t][i] F0[i] and sum_i iK1[t][i] w_i (sweep 0)
   __shared__ double s_lw[CPB * DIM * NL];  // w_a w_b dt / dx_d of every line
   __shared__ double s_dt[CPB], s_invdx[CPB][3];
-  // per-cell residual partials, one per warp the cell spans (res_slots), double-buffered by sweep
-  // parity; summed in warp order (cell_residual), so that the exit test is the same in every run
-  __shared__ double s_res[2][CPB][res_slots<nd>()];
+  __shared__ unsigned long long s_res[2][CPB];  // per-cell residual (residual_units), by sweep parity
   __shared__ __align__(8) uint64_t s_bar;  // completion of the staging copy
 
   const int tid = threadIdx.x;
@@ -171,6 +169,8 @@ predictor_kernel(CellArgs a) {
 #pragma unroll
       for (int d = 0; d < 3; d++)
         s_invdx[tid][d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
+      s_res[0][tid] = 0;
+      s_res[1][tid] = 0;
     }
     bool timed_out = false;
     if (PERSIST && a.bulk_luh) timed_out = !mbar_wait_bounded(&s_bar, iter & 1, kBulkWaitLimitNs);
@@ -513,8 +513,8 @@ predictor_kernel(CellArgs a) {
             }
         }
       }
-      // per-cell residual: segmented warp tree, then each segment head stores its warp's partial
-      // in this sweep's buffer (its last readers, two sweeps back, are behind a barrier)
+      // per-cell residual: segmented warp tree, one shared atomic per segment head, into this
+      // sweep's buffer (zeroed at least one barrier before any thread adds to it)
       {
         const int lane = tid & 31;
         const int seg_end = (lc + 1) * nd - 1;
@@ -523,7 +523,10 @@ predictor_kernel(CellArgs a) {
           const double o2 = __shfl_down_sync(0xffffffffu, res, off2);
           if (lane + off2 < 32 && tid + off2 <= seg_end) res += o2;
         }
-        if ((p == 0 || lane == 0) && work) s_res[s & 1][lc][(tid >> 5) - ((lc * nd) >> 5)] = res;
+        if ((p == 0 || lane == 0) && work) {
+          atomicAdd(&s_res[s & 1][lc], residual_units(res));
+          if (!finite(res) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+        }
       }
       __syncthreads();
       // exit test (:407-412): |res|^2 < 1e-7^2, unless a fixed sweep count is requested; every
@@ -531,12 +534,11 @@ predictor_kernel(CellArgs a) {
       unsigned conv = 0;
       if (a.max_picard <= 0) {
 #pragma unroll
-        for (int c = 0; c < CPB; c++) conv |= (cell_residual<nd>(s_res[s & 1][c], c) < 1e-7 * 1e-7 ? 1u : 0u) << c;
+        for (int c = 0; c < CPB; c++) conv |= ((double)s_res[s & 1][c] < kResidualTolUnits ? 1u : 0u) << c;
       }
       conv &= active;
       if (work) {
         sweeps = s + 1;
-        if (p == 0 && !finite(cell_residual<nd>(s_res[s & 1][lc], lc)) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
         done = (conv >> lc) & 1u;
         // the new iterate becomes the old one, except after the last sweep: lFhi is the flux of
         // the iterate that sweep started from (a fixed sweep count, or the cap without convergence)
@@ -557,6 +559,9 @@ predictor_kernel(CellArgs a) {
           last_old_is_luh = s == 0;
         }
       }
+      // the buffer of the next sweep: its last readers (the previous sweep's test) passed the
+      // barrier above; the next sweep's first barrier separates this from the next additions
+      if (tid < CPB) s_res[(s + 1) & 1][tid] = 0;
       active &= ~conv;
       // the gradients of the next sweep read the neighbours' copied iterate
       if (GRAD) __syncthreads();

@@ -92,9 +92,7 @@ predictor_mixed_kernel(CellArgs a) {
   __shared__ double s_w[n], s_Kxi[n * n];
   __shared__ double s_lw[CPB * DIM * NL];
   __shared__ double s_dt[CPB], s_invdx[CPB][3];
-  // per-cell residual partials, one per warp the cell spans (res_slots), double-buffered by sweep
-  // parity; summed in warp order (cell_residual), so that the exit test is the same in every run
-  __shared__ double s_res[2][CPB][res_slots<nd>()];
+  __shared__ unsigned long long s_res[2][CPB];  // per-cell residual (residual_units), by sweep parity
 
   const int tid = threadIdx.x;
   const bool inr = tid < CPB * nd;
@@ -126,6 +124,8 @@ predictor_mixed_kernel(CellArgs a) {
 #pragma unroll
     for (int d = 0; d < 3; d++)
       s_invdx[tid][d] = d < DIM ? 1.0 / (a.grid_dx ? a.grid_dx[g * 3 + d] : a.u_dx[d]) : 0.0;
+    s_res[0][tid] = 0;
+    s_res[1][tid] = 0;
   }
   double* u = sU + ((size_t)lc * nd + p) * DQ;
   if (inr) {
@@ -339,18 +339,20 @@ predictor_mixed_kernel(CellArgs a) {
         const double v = __shfl_down_sync(0xffffffffu, res, o2);
         if (lane + o2 < 32 && tid + o2 <= seg_end) res += v;
       }
-      if ((p == 0 || lane == 0) && work) s_res[s & 1][lc][(tid >> 5) - ((lc * nd) >> 5)] = res;
+      if ((p == 0 || lane == 0) && work) {
+          atomicAdd(&s_res[s & 1][lc], residual_units(res));
+          if (!finite(res) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
+        }
     }
     __syncthreads();
     unsigned conv = 0;
     if (a.max_picard <= 0) {
 #pragma unroll
-      for (int c = 0; c < CPB; c++) conv |= (cell_residual<nd>(s_res[s & 1][c], c) < 1e-7 * 1e-7 ? 1u : 0u) << c;
+      for (int c = 0; c < CPB; c++) conv |= ((double)s_res[s & 1][c] < kResidualTolUnits ? 1u : 0u) << c;
     }
     conv &= active;
     if (work) {
       sweeps = s + 1;
-      if (p == 0 && !finite(cell_residual<nd>(s_res[s & 1][lc], lc)) && a.status) atomicOr(a.status, ST_NONFINITE_PREDICTOR);
       done = (conv >> lc) & 1u;
       if (!done && s + 1 < maxIter) {
         // the new iterate becomes the old one: dq = delta (sweep 0's FP64 flux blocks, which alias
@@ -363,6 +365,7 @@ predictor_mixed_kernel(CellArgs a) {
         last_old_is_luh = s == 0;
       }
     }
+    if (tid < CPB) s_res[(s + 1) & 1][tid] = 0;
     active &= ~conv;
     if (!active) break;
   }
