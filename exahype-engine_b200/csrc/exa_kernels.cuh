@@ -100,7 +100,10 @@ struct Shape {
   static constexpr int nf = DIM == 3 ? n * n : n;          // nodes per face
   static constexpr int NL = nd / n;                        // lines per direction
   // cells per CTA: about 256 threads, at most 32 cells (the predictors' per-CTA cell masks)
-  static constexpr int CPB = nd >= 256 ? 1 : (256 / nd > 32 ? 32 : 256 / nd);
+  // threads per CTA aimed at: 256, or 128 for the 2D SWE shape (n=5, V=4), whose four resident
+  // CTAs per SM then wait at their barriers in groups of four warps instead of eight
+  static constexpr int kThreads = (DIM == 2 && n == 5 && V == 4) ? 128 : 256;
+  static constexpr int CPB = nd >= kThreads ? 1 : (kThreads / nd > 32 ? 32 : kThreads / nd);
   static constexpr int TPB = (CPB * nd + 31) / 32 * 32;    // whole warps; the tail threads idle
   static constexpr int sizeQhb = 2 * DIM * nf * D;
   static constexpr int sizeFhb = 2 * DIM * nf * V;
@@ -127,7 +130,11 @@ struct Shape {
     return sizeof(double) * (size_t)(even(CPB * qcs(dq) + smemF + CPB * nd * dq) + smemStage);
   }
   // resident CTAs per SM: two when their shared memory fits (228 KB per SM, 1 KB reserved per CTA)
-  static constexpr int blocks_for(int dq) { return 2 * (smem_for(dq) + 3 * 1024) <= 228 * 1024 ? 2 : 1; }
+  // (up to four for CTAs of at most 128 threads)
+  static constexpr int blocks_for(int dq) {
+    return TPB <= 128 ? ((int)(228 * 1024 / (smem_for(dq) + 3 * 1024)) > 4 ? 4 : ((int)(228 * 1024 / (smem_for(dq) + 3 * 1024)) < 1 ? 1 : (int)(228 * 1024 / (smem_for(dq) + 3 * 1024))))
+                      : (2 * (smem_for(dq) + 3 * 1024) <= 228 * 1024 ? 2 : 1);
+  }
   static constexpr bool fits_cta(size_t bytes) { return bytes + 4096 <= 227 * 1024; }
   // per-node stride of the iterate slices and the luh block in shared memory: D rounded up to an
   // odd count (an even stride puts several lanes of a warp on one bank), unless the padding
