@@ -339,7 +339,7 @@ int exa_limiter_dmp(exa_solver* s, int ncells, const double* luh, int nobs, doub
                     double* bmax, unsigned char* ok, void* stream);
 /* the same for one cell on host arrays, as the generated limiting solver calls them
  * (GenericLimiterSolverImplementation.template:40-62); exa_discreteMaximumPrincipleAndMinAndMaxSearch
- * sets *ok to the verdict */
+ * sets *ok to the decision */
 int exa_projectOnFVLimiterSpace(exa_solver* s, const double* luh, double* lim, int ghost);
 int exa_projectOnDGSpace(exa_solver* s, const double* lim, double* luh, int ghost);
 int exa_findCellLocalMinAndMax(exa_solver* s, const double* luh, int nobs, double* mn, double* mx);
